@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Benchmark: ICGN subsets/s on the second-order-at-scale workload.
+
+Workload (one step = one image pair through the whole hot path):
+    4096 x 4096 uint16 (12-bit) seeded speckle pair under 1% uniaxial strain,
+    0.5 deg rotation and 1e-6 px^-1 quadratic terms; circular subsets r = 30
+    on a 10 px grid (~150k subsets), 12-parameter (second-order) ICGN,
+    max_norm 1e-5, 50 iterations, FP32 interpolation / FP64 reductions.
+    step = prefilter(f) + prefilter(g) + batched ICGN solve of every subset.
+
+value : subsets/s with pixels, descriptors and outputs resident in HBM
+        (gpv_image_update_device + gpv_solve_batch_device), device-timed.
+e2e   : the same through the host C ABI (gpv_image_update from pinned host
+        pixels x2, gpv_solve_batch with host descriptors in / results out),
+        device-timed on the library stream; H2D / D2H bytes counted.
+roofline: the ICGN kernel against a live-measured FP32 FMA peak (algorithmic
+        work = 42 tap FMAs per target sample + 90 per reference sample).
+cpu_baseline: the FP64 C oracle (restatement of the reference's Rust solver)
+        on a bounded sample of the same subsets, all host threads.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU (torchrun): every rank solves its own replica of the workload
+(replicas only: the path has no exchange step); value = all ranks' subsets
+/ max over ranks of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "geopyv-dev_b200"))
+
+METRIC = "ICGN subsets/s at <=1e-3 px vs FP64 oracle; p50/p99 served solve latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--scale-down", type=int, default=1)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def load_workload(args):
+    from gpv import synth
+    t = time.time()
+    W = synth.workload(args.config, scale_down=args.scale_down)
+    W["gen_s"] = time.time() - t
+    return W
+
+
+def algorithmic_flop(res):
+    """2 x (42 FMA per target sample x iterations + 90 FMA per reference sample)."""
+    n = res["n_px"].astype(np.float64)
+    it = res["iterations"].astype(np.float64)
+    return 2.0 * (42.0 * float(np.sum(n * it)) + 90.0 * float(np.sum(n)))
+
+
+def cpu_baseline(W, args, nthreads=None, seconds=None, rng_seed=7):
+    """Oracle (FP64 C restatement) on a bounded sample: subsets/s of the full step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import gpv
+    O.build()
+    nthreads = nthreads or O.lib().gpvo_max_threads()
+    seconds = seconds or args.cpu_seconds
+    d = gpv.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
+    n = len(d)
+    rng = np.random.default_rng(rng_seed)
+    perm = rng.permutation(n)
+    f64 = W["f"].astype(np.float64)
+    t0 = time.perf_counter()
+    Cf = O.get_c(f64, 20, nthreads)
+    t_pref1 = time.perf_counter() - t0
+    Cg = O.get_c(W["g"].astype(np.float64), 20, nthreads)
+    # calibrate, then size the sample to ~seconds of solving
+    k = min(n, max(32, 4 * nthreads))
+    t0 = time.perf_counter()
+    O.solve_batch(Cf, Cg, W["f"].shape, 20, d[perm[:k]], max_norm=1e-5, max_iterations=50, nthreads=nthreads)
+    per = (time.perf_counter() - t0) / k
+    s = int(min(n - k, max(64, seconds / max(per, 1e-9))))
+    sample = perm[k:k + s]
+    t0 = time.perf_counter()
+    ref = O.solve_batch(Cf, Cg, W["f"].shape, 20, d[sample], max_norm=1e-5, max_iterations=50, nthreads=nthreads)
+    t_solve = time.perf_counter() - t0
+    per = t_solve / len(sample)
+    t_step = 2 * t_pref1 + per * n  # prefilter both images + every subset
+    return dict(value=n / t_step, cores=int(nthreads), per_subset_s=per, prefilter_s=t_pref1,
+                sample_idx=sample, sample_res=ref, n=n, solve_s=t_solve)
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    """--impl reference: the oracle restatement of the reference's CPU solver."""
+    if rank != 0:
+        return
+    W = load_workload(args)
+    steps = []
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(W, args, seconds=max(2.0, args.cpu_seconds / 3), rng_seed=100 + i)
+        if i >= args.warmup:
+            steps.append(b)
+    vals = [b["value"] for b in steps]
+    v = float(np.mean(vals))
+    b = steps[-1]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "subsets/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * W["coords"].shape[0] / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": W["name"], "subsets": int(W["coords"].shape[0])},
+        "cpu_baseline": {"value": v, "unit": "subsets/s", "cores": b["cores"], "kind": "port",
+                         "sample": f"{len(b['sample_idx'])} random subsets per step + prefilter of both images "
+                                   f"(FP64 C restatement of src/subset.rs / src/image.rs, OpenMP)"},
+        "e2e": {"value": v, "unit": "subsets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import ctypes as ct
+
+    import torch
+
+    import gpv
+    from gpv import _lib
+    torch.cuda.set_device(local)
+    W = load_workload(args)
+    h, w = W["f"].shape
+    n = len(W["coords"])
+    L = _lib.lib()
+    ctx = gpv.Context(local)
+    prec = gpv.PREC_FP64 if args.precision == "fp64" else gpv.PREC_MIXED
+    keep64 = prec == gpv.PREC_FP64
+    desc = gpv.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
+    max_r = int(W["radius"].max())
+    ctx.reserve(n, max_r, 50)
+    # images from device-resident pixels
+    px_dtype = W["f"].dtype
+    tdt = torch.uint8 if px_dtype == np.uint8 else torch.int16
+    f_dev = torch.from_numpy(W["f"].view(np.uint8 if px_dtype == np.uint8 else np.int16).copy()).cuda()
+    g_dev = torch.from_numpy(W["g"].view(np.uint8 if px_dtype == np.uint8 else np.int16).copy()).cuda()
+    dcode = _lib.DTYPES[px_dtype]
+    F = gpv.Image(image_gs=W["f"], border=20, keep_f64=keep64, ctx=ctx)
+    G = gpv.Image(image_gs=W["g"], border=20, keep_f64=keep64, ctx=ctx)
+    desc_dev = torch.from_numpy(desc.view(np.uint8).copy()).cuda()
+    key = 3 * desc["radius"].astype(np.int64) + desc["order"]
+    order = np.argsort(-key, kind="stable").astype(np.int32)
+    order_dev = torch.from_numpy(order).cuda()
+    out_dev = torch.empty(n * _lib.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    prm = _lib.SolveParams(max_norm=1e-5, tolerance=0.75, max_iterations=50, flags=0, precision=prec,
+                           reserved=0, mask=None, history=None)
+    stream = torch.cuda.current_stream()
+    sptr = ct.c_void_p(stream.cuda_stream)
+    launches_per_step = 5  # 2 images x (row pass + column pass) + 1 solve
+    # the prefilter runs on the library's context stream, the solve on torch's
+    # current stream; events order the two
+    ctx_stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def full_step(es0=None, es1=None):
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        ctx_stream.wait_event(ev)
+        _lib.check(L.gpv_image_update_device(F.handle, ct.c_void_p(f_dev.data_ptr()), dcode), "update f")
+        _lib.check(L.gpv_image_update_device(G.handle, ct.c_void_p(g_dev.data_ptr()), dcode), "update g")
+        ev2 = torch.cuda.Event()
+        ev2.record(ctx_stream)
+        stream.wait_event(ev2)
+        if es0 is not None:
+            es0.record(stream)
+        _lib.check(L.gpv_solve_batch_device(ctx.handle, F.handle, G.handle, ct.c_void_p(desc_dev.data_ptr()),
+                                            ct.c_void_p(order_dev.data_ptr()), n, ct.byref(prm),
+                                            ct.c_void_p(out_dev.data_ptr()), sptr), "solve")
+        if es1 is not None:
+            es1.record(stream)
+
+    peak_buf = ct.c_double(0.0)
+    _lib.check(L.gpv_probe_fp32_peak(ctx.handle, ct.byref(peak_buf)), "probe")
+    fp32_peak = peak_buf.value
+    for _ in range(args.warmup):
+        full_step()
+    torch.cuda.synchronize()
+    res = np.frombuffer(out_dev.cpu().numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    solve_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e0.record(stream)
+    for k in range(args.steps):
+        full_step(*solve_ev[k])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    cl = clocks.stop()
+    barrier(world)
+    t_ms = e0.elapsed_time(e1)
+    solve_ms = [a.elapsed_time(b) for a, b in solve_ev]
+    t_max = max_over_ranks(t_ms, world)
+    value = world * n * args.steps / (t_max * 1e-3)
+
+    # ---- e2e through the host C ABI (pinned host buffers) ----
+    f_pin = torch.from_numpy(W["f"].view(np.uint8 if px_dtype == np.uint8 else np.int16).copy()).pin_memory()
+    g_pin = torch.from_numpy(W["g"].view(np.uint8 if px_dtype == np.uint8 else np.int16).copy()).pin_memory()
+    d_pin = torch.from_numpy(desc.view(np.uint8).copy()).pin_memory()
+    o_pin = torch.empty(n * _lib.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+
+    def e2e_step():
+        _lib.check(L.gpv_image_update(F.handle, ct.c_void_p(f_pin.data_ptr()), dcode), "update f (host)")
+        _lib.check(L.gpv_image_update(G.handle, ct.c_void_p(g_pin.data_ptr()), dcode), "update g (host)")
+        _lib.check(L.gpv_solve_batch(ctx.handle, F.handle, G.handle, ct.c_void_p(d_pin.data_ptr()), n,
+                                     ct.byref(prm), ct.c_void_p(o_pin.data_ptr())), "solve (host)")
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    lat = []
+    a0.record(ctx_stream)
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        e2e_step()
+        lat.append(time.perf_counter() - t)
+    a1.record(ctx_stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(a0.elapsed_time(a1), world)
+    e2e_value = world * n * args.steps / (e2e_ms * 1e-3)
+    res_h = np.frombuffer(o_pin.numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
+    h2d = W["f"].nbytes + W["g"].nbytes + desc.nbytes
+    d2h = res_h.nbytes
+
+    if rank != 0:
+        return
+    # ---- accuracy on the CPU-baseline sample + CPU baseline ----
+    cpu = None
+    acc = {}
+    if not args.no_cpu_baseline:
+        cpu = cpu_baseline(W, args)
+        idx = cpu["sample_idx"]
+        ref = cpu["sample_res"]
+        ok = ref["status"] == 0
+        dpx = np.abs(res["p"][idx, :2] - ref["p"][:, :2])[ok]
+        dstr = np.abs(res["p"][idx, 2:6] - ref["p"][:, 2:6])[ok]
+        acc = {"oracle_sample": int(len(idx)), "max_disp_err_px": float(dpx.max()),
+               "max_strain_err": float(dstr.max()),
+               "flag_agreement": float(np.mean((res["converged"][idx] == ref["converged"]) &
+                                               (res["quality_ok"][idx] == ref["quality_ok"]))),
+               "iteration_agreement": float(np.mean(res["iterations"][idx] == ref["iterations"]))}
+    flop = algorithmic_flop(res)
+    solve_avg_ms = float(np.mean(solve_ms))
+    achieved = flop / (solve_avg_ms * 1e-3) / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "icgn_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            tj = json.load(open(tpath))
+            traffic = float(tj["bytes_per_subset_iteration"]) * float(np.sum(res["iterations"])) + \
+                float(tj.get("bytes_per_subset_setup", 0.0)) * n
+        except Exception:
+            traffic = None
+    samples = float(np.sum(res["n_px"].astype(np.float64) * (res["iterations"] + 1)))
+    line = {
+        "metric": METRIC, "value": value, "unit": "subsets/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if prec == gpv.PREC_MIXED else "f64", "data": "synthetic",
+        "config": {"workload": W["name"], "subsets": n, "image": [h, w], "pixel_dtype": str(px_dtype),
+                   "radius": max_r, "order": 2 if args.config == 2 else "mixed", "max_norm": 1e-5,
+                   "max_iterations": 50, "precision": args.precision,
+                   "step": "prefilter(f)+prefilter(g)+batched ICGN solve",
+                   "l2": "inputs larger than L2: 2 x 4136^2 FP32 coefficients + FP64 row pass (~410 MB) rewritten each step",
+                   "parallelism": f"replicas x{world}"},
+        "solve_ms": solve_avg_ms, "prefilter_ms": t_max / args.steps - solve_avg_ms,
+        "samples_per_s": world * samples * args.steps / (t_max * 1e-3),
+        "iterations_mean": float(np.mean(res["iterations"])),
+        "converged_frac": float(np.mean(res["converged"])),
+        "accuracy": acc,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
+                     "kernel": "icgn_mixed" if prec == gpv.PREC_MIXED else "icgn_fp64",
+                     "peak_source": "measured live: register-only FP32 FMA kernel (gpv_probe_fp32_peak)",
+                     "work": "2 x (42 FMA per target sample x iterations + 90 FMA per reference sample)"},
+        "e2e": {"value": e2e_value, "unit": "subsets/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)), "p99": 1e3 * float(np.percentile(lat, 99))}},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": cl,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = {"value": cpu["value"], "unit": "subsets/s", "cores": cpu["cores"], "kind": "port",
+                                "sample": f"{len(cpu['sample_idx'])} random subsets of the same batch solved by the FP64 C "
+                                          f"oracle in {cpu['solve_s']:.1f} s + oracle prefilter of both images "
+                                          f"({2 * cpu['prefilter_s']:.1f} s), scaled to the full step"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,474 @@
+// api.cpp -- the C ABI (include/gpv.h) over the device kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace gpv {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int DevBuf::ensure(size_t want) {
+    if (want <= bytes && ptr) return GPV_SUCCESS;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    const size_t sz = want < 256 ? 256 : want;
+    cudaError_t e = cudaMalloc(&ptr, sz);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        set_error(std::string("cudaMalloc(") + std::to_string(sz) + "): " + cudaGetErrorString(e));
+        return GPV_ERR_NOMEM;
+    }
+    bytes = sz;
+    return GPV_SUCCESS;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+struct short2_h {
+    int16_t x, y;
+};
+
+// Circular local masks for radii 1..max_radius in the scan order of
+// LocalMask::circle (src/masks.rs:69-109): rows y = -r..r, columns x = -r..r,
+// kept when sqrt(x^2 + y^2) <= r (i.e. x^2 + y^2 <= r^2 for integers).
+int ensure_tables(gpv_context *ctx, int max_radius) {
+    if (max_radius <= ctx->table_radius) return GPV_SUCCESS;
+    if (max_radius > 4000) {
+        set_error("radius above 4000 is not supported");
+        return GPV_ERR_INVALID;
+    }
+    std::vector<short2_h> offs;
+    std::vector<int32_t> toff(max_radius + 1, 0), tn(max_radius + 1, 0);
+    for (int r = 1; r <= max_radius; r++) {
+        toff[r] = (int32_t)offs.size();
+        for (int y = -r; y <= r; y++)
+            for (int x = -r; x <= r; x++)
+                if (x * x + y * y <= r * r) offs.push_back({(int16_t)x, (int16_t)y});
+        tn[r] = (int32_t)offs.size() - toff[r];
+    }
+    if (int rc = ctx->offs.ensure(offs.size() * sizeof(short2_h))) return rc;
+    if (int rc = ctx->tab_off.ensure(toff.size() * sizeof(int32_t))) return rc;
+    if (int rc = ctx->tab_n.ensure(tn.size() * sizeof(int32_t))) return rc;
+    GPV_CUDA_TRY(cudaMemcpy(ctx->offs.ptr, offs.data(), offs.size() * sizeof(short2_h), cudaMemcpyHostToDevice));
+    GPV_CUDA_TRY(cudaMemcpy(ctx->tab_off.ptr, toff.data(), toff.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    GPV_CUDA_TRY(cudaMemcpy(ctx->tab_n.ptr, tn.data(), tn.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    ctx->h_tab_off = toff;
+    ctx->h_tab_n = tn;
+    ctx->table_radius = max_radius;
+    return GPV_SUCCESS;
+}
+
+static size_t dtype_size(int dtype) {
+    switch (dtype) {
+        case GPV_U8: return 1;
+        case GPV_U16: return 2;
+        case GPV_F32: return 4;
+        case GPV_F64: return 8;
+        default: return 0;
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace gpv
+
+using namespace gpv;
+
+extern "C" {
+
+const char *gpv_version(void) { return "gpv-b200 0.1.0 (sm_100a)"; }
+
+int gpv_abi_version(void) { return GPV_ABI_VERSION; }
+
+size_t gpv_last_error(char *buf, size_t len) {
+    const std::string &e = g_last_error;
+    if (buf && len) {
+        const size_t k = std::min(len - 1, e.size());
+        std::memcpy(buf, e.data(), k);
+        buf[k] = 0;
+    }
+    return e.size();
+}
+
+int gpv_context_create(int device, gpv_context **out) {
+    if (!out) { set_error("out is NULL"); return GPV_ERR_INVALID; }
+    *out = nullptr;
+    int ndev = 0;
+    GPV_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) { set_error("device index out of range"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(device);
+    auto *ctx = new gpv_context();
+    ctx->device = device;
+    cudaError_t e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        set_error(std::string("context: ") + cudaGetErrorString(e));
+        delete ctx;
+        return GPV_ERR_CUDA;
+    }
+    *out = ctx;
+    return GPV_SUCCESS;
+}
+
+int gpv_context_destroy(gpv_context *ctx) {
+    if (!ctx) return GPV_SUCCESS;
+    DeviceGuard dg(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (DevBuf *b : {&ctx->offs, &ctx->tab_off, &ctx->tab_n, &ctx->scratch, &ctx->queue, &ctx->desc_dev, &ctx->out_dev,
+                      &ctx->order_dev, &ctx->hist_dev, &ctx->eval_dev})
+        b->release();
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return GPV_SUCCESS;
+}
+
+void *gpv_context_stream(gpv_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+static int image_alloc(gpv_context *ctx, int64_t h, int64_t w, int32_t border, uint32_t flags, int32_t dtype,
+                       gpv_image **out) {
+    if (!ctx || !out) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    *out = nullptr;
+    if (h < 1 || w < 1 || border < 3) { set_error("image needs h, w >= 1 and border >= 3"); return GPV_ERR_INVALID; }
+    if (h + 2 * border > (1 << 30) || w + 2 * border > (1 << 30)) { set_error("image too large"); return GPV_ERR_INVALID; }
+    if (!dtype_size(dtype)) { set_error("unknown pixel dtype"); return GPV_ERR_INVALID; }
+    auto *img = new gpv_image();
+    img->ctx = ctx;
+    img->h = h;
+    img->w = w;
+    img->border = border;
+    img->ch = h + 2 * border;
+    img->cw = w + 2 * border;
+    img->pitch32 = (img->cw + 31) / 32 * 32;
+    img->pitch64 = (img->cw + 15) / 16 * 16;
+    img->flags = flags;
+    cudaError_t e = cudaMalloc(&img->c32, sizeof(float) * img->pitch32 * img->ch);
+    if (e == cudaSuccess && (flags & GPV_IMAGE_KEEP_F64)) e = cudaMalloc(&img->c64, sizeof(double) * img->pitch64 * img->ch);
+    if (e == cudaSuccess) e = cudaMalloc(&img->rowpass, sizeof(double) * (img->h * img->cw + 2 * 89 + 8));
+    if (e != cudaSuccess) {
+        set_error(std::string("image allocation: ") + cudaGetErrorString(e));
+        cudaFree(img->c32);
+        cudaFree(img->c64);
+        cudaFree(img->rowpass);
+        delete img;
+        return GPV_ERR_NOMEM;
+    }
+    *out = img;
+    return GPV_SUCCESS;
+}
+
+int gpv_image_create(gpv_context *ctx, const void *px, int32_t dtype, int64_t h, int64_t w, int32_t border,
+                     uint32_t flags, gpv_image **out) {
+    if (!px) { set_error("px is NULL"); return GPV_ERR_INVALID; }
+    if (!ctx) { set_error("ctx is NULL"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(ctx->device);
+    int rc = image_alloc(ctx, h, w, border, flags, dtype, out);
+    if (rc) return rc;
+    gpv_image *img = *out;
+    img->px_bytes = dtype_size(dtype) * h * w;
+    cudaError_t e = cudaMalloc(&img->px_dev, img->px_bytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(img->px_dev, px, img->px_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+        set_error(std::string("pixel upload: ") + cudaGetErrorString(e));
+        gpv_image_destroy(img);
+        *out = nullptr;
+        return GPV_ERR_CUDA;
+    }
+    rc = prefilter_launch(img, img->px_dev, dtype, ctx->stream);
+    if (rc == GPV_SUCCESS) {
+        e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) { set_error(std::string("prefilter: ") + cudaGetErrorString(e)); rc = GPV_ERR_CUDA; }
+    }
+    if (rc) { gpv_image_destroy(img); *out = nullptr; }
+    return rc;
+}
+
+int gpv_image_create_device(gpv_context *ctx, const void *px_dev, int32_t dtype, int64_t h, int64_t w, int32_t border,
+                            uint32_t flags, gpv_image **out) {
+    if (!px_dev || !ctx) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(ctx->device);
+    int rc = image_alloc(ctx, h, w, border, flags, dtype, out);
+    if (rc) return rc;
+    rc = prefilter_launch(*out, px_dev, dtype, ctx->stream);
+    if (rc) { gpv_image_destroy(*out); *out = nullptr; }
+    return rc;
+}
+
+int gpv_image_update_device(gpv_image *img, const void *px_dev, int32_t dtype) {
+    if (!img || !px_dev) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(img->ctx->device);
+    return prefilter_launch(img, px_dev, dtype, img->ctx->stream);
+}
+
+int gpv_image_update(gpv_image *img, const void *px, int32_t dtype) {
+    if (!img || !px) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    const size_t bytes = dtype_size(dtype) * img->h * img->w;
+    if (!bytes) { set_error("unknown pixel dtype"); return GPV_ERR_INVALID; }
+    gpv_context *ctx = img->ctx;
+    DeviceGuard dg(ctx->device);
+    if (bytes > img->px_bytes) {
+        cudaFree(img->px_dev);
+        img->px_dev = nullptr;
+        img->px_bytes = 0;
+        GPV_CUDA_TRY(cudaMalloc(&img->px_dev, bytes));
+        img->px_bytes = bytes;
+    }
+    GPV_CUDA_TRY(cudaMemcpyAsync(img->px_dev, px, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    if (int rc = prefilter_launch(img, img->px_dev, dtype, ctx->stream)) return rc;
+    GPV_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GPV_SUCCESS;
+}
+
+int gpv_image_destroy(gpv_image *img) {
+    if (!img) return GPV_SUCCESS;
+    DeviceGuard dg(img->ctx->device);
+    cudaStreamSynchronize(img->ctx->stream);
+    cudaFree(img->c32);
+    cudaFree(img->c64);
+    cudaFree(img->rowpass);
+    cudaFree(img->px_dev);
+    delete img;
+    return GPV_SUCCESS;
+}
+
+int gpv_image_shape(const gpv_image *img, int64_t *h, int64_t *w, int32_t *border) {
+    if (!img) { set_error("img is NULL"); return GPV_ERR_INVALID; }
+    if (h) *h = img->h;
+    if (w) *w = img->w;
+    if (border) *border = img->border;
+    return GPV_SUCCESS;
+}
+
+int gpv_image_coefficients_f32(const gpv_image *img, float *out) {
+    if (!img || !out) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(img->ctx->device);
+    GPV_CUDA_TRY(cudaStreamSynchronize(img->ctx->stream));
+    GPV_CUDA_TRY(cudaMemcpy2D(out, sizeof(float) * img->cw, img->c32, sizeof(float) * img->pitch32,
+                              sizeof(float) * img->cw, img->ch, cudaMemcpyDeviceToHost));
+    return GPV_SUCCESS;
+}
+
+int gpv_image_coefficients_f64(const gpv_image *img, double *out) {
+    if (!img || !out) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    if (!img->c64) { set_error("image was created without GPV_IMAGE_KEEP_F64"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(img->ctx->device);
+    GPV_CUDA_TRY(cudaStreamSynchronize(img->ctx->stream));
+    GPV_CUDA_TRY(cudaMemcpy2D(out, sizeof(double) * img->cw, img->c64, sizeof(double) * img->pitch64,
+                              sizeof(double) * img->cw, img->ch, cudaMemcpyDeviceToHost));
+    return GPV_SUCCESS;
+}
+
+int gpv_image_eval(const gpv_image *img, const double *xy, int64_t n, int32_t precision, double *val, double *grad) {
+    if (!img || (!xy && n) || (!val && n)) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    if (n < 0) { set_error("n < 0"); return GPV_ERR_INVALID; }
+    if (n == 0) return GPV_SUCCESS;
+    gpv_context *ctx = img->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    if (int rc = ctx->eval_dev.ensure(sizeof(double) * 5 * n)) return rc;
+    double *dxy = static_cast<double *>(ctx->eval_dev.ptr), *dout = dxy + 2 * n;
+    GPV_CUDA_TRY(cudaMemcpyAsync(dxy, xy, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, ctx->stream));
+    if (int rc = eval_launch(img, dxy, n, precision, dout, ctx->stream)) return rc;
+    std::vector<double> h(3 * n);
+    GPV_CUDA_TRY(cudaMemcpyAsync(h.data(), dout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+    GPV_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int64_t i = 0; i < n; i++) {
+        val[i] = h[3 * i];
+        if (grad) {
+            grad[2 * i] = h[3 * i + 1];
+            grad[2 * i + 1] = h[3 * i + 2];
+        }
+    }
+    return GPV_SUCCESS;
+}
+
+int gpv_mask_create(gpv_context *ctx, const uint8_t *mask, int64_t h, int64_t w, gpv_mask **out) {
+    if (!ctx || !mask || !out || h < 1 || w < 1) { set_error("invalid mask arguments"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(ctx->device);
+    auto *m = new gpv_mask();
+    m->ctx = ctx;
+    m->h = h;
+    m->w = w;
+    cudaError_t e = cudaMalloc(&m->dev, (size_t)h * w);
+    if (e == cudaSuccess) e = cudaMemcpy(m->dev, mask, (size_t)h * w, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        set_error(std::string("mask upload: ") + cudaGetErrorString(e));
+        cudaFree(m->dev);
+        delete m;
+        return GPV_ERR_CUDA;
+    }
+    *out = m;
+    return GPV_SUCCESS;
+}
+
+int gpv_mask_destroy(gpv_mask *m) {
+    if (!m) return GPV_SUCCESS;
+    DeviceGuard dg(m->ctx->device);
+    cudaFree(m->dev);
+    delete m;
+    return GPV_SUCCESS;
+}
+
+int gpv_context_reserve(gpv_context *ctx, int64_t n_subsets, int32_t max_radius, int32_t max_iterations) {
+    if (!ctx || n_subsets < 0 || max_radius < 1) { set_error("invalid reserve arguments"); return GPV_ERR_INVALID; }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    if (int rc = ensure_tables(ctx, max_radius)) return rc;
+    const int64_t npx = ctx->h_tab_n[max_radius];
+    const int64_t stride = 4 * ((npx + 31) / 32 * 32);
+    // enough for either kernel: 8 B per element, one slot per resident warp
+    const size_t need = (size_t)ctx->num_sms * 64 * stride * sizeof(double);
+    if (int rc = ctx->scratch.ensure(need)) return rc;
+    if (int rc = ctx->queue.ensure(64)) return rc;
+    if (int rc = ctx->desc_dev.ensure(sizeof(gpv_subset_desc) * (size_t)n_subsets)) return rc;
+    if (int rc = ctx->out_dev.ensure(sizeof(gpv_subset_result) * (size_t)n_subsets)) return rc;
+    if (int rc = ctx->order_dev.ensure(sizeof(int32_t) * (size_t)n_subsets)) return rc;
+    (void)max_iterations;
+    return GPV_SUCCESS;
+}
+
+static int check_pair(const gpv_image *f, const gpv_image *g, const gpv_solve_params *prm) {
+    if (!f || !g || !prm) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    if (f->h != g->h || f->w != g->w || f->border != g->border) {
+        set_error("reference and target images must have the same shape and border");
+        return GPV_ERR_INVALID;
+    }
+    if (f->ctx != g->ctx) { set_error("images belong to different contexts"); return GPV_ERR_INVALID; }
+    if (prm->max_iterations < 0) { set_error("max_iterations < 0"); return GPV_ERR_INVALID; }
+    if (prm->precision != GPV_PREC_MIXED && prm->precision != GPV_PREC_FP64) {
+        set_error("unknown precision");
+        return GPV_ERR_INVALID;
+    }
+    if (prm->precision == GPV_PREC_FP64 && (!f->c64 || !g->c64)) {
+        set_error("GPV_PREC_FP64 needs images created with GPV_IMAGE_KEEP_F64");
+        return GPV_ERR_INVALID;
+    }
+    if (!(prm->max_norm >= 0.0)) { set_error("max_norm must be >= 0"); return GPV_ERR_INVALID; }
+    return GPV_SUCCESS;
+}
+
+int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc, int64_t n,
+                    const gpv_solve_params *prm, gpv_subset_result *out) {
+    if (!ctx) { set_error("ctx is NULL"); return GPV_ERR_INVALID; }
+    if (int rc = check_pair(f, g, prm)) return rc;
+    if (n < 0 || (n > 0 && (!desc || !out))) { set_error("invalid batch arrays"); return GPV_ERR_INVALID; }
+    if (n > INT32_MAX) { set_error("batch too large"); return GPV_ERR_INVALID; }
+    if (n == 0) return GPV_SUCCESS;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    int max_r = 1;
+    for (int64_t i = 0; i < n; i++)
+        if (desc[i].radius > max_r && desc[i].radius <= 4000) max_r = desc[i].radius;
+    if (int rc = ensure_tables(ctx, max_r)) return rc;
+    // largest subsets first (longest-processing-time order for the work queue)
+    // bucket key = 3 * radius + min(order, 2): larger radius first, order 2 before 1 before 0
+    std::vector<int32_t> order(n);
+    {
+        const int nk = 3 * (max_r + 1);
+        std::vector<int64_t> start(nk + 1, 0);
+        auto key = [&](int64_t i) -> int {
+            const int r = desc[i].radius, o = desc[i].order;
+            if (r < 1 || r > max_r || o < 0 || o > 2) return 0;
+            return nk - 1 - (3 * r + o);
+        };
+        for (int64_t i = 0; i < n; i++) start[key(i) + 1]++;
+        for (int k = 0; k < nk; k++) start[k + 1] += start[k];
+        for (int64_t i = 0; i < n; i++) order[start[key(i)]++] = (int32_t)i;
+    }
+    if (int rc = ctx->desc_dev.ensure(sizeof(gpv_subset_desc) * n)) return rc;
+    if (int rc = ctx->out_dev.ensure(sizeof(gpv_subset_result) * n)) return rc;
+    if (int rc = ctx->order_dev.ensure(sizeof(int32_t) * n)) return rc;
+    double *hist_dev = nullptr;
+    const size_t hist_bytes = sizeof(double) * 3 * (size_t)n * (size_t)(prm->max_iterations > 0 ? prm->max_iterations : 1);
+    if (prm->history) {
+        if (int rc = ctx->hist_dev.ensure(hist_bytes)) return rc;
+        hist_dev = static_cast<double *>(ctx->hist_dev.ptr);
+        GPV_CUDA_TRY(cudaMemsetAsync(hist_dev, 0, hist_bytes, ctx->stream));
+    }
+    GPV_CUDA_TRY(cudaMemcpyAsync(ctx->desc_dev.ptr, desc, sizeof(gpv_subset_desc) * n, cudaMemcpyHostToDevice, ctx->stream));
+    GPV_CUDA_TRY(cudaMemcpyAsync(ctx->order_dev.ptr, order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    SolveLaunch L;
+    L.f = f;
+    L.g = g;
+    L.desc = static_cast<const gpv_subset_desc *>(ctx->desc_dev.ptr);
+    L.order = static_cast<const int32_t *>(ctx->order_dev.ptr);
+    L.n = n;
+    L.prm = prm;
+    L.mask = prm->mask ? prm->mask->dev : nullptr;
+    L.mh = prm->mask ? prm->mask->h : 0;
+    L.mw = prm->mask ? prm->mask->w : 0;
+    L.out = static_cast<gpv_subset_result *>(ctx->out_dev.ptr);
+    L.history = hist_dev;
+    L.max_radius = max_r;
+    if (int rc = solve_launch(ctx, L, ctx->stream)) return rc;
+    GPV_CUDA_TRY(cudaMemcpyAsync(out, ctx->out_dev.ptr, sizeof(gpv_subset_result) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    if (prm->history) {
+        GPV_CUDA_TRY(cudaMemcpyAsync(prm->history, hist_dev, hist_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    GPV_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GPV_SUCCESS;
+}
+
+int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
+                           const int32_t *work_order_dev, int64_t n, const gpv_solve_params *prm,
+                           gpv_subset_result *out_dev, void *stream) {
+    if (!ctx) { set_error("ctx is NULL"); return GPV_ERR_INVALID; }
+    if (int rc = check_pair(f, g, prm)) return rc;
+    if (n < 0 || (n > 0 && (!desc_dev || !out_dev))) { set_error("invalid batch arrays"); return GPV_ERR_INVALID; }
+    if (n > INT32_MAX) { set_error("batch too large"); return GPV_ERR_INVALID; }
+    if (n == 0) return GPV_SUCCESS;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    if (ctx->table_radius < 1) {
+        set_error("call gpv_context_reserve first (it fixes the largest radius the device path accepts)");
+        return GPV_ERR_INVALID;
+    }
+    SolveLaunch L;
+    L.f = f;
+    L.g = g;
+    L.desc = desc_dev;
+    L.order = work_order_dev;
+    L.n = n;
+    L.prm = prm;
+    L.mask = prm->mask ? prm->mask->dev : nullptr;
+    L.mh = prm->mask ? prm->mask->h : 0;
+    L.mw = prm->mask ? prm->mask->w : 0;
+    L.out = out_dev;
+    L.history = prm->history;
+    L.max_radius = ctx->table_radius;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    return solve_launch(ctx, L, s);
+}
+
+int gpv_probe_fp32_peak(gpv_context *ctx, double *tflops) {
+    if (!ctx || !tflops) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    return probe_fp32_peak(ctx, tflops);
+}
+
+}  // extern "C"

@@ -1,0 +1,1238 @@
+// icgn.cu -- batched inverse-compositional Gauss-Newton subset solves.
+//
+// Reference: Subset::new (src/subset.rs:836-919) and solve_icgn_result
+// (src/subset.rs:1117-1219) with apply_warp_into (:262-300),
+// steepest_descent (:311-343), compute_hessian (:348-364),
+// delta_p_and_znssd_icgn (:418-446), compose_icgn (:487-611),
+// convergence_norm (:622-649) and omitted_mode_diagnostic (:698-820).
+//
+// Two kernels:
+//  * icgn_mixed  -- one warp per subset, persistent (warps take subsets from
+//    an atomic work queue, largest first).  Interpolation, warping and
+//    residuals in FP32 on FP32 coefficients; the mean / norm sums are
+//    FP32 partials over 8 pixels per lane carried in FP64, and every sum is
+//    combined across lanes in FP64; the Hessian is
+//    assembled in FP64 from gradient moments, Jacobi-scaled and inverted by
+//    a lane-parallel Gauss-Jordan; warp composition is FP64.  The ICGN update
+//    is evaluated in a single pass per iteration through the identities
+//        sum (f-f_m)(g-g_m)       = sum (f-f_m) g~ - g~_m sum (f-f_m)
+//        grad_j                   = A_j - (df/dg) (B_j - g~_m S_j)
+//        ZNSSD                    = 2 - 2 sum(f-f_m)(g-g_m) / (df dg)
+//    with g~ = g - f_m, A_j = sum SDI_ij (f_i - f_m), S_j = sum SDI_ij and
+//    B_j = sum SDI_ij g~_i.
+//  * icgn_fp64   -- the plain form: one thread block per subset, FP64
+//    throughout on FP64 coefficients, and the reference's three sweeps per
+//    iteration (g_m, then delta_g, then the fused update + ZNSSD).
+#include <cfloat>
+#include <cmath>
+
+#include "internal.h"
+#include "spline.cuh"
+
+namespace gpv {
+namespace {
+
+constexpr int kMixedWarps = 8;  // warps per block of the mixed kernel
+constexpr int kChunk = 8;       // pixels per lane between FP64 flushes
+constexpr int kFp64Threads = 256;
+constexpr int kFp64Warps = kFp64Threads / 32;
+
+struct KArgs {
+    const float *f32, *g32;
+    const double *f64, *g64;
+    int64_t pitch32, pitch64;
+    int h, w, border;
+    const gpv_subset_desc *desc;
+    const int32_t *order;
+    int n;
+    const short2 *offs;
+    const int32_t *tab_off, *tab_n;
+    int max_radius;
+    const uint8_t *mask;
+    int mh, mw;
+    double max_norm, tolerance;
+    int max_iter, flags;
+    gpv_subset_result *out;
+    double *history;
+    void *scratch;
+    int64_t scratch_stride;  // elements (float for mixed, double for fp64) per worker
+    int *queue;
+};
+
+template <int ORDER>
+struct Ord {
+    static constexpr int M = ORDER == 0 ? 2 : (ORDER == 1 ? 6 : 12);  // parameters
+    static constexpr int NMU = M / 2;                                 // SDI monomials per gradient axis
+    static constexpr int DEG = ORDER;                                 // degree of the warp monomials
+    static constexpr int NMOM = (2 * DEG + 1) * (2 * DEG + 2) / 2;    // monomials of degree <= 2*DEG
+};
+
+// SDI monomial mu (src/subset.rs:324-340): 1, dx, dy, dx^2/2, dx dy, dy^2/2
+__host__ __device__ constexpr int mu_a(int mu) { return mu == 1 ? 1 : (mu == 3 ? 2 : (mu == 4 ? 1 : 0)); }
+__host__ __device__ constexpr int mu_b(int mu) { return mu == 2 ? 1 : (mu == 4 ? 1 : (mu == 5 ? 2 : 0)); }
+__host__ __device__ constexpr double mu_c(int mu) { return (mu == 3 || mu == 5) ? 0.5 : 1.0; }
+// index of monomial dx^a dy^b among those of degree <= D, ordered by degree then b
+__host__ __device__ constexpr int mom_idx(int a, int b) { return (a + b) * (a + b + 1) / 2 + b; }
+
+template <typename T>
+__device__ __forceinline__ T mu_val(int mu, T dx, T dy) {
+    switch (mu) {
+        case 0: return T(1);
+        case 1: return dx;
+        case 2: return dy;
+        case 3: return T(0.5) * dx * dx;
+        case 4: return dx * dy;
+        default: return T(0.5) * dy * dy;
+    }
+}
+
+// Global-mask test of LocalMask::mask_update (src/masks.rs:199-263): the
+// template pixel maps to image pixel trunc(centre) + offset; the extracted
+// window always stops one short of the last mask row / column.
+__device__ __forceinline__ bool mask_ok(const KArgs &A, int cxi, int cyi, int ox, int oy) {
+    if (!A.mask) return true;
+    const int X = cxi + ox, Y = cyi + oy;
+    if (X < 0 || Y < 0 || X > A.mw - 2 || Y > A.mh - 2) return false;
+    return A.mask[(int64_t)Y * A.mw + X] != 0;
+}
+
+// ---------------------------------------------------------------------
+// Warp composition (compose_icgn, src/subset.rs:487-611) in FP64.
+// Order 2 needs only rows 3 and 4 of W_old * W_delta^-1 (the u and v rows
+// that hold the 12 parameters); they are the solution Y of Y W_delta = R,
+// R = rows 3, 4 of W_old.  Returns false if W_delta is singular.
+// ---------------------------------------------------------------------
+__device__ bool compose1(const double *p, const double *d, double *out) {
+    const double a = 1.0 + d[2], b = d[4], c = d[3], e = 1.0 + d[5];
+    const double det = a * e - b * c;
+    if (det == 0.0 || !isfinite(det)) return false;
+    const double ia = e / det, ib = -b / det, ic = -c / det, ie = a / det;
+    // W_delta^-1 = [[ia, ib, -(ia du + ib dv)], [ic, ie, -(ic du + ie dv)], [0, 0, 1]]
+    const double tx = -(ia * d[0] + ib * d[1]), ty = -(ic * d[0] + ie * d[1]);
+    const double B00 = 1.0 + p[2], B01 = p[4], B10 = p[3], B11 = 1.0 + p[5];
+    const double n00 = B00 * ia + B01 * ic, n01 = B00 * ib + B01 * ie;
+    const double n10 = B10 * ia + B11 * ic, n11 = B10 * ib + B11 * ie;
+    out[0] = B00 * tx + B01 * ty + p[0];
+    out[1] = B10 * tx + B11 * ty + p[1];
+    out[2] = n00 - 1.0;
+    out[3] = n10;
+    out[4] = n01;
+    out[5] = n11 - 1.0;
+    return true;
+}
+
+// Lifted 6x6 warp of an order-2 parameter vector on [x^2, xy, y^2, x, y, 1]
+// (src/subset.rs:547-593); W is row-major 36 doubles.
+__device__ void lifted(const double *q, double *W) {
+    const double u = q[0], v = q[1], ux = q[2], vx = q[3], uy = q[4], vy = q[5];
+    const double uxx = q[6], vxx = q[7], uxy = q[8], vxy = q[9], uyy = q[10], vyy = q[11];
+    W[0] = 1.0 + 2.0 * ux + ux * ux + u * uxx;
+    W[1] = 2.0 * u * uxy + 2.0 * (1.0 + ux) * uy;
+    W[2] = uy * uy + u * uyy;
+    W[3] = 2.0 * u * (1.0 + ux);
+    W[4] = 2.0 * u * uy;
+    W[5] = u * u;
+    W[6] = 0.5 * (v * uxx + 2.0 * (1.0 + ux) * vx + u * vxx);
+    W[7] = 1.0 + uy * vx + ux * vy + v * uxy + u * vxy + vy + ux;
+    W[8] = 0.5 * (v * uyy + 2.0 * uy * (1.0 + vy) + u * vyy);
+    W[9] = v + v * ux + u * vx;
+    W[10] = u + v * uy + u * vy;
+    W[11] = u * v;
+    W[12] = vx * vx + v * vxx;
+    W[13] = 2.0 * v * vxy + 2.0 * vx * (1.0 + vy);
+    W[14] = 1.0 + 2.0 * vy + vy * vy + v * vyy;
+    W[15] = 2.0 * v * vx;
+    W[16] = 2.0 * v * (1.0 + vy);
+    W[17] = v * v;
+    W[18] = 0.5 * uxx; W[19] = uxy; W[20] = 0.5 * uyy; W[21] = 1.0 + ux; W[22] = uy; W[23] = u;
+    W[24] = 0.5 * vxx; W[25] = vxy; W[26] = 0.5 * vyy; W[27] = vx; W[28] = 1.0 + vy; W[29] = v;
+    W[30] = 0.0; W[31] = 0.0; W[32] = 0.0; W[33] = 0.0; W[34] = 0.0; W[35] = 1.0;
+}
+
+// Order-2 composition by one thread; LU with partial pivoting of W_delta^T.
+// ws: 96 doubles of scratch (shared or local memory).
+__device__ __noinline__ bool compose2(const double *p, const double *d, double *out, double *ws) {
+    double *A = ws, *X = ws + 36, *W = ws + 48;  // A = W_delta^T, X = [R^T] (6x2), W: scratch 6x6
+    lifted(d, W);
+    for (int i = 0; i < 6; i++)
+        for (int j = 0; j < 6; j++) A[i * 6 + j] = W[j * 6 + i];
+    // R = rows 3, 4 of W_old: [0.5 uxx, uxy, 0.5 uyy, 1+ux, uy, u] and the v row
+    X[0] = 0.5 * p[6]; X[1] = 0.5 * p[7];
+    X[2] = p[8];       X[3] = p[9];
+    X[4] = 0.5 * p[10]; X[5] = 0.5 * p[11];
+    X[6] = 1.0 + p[2]; X[7] = p[3];
+    X[8] = p[4];       X[9] = 1.0 + p[5];
+    X[10] = p[0];      X[11] = p[1];
+    for (int k = 0; k < 6; k++) {
+        int piv = k;
+        double best = fabs(A[k * 6 + k]);
+        for (int i = k + 1; i < 6; i++)
+            if (fabs(A[i * 6 + k]) > best) { best = fabs(A[i * 6 + k]); piv = i; }
+        if (!(best > 0.0) || !isfinite(best)) return false;
+        if (piv != k) {
+            for (int j = 0; j < 6; j++) { double t = A[k * 6 + j]; A[k * 6 + j] = A[piv * 6 + j]; A[piv * 6 + j] = t; }
+            for (int j = 0; j < 2; j++) { double t = X[k * 2 + j]; X[k * 2 + j] = X[piv * 2 + j]; X[piv * 2 + j] = t; }
+        }
+        const double inv = 1.0 / A[k * 6 + k];
+        for (int i = k + 1; i < 6; i++) {
+            const double f = A[i * 6 + k] * inv;
+            if (f == 0.0) continue;
+            for (int j = k; j < 6; j++) A[i * 6 + j] -= f * A[k * 6 + j];
+            X[i * 2] -= f * X[k * 2];
+            X[i * 2 + 1] -= f * X[k * 2 + 1];
+        }
+    }
+    for (int k = 5; k >= 0; k--) {
+        for (int j = k + 1; j < 6; j++) {
+            X[k * 2] -= A[k * 6 + j] * X[j * 2];
+            X[k * 2 + 1] -= A[k * 6 + j] * X[j * 2 + 1];
+        }
+        X[k * 2] /= A[k * 6 + k];
+        X[k * 2 + 1] /= A[k * 6 + k];
+    }
+    // row 3 of W_new = X[:, 0], row 4 = X[:, 1]
+    out[0] = X[10]; out[1] = X[11];
+    out[2] = X[6] - 1.0; out[3] = X[7];
+    out[4] = X[8]; out[5] = X[9] - 1.0;
+    out[6] = 2.0 * X[0]; out[7] = 2.0 * X[1];
+    out[8] = X[2]; out[9] = X[3];
+    out[10] = 2.0 * X[4]; out[11] = 2.0 * X[5];
+    return true;
+}
+
+template <int M>
+__device__ double conv_norm(const double *dp, double size) {
+    if (M == 2) return sqrt(dp[0] * dp[0] + dp[1] * dp[1]);
+    double s = dp[0] * dp[0] + dp[1] * dp[1];
+#pragma unroll
+    for (int k = 2; k < 6; k++) s += (dp[k] * size) * (dp[k] * size);
+    if (M == 12) {
+#pragma unroll
+        for (int k = 6; k < 12; k++) {
+            const double t = 0.5 * dp[k] * size * size;
+            s += t * t;
+        }
+    }
+    return sqrt(s);
+}
+
+// Lane-parallel Gauss-Jordan inverse of the Jacobi-scaled SPD Hessian, in
+// shared memory (lane c owns column c of the augmented [H~ | I]).
+// H: M*M (in), aug: M*2M scratch, Hinv: M*M (out).  Returns false when a
+// pivot is not positive (singular Hessian).  Warp-uniform result.
+template <int M>
+__device__ bool spd_inverse_warp(const double *H, double *aug, double *Hinv, int lane) {
+    constexpr int W2 = 2 * M;
+    bool ok = true;
+    for (int i = 0; i < M; i++) ok = ok && (H[i * M + i] > 0.0) && isfinite(H[i * M + i]);
+    if (!ok) return false;
+    for (int e = lane; e < M * W2; e += 32) {
+        const int i = e / W2, c = e % W2;
+        aug[e] = c < M ? H[i * M + c] / sqrt(H[i * M + i] * H[c * M + c]) : (c - M == i ? 1.0 : 0.0);
+    }
+    __syncwarp();
+    for (int k = 0; k < M; k++) {
+        const double piv = aug[k * W2 + k];
+        if (!(piv > 0.0) || !isfinite(piv)) return false;  // uniform (same smem value)
+        const int c = lane;
+        double rk = 0.0;
+        if (c < W2) rk = aug[k * W2 + c] / piv;
+        if (c < W2 && c != k) {
+            for (int i = 0; i < M; i++)
+                if (i != k) aug[i * W2 + c] = fma(-aug[i * W2 + k], rk, aug[i * W2 + c]);
+        }
+        __syncwarp();
+        if (c < W2) aug[k * W2 + c] = rk;
+        if (c == k)
+            for (int i = 0; i < M; i++)
+                if (i != k) aug[i * W2 + k] = 0.0;
+        __syncwarp();
+    }
+    for (int e = lane; e < M * M; e += 32) {
+        const int i = e / M, c = e % M;
+        Hinv[e] = aug[i * W2 + M + c] / sqrt(H[i * M + i] * H[c * M + c]);
+    }
+    __syncwarp();
+    return true;
+}
+
+// Assemble H (M x M) from gradient moments mom[pair][NMOM] (pair 0 = gx gx,
+// 1 = gx gy, 2 = gy gy): H[j][k] = c_j c_k sum g_cj g_ck mu_j mu_k.
+template <int ORDER>
+__device__ void assemble_hessian(const double *mom, double *H, int lane) {
+    using O = Ord<ORDER>;
+    for (int e = lane; e < O::M * O::M; e += 32) {
+        const int j = e / O::M, k = e % O::M;
+        const int cj = j & 1, ck = k & 1, mj = j >> 1, mk = k >> 1;
+        const int pair = cj + ck;  // 0 xx, 1 xy, 2 yy
+        const int a = mu_a(mj) + mu_a(mk), b = mu_b(mj) + mu_b(mk);
+        H[e] = mu_c(mj) * mu_c(mk) * mom[pair * O::NMOM + mom_idx(a, b)];
+    }
+    __syncwarp();
+}
+
+struct WarpSmem {
+    double mom[3 * 15];
+    double H[144];
+    double Hinv[144];
+    double aug[288];
+    double A[12], S[12];
+    double p[12], pprev[12], dp[12], grad[12];
+    double red[16];   // reduced sums of the current iteration
+    double misc[8];
+    int flag[4];
+};
+
+__device__ __forceinline__ void write_history(const KArgs &A, int idx, int it, double nrm, double zncc, double znssd) {
+    if (A.history) {
+        double *h = A.history + ((int64_t)idx * A.max_iter + (it - 1)) * 3;
+        h[0] = nrm;
+        h[1] = zncc;
+        h[2] = znssd;
+    }
+}
+
+__device__ void write_failed(const KArgs &A, int idx, const gpv_subset_desc &d, int m, int status, int npx, double fm,
+                             double df) {
+    gpv_subset_result *o = A.out + idx;
+#pragma unroll
+    for (int k = 0; k < 12; k++) o->p[k] = k < m ? d.p0[k] : 0.0;
+    o->c_zncc = 0.0;
+    o->c_znssd = 4.0;
+    o->norm = 0.0;
+    o->eta_u = 0.0;
+    o->eta_v = 0.0;
+    o->f_m = fm;
+    o->delta_f = df;
+    o->sssig = 0.0;
+    o->sigma = 0.0;
+    o->iterations = 0;
+    o->converged = 0;
+    o->quality_ok = 0;
+    o->status = status;
+    o->n_px = npx;
+    o->has_eta = 0;
+}
+
+// Omitted-mode diagnostic from per-pixel (f, gx, gy, g) held by a worker;
+// all sums FP64.  `reduce` is a functor summing a double over the worker.
+// Returns eta_u, eta_v (src/subset.rs:698-820).
+template <int ORDER, typename Reduce, typename Load>
+__device__ void eta_sums(int npx, int tid, int nthr, double n, double fm, double df, double gm, double dg, Load load,
+                         Reduce reduce, double &eu, double &ev) {
+    constexpr int K = ORDER + 2;
+    double se = 0, sx = 0, sxx = 0, sy = 0, syy = 0;
+    for (int i = tid; i < npx; i += nthr) {
+        double f, gx, gy, g, dx, dy;
+        if (!load(i, f, gx, gy, g, dx, dy)) continue;
+        const double e = (f - fm) / df - (g - gm) / dg;
+        se += e;
+        sx += gx; sxx += gx * gx;
+        sy += gy; syy += gy * gy;
+    }
+    se = reduce(se); sx = reduce(sx); sxx = reduce(sxx); sy = reduce(sy); syy = reduce(syy);
+    const double eb = se / n;
+    const double mx = sx / n, my = sy / n;
+    double vx = sxx / n - mx * mx, vy = syy / n - my * my;
+    const double sdx = sqrt(vx > 1e-18 ? vx : 1e-18), sdy = sqrt(vy > 1e-18 ? vy : 1e-18);
+    // one pass per (component, mode): three live accumulators
+    double eta[2];
+#pragma unroll 1
+    for (int c = 0; c < 2; c++) {
+        double ss = 0.0;
+#pragma unroll 1
+        for (int k = 0; k < K; k++) {
+            double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+            for (int i = tid; i < npx; i += nthr) {
+                double f, gx, gy, g, dx, dy;
+                if (!load(i, f, gx, gy, g, dx, dy)) continue;
+                const double e = (f - fm) / df - (g - gm) / dg;
+                const double z = c == 0 ? (gx - mx) / sdx : (gy - my) / sdy;
+                double md;
+                if (ORDER == 0) md = k == 0 ? dx : dy;
+                else if (ORDER == 1) md = k == 0 ? dx * dx : (k == 1 ? dx * dy : dy * dy);
+                else md = k == 0 ? dx * dx * dx : (k == 1 ? dx * dx * dy : (k == 2 ? dx * dy * dy : dy * dy * dy));
+                const double raw = z * md;
+                a1 += raw;
+                a2 += raw * raw;
+                a3 += raw * e;
+            }
+            a1 = reduce(a1);
+            a2 = reduce(a2);
+            a3 = reduce(a3);
+            const double mean = a1 / n;
+            const double var = a2 / n - mean * mean;
+            const double sd = sqrt(var > 1e-18 ? var : 1e-18);
+            const double pr = (a3 - eb * a1) / (sd * n);
+            ss += pr * pr;
+        }
+        eta[c] = sqrt(ss);
+    }
+    eu = eta[0];
+    ev = eta[1];
+}
+
+// =====================================================================
+// Mixed-precision warp-per-subset solve
+// =====================================================================
+template <int ORDER>
+__device__ void mixed_subset(const KArgs &A, int idx, const gpv_subset_desc &d, float *S, int64_t nmax, WarpSmem &sm,
+                             int lane) {
+    using O = Ord<ORDER>;
+    constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM;
+    const int r = d.radius;
+    const int npx_t = A.tab_n[r];
+    const short2 *po = A.offs + A.tab_off[r];
+    float *Sf = S, *Sgx = S + nmax, *Sgy = S + 2 * nmax, *Sg = S + 3 * nmax;
+    const double cx = d.coord[0], cy = d.coord[1];
+    const int cxi = (int)cx, cyi = (int)cy;  // `as isize` (truncation) for the mask window
+    const double fxd = floor(cx), fyd = floor(cy);
+    const int bx = (int)fxd, by = (int)fyd;
+    const float fx = (float)(cx - fxd), fy = (float)(cy - fyd);
+    const float *F = A.f32 + (int64_t)(A.border - 2) * A.pitch32 + (A.border - 2);
+    const float *G = A.g32 + (int64_t)(A.border - 2) * A.pitch32 + (A.border - 2);
+
+    // ---- setup pass 1: f, grad f, sum f, SSSIG ------------------------------
+    double sum_f = 0.0, sssig = 0.0;
+    int cnt = 0;
+    for (int i = lane; i < npx_t; i += 32) {
+        const short2 o = po[i];
+        if (!mask_ok(A, cxi, cyi, o.x, o.y)) {
+            Sf[i] = __int_as_float(0x7fc00000);  // NaN marks a masked pixel
+            continue;
+        }
+        int ix, iy;
+        float tx, ty;
+        split_clamped(bx, fx + (float)o.x, A.w, ix, tx);
+        split_clamped(by, fy + (float)o.y, A.h, iy, ty);
+        float a[6], da[6], b[6], db[6];
+        basis(ty, a); dbasis(ty, da);
+        basis(tx, b); dbasis(tx, db);
+        float gx, gy;
+        const float f = contract_grad<float>(F + (int64_t)iy * A.pitch32 + ix, A.pitch32, a, da, b, db, gx, gy);
+        Sf[i] = f; Sgx[i] = gx; Sgy[i] = gy;
+        sum_f += (double)f;
+        sssig += 0.5 * ((double)gx * gx + (double)gy * gy);
+        cnt++;
+    }
+    __syncwarp();
+    const int n = warp_sum_int(cnt);
+    sum_f = warp_sum(sum_f);
+    sssig = warp_sum(sssig);
+    // ---- setup pass 1b: gradient moments for the Hessian (FP32 per lane) ----
+    {
+        float mom[3][NMOM];
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < NMOM; q++) mom[p][q] = 0.f;
+        for (int i = lane; i < npx_t; i += 32) {
+            if (Sf[i] != Sf[i]) continue;
+            const short2 o = po[i];
+            const float gx = Sgx[i], gy = Sgy[i];
+            const float dx = (float)o.x, dy = (float)o.y;
+            float pxp[2 * 2 + 1], pyp[2 * 2 + 1];
+            pxp[0] = 1.f; pyp[0] = 1.f;
+#pragma unroll
+            for (int e = 1; e <= 2 * O::DEG; e++) { pxp[e] = pxp[e - 1] * dx; pyp[e] = pyp[e - 1] * dy; }
+            const float gg[3] = {gx * gx, gx * gy, gy * gy};
+#pragma unroll
+            for (int dgr = 0; dgr <= 2 * O::DEG; dgr++)
+#pragma unroll
+                for (int bb = 0; bb <= dgr; bb++) {
+                    const float mono = pxp[dgr - bb] * pyp[bb];
+#pragma unroll
+                    for (int p = 0; p < 3; p++)
+                        mom[p][mom_idx(dgr - bb, bb)] = fmaf(gg[p], mono, mom[p][mom_idx(dgr - bb, bb)]);
+                }
+        }
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < NMOM; q++) {
+                const double v = warp_sum((double)mom[p][q]);
+                if (lane == 0) sm.mom[p * NMOM + q] = v;
+            }
+    }
+    if (n == 0) {
+        if (lane == 0) write_failed(A, idx, d, M, GPV_EMPTY_MASK, 0, 0.0, 0.0);
+        return;
+    }
+    const double dn = (double)n;
+    const double fm = sum_f / dn;
+    const float fmf = (float)fm;
+
+    // ---- setup pass 2: delta_f, A_j, S_j ---------------------------------
+    double sa = 0.0, saa = 0.0, Aj[M], Sj[M];
+#pragma unroll
+    for (int j = 0; j < M; j++) Aj[j] = Sj[j] = 0.0;
+    for (int i = lane; i < npx_t; i += 32) {
+        const float f = Sf[i];
+        if (f != f) continue;
+        const short2 o = po[i];
+        const double a = (double)f - fm;
+        const double gx = Sgx[i], gy = Sgy[i], dx = o.x, dy = o.y;
+        sa += a;
+        saa += a * a;
+#pragma unroll
+        for (int mu = 0; mu < NMU; mu++) {
+            const double mv = mu_val<double>(mu, dx, dy);
+            Aj[2 * mu] += gx * mv * a;
+            Aj[2 * mu + 1] += gy * mv * a;
+            Sj[2 * mu] += gx * mv;
+            Sj[2 * mu + 1] += gy * mv;
+        }
+    }
+    sa = warp_sum(sa);
+    saa = warp_sum(saa);
+#pragma unroll
+    for (int j = 0; j < M; j++) {
+        const double av = warp_sum(Aj[j]), sv = warp_sum(Sj[j]);
+        if (lane == 0) { sm.A[j] = av; sm.S[j] = sv; }
+    }
+    const double df = sqrt(saa);
+    if (df == 0.0) {
+        if (lane == 0) write_failed(A, idx, d, M, GPV_FEATURELESS, n, fm, df);
+        return;
+    }
+    __syncwarp();
+    assemble_hessian<ORDER>(sm.mom, sm.H, lane);
+    if (!spd_inverse_warp<M>(sm.H, sm.aug, sm.Hinv, lane)) {
+        if (lane == 0) {
+            write_failed(A, idx, d, M, GPV_SINGULAR_H, n, fm, df);
+            A.out[idx].sssig = sssig;
+            A.out[idx].sigma = sqrt(saa / dn);
+        }
+        return;
+    }
+
+    // ---- ICGN iterations ---------------------------------------------------
+    // Warp-uniform FP64 state (p, previous p, increment) lives in shared memory.
+    const double size = sqrt(dn);
+    if (lane < M) {
+        sm.p[lane] = d.p0[lane];
+        sm.pprev[lane] = d.p0[lane];
+    }
+    __syncwarp();
+    int iters = 0, status = GPV_OK;
+    bool converged = false;
+    double c_zncc = 0.0, c_znssd = 4.0, last_norm = 0.0, gm_last = 0.0, dg_last = 0.0;
+    for (int it = 1; it <= A.max_iter; it++) {
+        // local warp coefficients (FP32) about an exact integer base
+        const double X0 = cx + sm.p[0], Y0 = cy + sm.p[1];
+        const double bxd = floor(X0), byd = floor(Y0);
+        const int wbx = (int)bxd, wby = (int)byd;
+        const float ox = (float)(X0 - bxd), oy = (float)(Y0 - byd);
+        float ux = 0.f, uy = 0.f, vx = 0.f, vy = 0.f, uxx = 0.f, uxy = 0.f, uyy = 0.f, vxx = 0.f, vxy = 0.f, vyy = 0.f;
+        if (ORDER >= 1) { ux = (float)sm.p[2]; vx = (float)sm.p[3]; uy = (float)sm.p[4]; vy = (float)sm.p[5]; }
+        if (ORDER == 2) {
+            uxx = (float)(0.5 * sm.p[6 % M]); vxx = (float)(0.5 * sm.p[7 % M]); uxy = (float)sm.p[8 % M];
+            vxy = (float)sm.p[9 % M]; uyy = (float)(0.5 * sm.p[10 % M]); vyy = (float)(0.5 * sm.p[11 % M]);
+        }
+        // mean / norm sums: FP32 partials over kChunk pixels, FP64 across
+        // chunks and lanes.  Steepest-descent sums B_j: FP32 per lane (their
+        // rounding moves the increment by < 1e-9 px), FP64 across lanes.
+        double s1 = 0.0, s2 = 0.0, sfg = 0.0;
+        float pb[M];
+#pragma unroll
+        for (int j = 0; j < M; j++) pb[j] = 0.f;
+        for (int base = 0; base < npx_t; base += 32 * kChunk) {
+            float p1 = 0.f, p2 = 0.f, pfg = 0.f;
+#pragma unroll
+            for (int c = 0; c < kChunk; c++) {
+                const int i = base + c * 32 + lane;
+                if (i < npx_t) {
+                    const float fv = Sf[i];
+                    if (fv == fv) {
+                        const short2 o = po[i];
+                        const float dx = (float)o.x, dy = (float)o.y;
+                        float lx = fmaf(uy, dy, fmaf(ux, dx, ox)) + dx;
+                        float ly = fmaf(vy, dy, fmaf(vx, dx, oy)) + dy;
+                        float dxx = 0.f, dxy = 0.f, dyy = 0.f;
+                        if (ORDER == 2) {
+                            dxx = dx * dx; dxy = dx * dy; dyy = dy * dy;
+                            lx += fmaf(uxx, dxx, fmaf(uxy, dxy, uyy * dyy));
+                            ly += fmaf(vxx, dxx, fmaf(vxy, dxy, vyy * dyy));
+                        }
+                        int ix, iy;
+                        float tx, ty;
+                        split_clamped(wbx, lx, A.w, ix, tx);
+                        split_clamped(wby, ly, A.h, iy, ty);
+                        float a[6], b[6];
+                        basis(ty, a);
+                        basis(tx, b);
+                        const float g = contract<float>(G + (int64_t)iy * A.pitch32 + ix, A.pitch32, a, b);
+                        const float gc = g - fmf;
+                        p1 += gc;
+                        p2 = fmaf(gc, gc, p2);
+                        pfg = fmaf(fv - fmf, gc, pfg);
+                        const float gxg = Sgx[i] * gc, gyg = Sgy[i] * gc;
+                        pb[0] += gxg;
+                        pb[1] += gyg;
+                        if (ORDER >= 1) {
+                            pb[2 % M] = fmaf(gxg, dx, pb[2 % M]); pb[3 % M] = fmaf(gyg, dx, pb[3 % M]);
+                            pb[4 % M] = fmaf(gxg, dy, pb[4 % M]); pb[5 % M] = fmaf(gyg, dy, pb[5 % M]);
+                        }
+                        if (ORDER == 2) {
+                            const float hxx = 0.5f * dxx, hyy = 0.5f * dyy;
+                            pb[6 % M] = fmaf(gxg, hxx, pb[6 % M]); pb[7 % M] = fmaf(gyg, hxx, pb[7 % M]);
+                            pb[8 % M] = fmaf(gxg, dxy, pb[8 % M]); pb[9 % M] = fmaf(gyg, dxy, pb[9 % M]);
+                            pb[10 % M] = fmaf(gxg, hyy, pb[10 % M]); pb[11 % M] = fmaf(gyg, hyy, pb[11 % M]);
+                        }
+                    }
+                }
+            }
+            s1 += (double)p1;
+            s2 += (double)p2;
+            sfg += (double)pfg;
+        }
+        // reduce; lane 0 keeps the totals in shared memory
+        {
+            double v;
+            v = warp_sum(s1); if (lane == 0) sm.red[0] = v;
+            v = warp_sum(s2); if (lane == 0) sm.red[1] = v;
+            v = warp_sum(sfg); if (lane == 0) sm.red[2] = v;
+#pragma unroll
+            for (int j = 0; j < M; j++) {
+                v = warp_sum((double)pb[j]);
+                if (lane == 0) sm.red[3 + j] = v;
+            }
+        }
+        __syncwarp();
+        const double gmt = sm.red[0] / dn;               // mean of g - f_m
+        const double dg2 = sm.red[1] - sm.red[0] * gmt;  // sum (g - g_m)^2
+        const double dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
+        const double sab = sm.red[2] - gmt * sa;         // sum (f - f_m)(g - g_m)
+        const double znssd = 2.0 - 2.0 * sab / (df * dg);
+        const double ratio = df / dg;
+        if (lane < M) sm.grad[lane] = sm.A[lane] - ratio * (sm.red[3 + lane] - gmt * sm.S[lane]);
+        __syncwarp();
+        if (lane < M) {
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < M; k++) acc = fma(sm.Hinv[lane * M + k], sm.grad[k], acc);
+            sm.dp[lane] = -acc;
+            sm.pprev[lane] = sm.p[lane];
+        }
+        __syncwarp();
+        gm_last = fm + gmt;
+        dg_last = dg;
+        if (lane == 0) {
+            double pn[12], dpl[12], pl[12];
+#pragma unroll
+            for (int k = 0; k < 12; k++) {
+                dpl[k] = sm.dp[k % M];
+                pl[k] = sm.p[k % M];
+            }
+            bool ok = true;
+            if (ORDER == 0) {
+                pn[0] = pl[0] - dpl[0];
+                pn[1] = pl[1] - dpl[1];
+            } else if (ORDER == 1) {
+                ok = compose1(pl, dpl, pn);
+            } else {
+                ok = compose2(pl, dpl, pn, sm.aug);
+            }
+            if (ok) {
+#pragma unroll
+                for (int k = 0; k < M; k++) sm.p[k] = pn[k];
+            }
+            sm.flag[0] = ok;
+            sm.misc[0] = conv_norm<M>(dpl, size);
+        }
+        __syncwarp();
+        if (!sm.flag[0]) {
+            status = GPV_SINGULAR_WDELTA;  // p keeps the last valid warp
+            break;
+        }
+        const double nrm = sm.misc[0];
+        c_znssd = znssd;
+        c_zncc = 1.0 - znssd / 2.0;
+        iters = it;
+        last_norm = nrm;
+        if (lane == 0) write_history(A, idx, it, nrm, c_zncc, c_znssd);
+        if (!isfinite(nrm)) { status = GPV_NONFINITE; break; }
+        if (nrm < A.max_norm) { converged = true; break; }
+    }
+
+    // ---- eta diagnostic at the last sampled warp (optional) ----------------
+    double eu = 0.0, ev = 0.0;
+    const bool want_eta = (A.flags & GPV_SOLVE_ETA) && iters > 0 && status == GPV_OK;
+    if (want_eta) {
+        const double *pprev = sm.pprev;
+        const double X0 = cx + pprev[0], Y0 = cy + pprev[1];
+        const double bxd = floor(X0), byd = floor(Y0);
+        const int wbx = (int)bxd, wby = (int)byd;
+        const double ox = X0 - bxd, oy = Y0 - byd;
+        for (int i = lane; i < npx_t; i += 32) {
+            if (Sf[i] != Sf[i]) continue;
+            const short2 o = po[i];
+            const double dx = o.x, dy = o.y;
+            double lx = ox + dx, ly = oy + dy;
+            if (ORDER >= 1) {
+                lx += pprev[2] * dx + pprev[4] * dy;
+                ly += pprev[3] * dx + pprev[5] * dy;
+            }
+            if (ORDER == 2) {
+                lx += 0.5 * pprev[6 % M] * dx * dx + pprev[8 % M] * dx * dy + 0.5 * pprev[10 % M] * dy * dy;
+                ly += 0.5 * pprev[7 % M] * dx * dx + pprev[9 % M] * dx * dy + 0.5 * pprev[11 % M] * dy * dy;
+            }
+            int ix, iy;
+            float tx, ty;
+            split_clamped(wbx, (float)lx, A.w, ix, tx);
+            split_clamped(wby, (float)ly, A.h, iy, ty);
+            float a[6], b[6];
+            basis(ty, a);
+            basis(tx, b);
+            Sg[i] = contract<float>(G + (int64_t)iy * A.pitch32 + ix, A.pitch32, a, b);
+        }
+        __syncwarp();
+        auto load = [&](int i, double &f, double &gx, double &gy, double &g, double &dx, double &dy) -> bool {
+            const float fv = Sf[i];
+            if (fv != fv) return false;
+            const short2 o = po[i];
+            f = fv; gx = Sgx[i]; gy = Sgy[i]; g = Sg[i]; dx = o.x; dy = o.y;
+            return true;
+        };
+        auto red = [](double v) { return warp_sum(v); };
+        eta_sums<ORDER>(npx_t, lane, 32, dn, fm, df, gm_last, dg_last, load, red, eu, ev);
+    }
+    if (lane == 0) {
+        gpv_subset_result *o = A.out + idx;
+#pragma unroll
+        for (int k = 0; k < 12; k++) o->p[k] = k < M ? sm.p[k % M] : 0.0;
+        o->c_zncc = c_zncc;
+        o->c_znssd = c_znssd;
+        o->norm = last_norm;
+        o->eta_u = eu;
+        o->eta_v = ev;
+        o->f_m = fm;
+        o->delta_f = df;
+        o->sssig = sssig;
+        o->sigma = sqrt(saa / dn);
+        o->iterations = iters;
+        o->converged = converged;
+        o->quality_ok = converged && c_zncc >= A.tolerance;
+        o->status = status;
+        o->n_px = n;
+        o->has_eta = want_eta;
+    }
+}
+
+__global__ void __launch_bounds__(kMixedWarps * 32, 2) icgn_mixed(KArgs A) {
+    __shared__ WarpSmem smem[kMixedWarps];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t gw = (int64_t)blockIdx.x * kMixedWarps + wib;
+    const int64_t nmax = A.scratch_stride / 4;
+    float *S = reinterpret_cast<float *>(A.scratch) + gw * A.scratch_stride;
+    WarpSmem &sm = smem[wib];
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = atomicAdd(A.queue, 1);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= A.n) break;
+        const int idx = A.order ? A.order[item] : item;
+        const gpv_subset_desc d = A.desc[idx];
+        if (d.radius < 1 || d.radius > A.max_radius || d.order < 0 || d.order > 2) {
+            if (lane == 0) write_failed(A, idx, d, 12, GPV_INVALID_SUBSET, 0, 0.0, 0.0);
+            continue;
+        }
+        switch (d.order) {
+            case 0: mixed_subset<0>(A, idx, d, S, nmax, sm, lane); break;
+            case 1: mixed_subset<1>(A, idx, d, S, nmax, sm, lane); break;
+            default: mixed_subset<2>(A, idx, d, S, nmax, sm, lane); break;
+        }
+        __syncwarp();
+    }
+}
+
+// =====================================================================
+// Plain FP64 block-per-subset solve
+// =====================================================================
+struct BlockSmem {
+    double red[kFp64Warps][16];
+    double bcast[32];
+    double mom[3 * 15];
+    double H[144];
+    double Hinv[144];
+    int flag[4];
+};
+
+// Sum K values over the block; every thread receives the totals in v.
+template <int K>
+__device__ void block_sum(double (&v)[K], BlockSmem &sm) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; k++) sm.red[wid][k] = v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kFp64Warps; w++) s += sm.red[w][k];
+        v[k] = s;
+    }
+}
+
+__device__ double block_sum1(double x, BlockSmem &sm) {
+    double v[1] = {x};
+    block_sum<1>(v, sm);
+    return v[0];
+}
+
+// Serial Gauss-Jordan with partial pivoting (one thread).
+template <int M>
+__device__ bool gj_inverse_serial(const double *Ain, double *Ainv) {
+    double a[M][2 * M];
+    for (int i = 0; i < M; i++)
+        for (int j = 0; j < 2 * M; j++) a[i][j] = j < M ? Ain[i * M + j] : (j - M == i ? 1.0 : 0.0);
+    for (int k = 0; k < M; k++) {
+        int piv = k;
+        double best = fabs(a[k][k]);
+        for (int i = k + 1; i < M; i++)
+            if (fabs(a[i][k]) > best) { best = fabs(a[i][k]); piv = i; }
+        if (!(best > 0.0) || !isfinite(best)) return false;
+        if (piv != k)
+            for (int j = 0; j < 2 * M; j++) { double t = a[k][j]; a[k][j] = a[piv][j]; a[piv][j] = t; }
+        const double dinv = 1.0 / a[k][k];
+        for (int j = 0; j < 2 * M; j++) a[k][j] *= dinv;
+        for (int i = 0; i < M; i++) {
+            if (i == k) continue;
+            const double f = a[i][k];
+            if (f == 0.0) continue;
+            for (int j = 0; j < 2 * M; j++) a[i][j] -= f * a[k][j];
+        }
+    }
+    for (int i = 0; i < M; i++)
+        for (int j = 0; j < M; j++) Ainv[i * M + j] = a[i][j + M];
+    return true;
+}
+
+template <int ORDER>
+__device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, double *S, int64_t nmax, BlockSmem &sm) {
+    using O = Ord<ORDER>;
+    constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int r = d.radius;
+    const int npx_t = A.tab_n[r];
+    const short2 *po = A.offs + A.tab_off[r];
+    double *Sf = S, *Sgx = S + nmax, *Sgy = S + 2 * nmax, *Sg = S + 3 * nmax;
+    const double cx = d.coord[0], cy = d.coord[1];
+    const int cxi = (int)cx, cyi = (int)cy;
+    const double fxd = floor(cx), fyd = floor(cy);
+    const int bx = (int)fxd, by = (int)fyd;
+    const double fx = cx - fxd, fy = cy - fyd;
+    const double *F = A.f64 + (int64_t)(A.border - 2) * A.pitch64 + (A.border - 2);
+    const double *G = A.g64 + (int64_t)(A.border - 2) * A.pitch64 + (A.border - 2);
+
+    // Subset::new: f, grad f (:877-884)
+    double loc[4] = {0, 0, 0, 0};  // sum f, count, sssig
+    for (int i = tid; i < npx_t; i += nthr) {
+        const short2 o = po[i];
+        if (!mask_ok(A, cxi, cyi, o.x, o.y)) { Sf[i] = __longlong_as_double(0x7ff8000000000000ll); continue; }
+        int ix, iy;
+        double tx, ty;
+        split_clamped(bx, fx + (double)o.x, A.w, ix, tx);
+        split_clamped(by, fy + (double)o.y, A.h, iy, ty);
+        double a[6], da[6], b[6], db[6];
+        basis(ty, a); dbasis(ty, da);
+        basis(tx, b); dbasis(tx, db);
+        double gx, gy;
+        const double f = contract_grad<double>(F + (int64_t)iy * A.pitch64 + ix, A.pitch64, a, da, b, db, gx, gy);
+        Sf[i] = f; Sgx[i] = gx; Sgy[i] = gy;
+        loc[0] += f;
+        loc[1] += 1.0;
+        loc[2] += 0.5 * (gx * gx + gy * gy);
+    }
+    block_sum<4>(loc, sm);
+    const int n = (int)loc[1];
+    const double sssig = loc[2];
+    if (n == 0) {
+        if (tid == 0) write_failed(A, idx, d, M, GPV_EMPTY_MASK, 0, 0.0, 0.0);
+        return;
+    }
+    const double dn = (double)n, fm = loc[0] / dn;
+    double ss = 0.0;
+    for (int i = tid; i < npx_t; i += nthr) {
+        const double f = Sf[i];
+        if (f != f) continue;
+        ss += (f - fm) * (f - fm);
+    }
+    ss = block_sum1(ss, sm);
+    const double df = sqrt(ss);
+    if (df == 0.0) {
+        if (tid == 0) write_failed(A, idx, d, M, GPV_FEATURELESS, n, fm, df);
+        return;
+    }
+    // compute_hessian (:348-364) via FP64 gradient moments
+    double mom[3 * NMOM];
+#pragma unroll
+    for (int q = 0; q < 3 * NMOM; q++) mom[q] = 0.0;
+    for (int i = tid; i < npx_t; i += nthr) {
+        const double f = Sf[i];
+        if (f != f) continue;
+        const short2 o = po[i];
+        const double gx = Sgx[i], gy = Sgy[i], dx = o.x, dy = o.y;
+        double pxp[5], pyp[5];
+        pxp[0] = pyp[0] = 1.0;
+#pragma unroll
+        for (int e = 1; e <= 2 * O::DEG; e++) { pxp[e] = pxp[e - 1] * dx; pyp[e] = pyp[e - 1] * dy; }
+        const double gg[3] = {gx * gx, gx * gy, gy * gy};
+#pragma unroll
+        for (int dgr = 0; dgr <= 2 * O::DEG; dgr++)
+#pragma unroll
+            for (int bb = 0; bb <= dgr; bb++) {
+                const double mono = pxp[dgr - bb] * pyp[bb];
+#pragma unroll
+                for (int p = 0; p < 3; p++) mom[p * NMOM + mom_idx(dgr - bb, bb)] += gg[p] * mono;
+            }
+    }
+#pragma unroll
+    for (int q = 0; q < 3 * NMOM; q++) {
+        const double v = block_sum1(mom[q], sm);
+        if (tid == 0) sm.mom[q] = v;
+    }
+    __syncthreads();
+    if (tid < 32) assemble_hessian<ORDER>(sm.mom, sm.H, tid);
+    __syncthreads();
+    if (tid == 0) sm.flag[0] = gj_inverse_serial<M>(sm.H, sm.Hinv);
+    __syncthreads();
+    if (!sm.flag[0]) {
+        if (tid == 0) {
+            write_failed(A, idx, d, M, GPV_SINGULAR_H, n, fm, df);
+            A.out[idx].sssig = sssig;
+            A.out[idx].sigma = sqrt(ss / dn);
+        }
+        return;
+    }
+    const double size = sqrt(dn);
+    double p[M], pprev[M];
+#pragma unroll
+    for (int k = 0; k < M; k++) p[k] = pprev[k] = d.p0[k];
+    int iters = 0, status = GPV_OK;
+    bool converged = false;
+    double c_zncc = 0.0, c_znssd = 4.0, last_norm = 0.0, gm_last = 0.0, dg_last = 0.0;
+    for (int it = 1; it <= A.max_iter; it++) {
+        // apply_warp_into + eval (:1158-1161)
+        double sg = 0.0;
+        for (int i = tid; i < npx_t; i += nthr) {
+            if (Sf[i] != Sf[i]) continue;
+            const short2 o = po[i];
+            const double dx = o.x, dy = o.y;
+            double xw = cx + dx + p[0], yw = cy + dy + p[1];
+            if (ORDER >= 1) {
+                xw = (cx + dx) + p[0] + p[2] * dx + p[4] * dy;
+                yw = (cy + dy) + p[1] + p[3] * dx + p[5] * dy;
+            }
+            if (ORDER == 2) {
+                xw += 0.5 * p[6 % M] * dx * dx + p[8 % M] * dx * dy + 0.5 * p[10 % M] * dy * dy;
+                yw += 0.5 * p[7 % M] * dx * dx + p[9 % M] * dx * dy + 0.5 * p[11 % M] * dy * dy;
+            }
+            const double xfl = floor(xw), yfl = floor(yw);
+            int ix, iy;
+            double tx, ty;
+            split_clamped((int)xfl, xw - xfl, A.w, ix, tx);
+            split_clamped((int)yfl, yw - yfl, A.h, iy, ty);
+            double a[6], b[6];
+            basis(ty, a);
+            basis(tx, b);
+            const double g = contract<double>(G + (int64_t)iy * A.pitch64 + ix, A.pitch64, a, b);
+            Sg[i] = g;
+            sg += g;
+        }
+        sg = block_sum1(sg, sm);
+        const double gm = sg / dn;
+        double sgg = 0.0;
+        for (int i = tid; i < npx_t; i += nthr) {
+            if (Sf[i] != Sf[i]) continue;
+            sgg += (Sg[i] - gm) * (Sg[i] - gm);
+        }
+        sgg = block_sum1(sgg, sm);
+        const double dg = sqrt(sgg);
+        // delta_p_and_znssd_icgn (:418-446)
+        const double ratio = df / dg;
+        double acc[M + 1];
+#pragma unroll
+        for (int k = 0; k <= M; k++) acc[k] = 0.0;
+        for (int i = tid; i < npx_t; i += nthr) {
+            const double f = Sf[i];
+            if (f != f) continue;
+            const short2 o = po[i];
+            const double a = f - fm, b = Sg[i] - gm;
+            const double z = a / df - b / dg;
+            acc[M] += z * z;
+            const double br = a - ratio * b;
+            const double gx = Sgx[i], gy = Sgy[i], dx = o.x, dy = o.y;
+#pragma unroll
+            for (int mu = 0; mu < NMU; mu++) {
+                const double mv = mu_val<double>(mu, dx, dy);
+                acc[2 * mu] += gx * mv * br;
+                acc[2 * mu + 1] += gy * mv * br;
+            }
+        }
+        block_sum<M + 1>(acc, sm);
+        double dp[M];
+#pragma unroll
+        for (int j = 0; j < M; j++) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < M; k++) s += sm.Hinv[j * M + k] * acc[k];
+            dp[j] = -s;
+        }
+#pragma unroll
+        for (int k = 0; k < M; k++) pprev[k] = p[k];
+        gm_last = gm;
+        dg_last = dg;
+        bool ok = true;
+        if (ORDER == 0) {
+            p[0] -= dp[0];
+            p[1] -= dp[1];
+        } else if (ORDER == 1) {
+            double pn[6];
+            ok = compose1(p, dp, pn);
+            if (ok) {
+#pragma unroll
+                for (int k = 0; k < 6; k++) p[k] = pn[k];
+            }
+        } else {
+            __syncthreads();
+            if (tid == 0) {
+                double pn[12];
+                double ws[96];
+                sm.flag[1] = compose2(p, dp, pn, ws);
+                for (int k = 0; k < 12; k++) sm.bcast[k] = pn[k];
+            }
+            __syncthreads();
+            ok = sm.flag[1] != 0;
+            if (ok) {
+#pragma unroll
+                for (int k = 0; k < M; k++) p[k] = sm.bcast[k];
+            }
+        }
+        if (!ok) {
+#pragma unroll
+            for (int k = 0; k < M; k++) p[k] = pprev[k];
+            status = GPV_SINGULAR_WDELTA;
+            break;
+        }
+        const double nrm = conv_norm<M>(dp, size);
+        c_znssd = acc[M];
+        c_zncc = 1.0 - acc[M] / 2.0;
+        iters = it;
+        last_norm = nrm;
+        if (tid == 0) write_history(A, idx, it, nrm, c_zncc, c_znssd);
+        if (!isfinite(nrm)) { status = GPV_NONFINITE; break; }
+        if (nrm < A.max_norm) { converged = true; break; }
+    }
+    double eu = 0.0, ev = 0.0;
+    const bool want_eta = (A.flags & GPV_SOLVE_ETA) && iters > 0 && status == GPV_OK;
+    if (want_eta) {
+        auto load = [&](int i, double &f, double &gx, double &gy, double &g, double &dx, double &dy) -> bool {
+            f = Sf[i];
+            if (f != f) return false;
+            const short2 o = po[i];
+            gx = Sgx[i]; gy = Sgy[i]; g = Sg[i]; dx = o.x; dy = o.y;
+            return true;
+        };
+        auto red = [&](double v) { return block_sum1(v, sm); };
+        eta_sums<ORDER>(npx_t, tid, nthr, dn, fm, df, gm_last, dg_last, load, red, eu, ev);
+    }
+    if (tid == 0) {
+        gpv_subset_result *o = A.out + idx;
+#pragma unroll
+        for (int k = 0; k < 12; k++) o->p[k] = k < M ? p[k % M] : 0.0;
+        o->c_zncc = c_zncc;
+        o->c_znssd = c_znssd;
+        o->norm = last_norm;
+        o->eta_u = eu;
+        o->eta_v = ev;
+        o->f_m = fm;
+        o->delta_f = df;
+        o->sssig = sssig;
+        o->sigma = sqrt(ss / dn);
+        o->iterations = iters;
+        o->converged = converged;
+        o->quality_ok = converged && c_zncc >= A.tolerance;
+        o->status = status;
+        o->n_px = n;
+        o->has_eta = want_eta;
+    }
+}
+
+__global__ void __launch_bounds__(kFp64Threads) icgn_fp64(KArgs A) {
+    __shared__ BlockSmem sm;
+    __shared__ int item_s;
+    double *S = reinterpret_cast<double *>(A.scratch) + (int64_t)blockIdx.x * A.scratch_stride;
+    const int64_t nmax = A.scratch_stride / 4;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item_s = atomicAdd(A.queue, 1);
+        __syncthreads();
+        const int item = item_s;
+        if (item >= A.n) break;
+        const int idx = A.order ? A.order[item] : item;
+        const gpv_subset_desc d = A.desc[idx];
+        if (d.radius < 1 || d.radius > A.max_radius || d.order < 0 || d.order > 2) {
+            if (threadIdx.x == 0) write_failed(A, idx, d, 12, GPV_INVALID_SUBSET, 0, 0.0, 0.0);
+            continue;
+        }
+        switch (d.order) {
+            case 0: fp64_subset<0>(A, idx, d, S, nmax, sm); break;
+            case 1: fp64_subset<1>(A, idx, d, S, nmax, sm); break;
+            default: fp64_subset<2>(A, idx, d, S, nmax, sm); break;
+        }
+    }
+}
+
+// Point evaluation (gpv_image_eval): one thread per point.
+template <typename T, typename C>
+__global__ void eval_points(const C *coef, int64_t pitch, int h, int w, int border, const double *xy, int64_t n,
+                            double *out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = xy[2 * i], y = xy[2 * i + 1];
+    // clamp as Image::eval, then split about an exact integer base
+    const double xc = fmin(fmax(x, 0.0), (double)w - 1e-9), yc = fmin(fmax(y, 0.0), (double)h - 1e-9);
+    const double xf = floor(xc), yf = floor(yc);
+    int ix, iy;
+    T tx, ty;
+    split_clamped((int)xf, (T)(xc - xf), w, ix, tx);
+    split_clamped((int)yf, (T)(yc - yf), h, iy, ty);
+    T a[6], da[6], b[6], db[6];
+    basis(ty, a); dbasis(ty, da);
+    basis(tx, b); dbasis(tx, db);
+    T gx, gy;
+    const C *p = coef + (int64_t)(iy + border - 2) * pitch + (ix + border - 2);
+    const T v = contract_grad<T>(p, pitch, a, da, b, db, gx, gy);
+    out[3 * i] = (double)v;
+    out[3 * i + 1] = (double)gx;
+    out[3 * i + 2] = (double)gy;
+}
+
+}  // namespace
+
+int eval_launch(const gpv_image *img, const double *xy_dev, int64_t n, int precision, double *out_dev, cudaStream_t s) {
+    if (n == 0) return GPV_SUCCESS;
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (precision == GPV_PREC_FP64) {
+        if (!img->c64) { set_error("FP64 evaluation needs GPV_IMAGE_KEEP_F64"); return GPV_ERR_INVALID; }
+        eval_points<double, double><<<blocks, 256, 0, s>>>(img->c64, img->pitch64, (int)img->h, (int)img->w,
+                                                           img->border, xy_dev, n, out_dev);
+    } else {
+        eval_points<float, float><<<blocks, 256, 0, s>>>(img->c32, img->pitch32, (int)img->h, (int)img->w, img->border,
+                                                         xy_dev, n, out_dev);
+    }
+    GPV_CUDA_TRY(cudaGetLastError());
+    return GPV_SUCCESS;
+}
+
+int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
+    if (L.n == 0) return GPV_SUCCESS;
+    const gpv_solve_params *prm = L.prm;
+    const bool fp64 = prm->precision == GPV_PREC_FP64;
+    KArgs A;
+    A.f32 = L.f->c32; A.g32 = L.g->c32;
+    A.f64 = L.f->c64; A.g64 = L.g->c64;
+    A.pitch32 = L.f->pitch32; A.pitch64 = L.f->pitch64;
+    A.h = (int)L.f->h; A.w = (int)L.f->w; A.border = L.f->border;
+    A.desc = L.desc; A.order = L.order; A.n = (int)L.n;
+    A.offs = static_cast<const short2 *>(ctx->offs.ptr);
+    A.tab_off = static_cast<const int32_t *>(ctx->tab_off.ptr);
+    A.tab_n = static_cast<const int32_t *>(ctx->tab_n.ptr);
+    A.max_radius = L.max_radius;
+    A.mask = L.mask; A.mh = (int)L.mh; A.mw = (int)L.mw;
+    A.max_norm = prm->max_norm; A.tolerance = prm->tolerance;
+    A.max_iter = prm->max_iterations; A.flags = prm->flags;
+    A.out = L.out; A.history = L.history;
+    const int64_t npx_max = ctx->h_tab_n[L.max_radius];
+    int workers, threads;
+    size_t elem;
+    if (fp64) {
+        int per_sm = 0;
+        GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_fp64, kFp64Threads, 0));
+        if (per_sm < 1) per_sm = 1;
+        workers = ctx->num_sms * per_sm;
+        threads = kFp64Threads;
+        elem = sizeof(double);
+    } else {
+        if (ctx->mixed_blocks_per_sm == 0) {
+            int per_sm = 0;
+            GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icgn_mixed, kMixedWarps * 32, 0));
+            ctx->mixed_blocks_per_sm = per_sm < 1 ? 1 : per_sm;
+        }
+        workers = ctx->num_sms * ctx->mixed_blocks_per_sm * kMixedWarps;  // warps
+        threads = kMixedWarps * 32;
+        elem = sizeof(float);
+    }
+    const int64_t stride = 4 * ((npx_max + 31) / 32 * 32);
+    const size_t need = (size_t)workers * stride * elem;
+    if (int rc = ctx->scratch.ensure(need)) return rc;
+    if (int rc = ctx->queue.ensure(64)) return rc;
+    A.scratch = ctx->scratch.ptr;
+    A.scratch_stride = stride;
+    A.queue = static_cast<int *>(ctx->queue.ptr);
+    GPV_CUDA_TRY(cudaMemsetAsync(A.queue, 0, sizeof(int), s));
+    if (fp64) {
+        icgn_fp64<<<workers, threads, 0, s>>>(A);
+    } else {
+        icgn_mixed<<<workers / kMixedWarps, threads, 0, s>>>(A);
+    }
+    GPV_CUDA_TRY(cudaGetLastError());
+    return GPV_SUCCESS;
+}
+
+}  // namespace gpv
+
+// ---------------------------------------------------------------------------
+// FP32 FMA throughput probe: independent FMA chains in registers only.
+// ---------------------------------------------------------------------------
+namespace gpv {
+namespace {
+constexpr int kProbeChains = 8;
+constexpr int kProbeIters = 4096;
+__global__ void __launch_bounds__(256) fma_probe(float *out, float a, float b) {
+    float x[kProbeChains];
+#pragma unroll
+    for (int c = 0; c < kProbeChains; c++) x[c] = (float)(threadIdx.x + c);
+    for (int it = 0; it < kProbeIters; it++) {
+#pragma unroll
+        for (int c = 0; c < kProbeChains; c++) x[c] = fmaf(x[c], a, b);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < kProbeChains; c++) s += x[c];
+    if (s == 1234.5f) out[threadIdx.x] = s;  // keeps the chains live
+}
+}  // namespace
+
+int probe_fp32_peak(gpv_context *ctx, double *tflops) {
+    const int blocks = ctx->num_sms * 8;
+    float *out = nullptr;
+    GPV_CUDA_TRY(cudaMalloc(&out, 256 * sizeof(float)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 0.0;
+    for (int rep = 0; rep < 5; rep++) {
+        cudaEventRecord(e0, ctx->stream);
+        fma_probe<<<blocks, 256, 0, ctx->stream>>>(out, 0.9999f, 1e-4f);
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double flop = 2.0 * blocks * 256.0 * kProbeChains * kProbeIters;
+        if (rep > 0 && ms > 0.f) best = fmax(best, flop / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    GPV_CUDA_TRY(cudaGetLastError());
+    *tflops = best;
+    return GPV_SUCCESS;
+}
+}  // namespace gpv

@@ -1,0 +1,105 @@
+// internal.h -- host-side objects behind the C ABI (include/gpv.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gpv.h"
+
+namespace gpv {
+
+void set_error(const std::string &msg);
+
+#define GPV_CUDA_TRY(expr)                                                                       \
+    do {                                                                                         \
+        cudaError_t _e = (expr);                                                                 \
+        if (_e != cudaSuccess) {                                                                 \
+            ::gpv::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));                \
+            return GPV_ERR_CUDA;                                                                 \
+        }                                                                                        \
+    } while (0)
+
+// Taps of the periodised inverse quintic filter for one circular length.
+// c[n] = sum_{m=-ml}^{mr} h[m + ml] * x[(n - m) mod N].
+struct Taps {
+    int n = 0, ml = 0, mr = 0;
+    std::vector<double> h;
+};
+const Taps &taps_for(int64_t n);  // cached, thread-safe
+
+// Device buffer that only grows.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want);
+    void release();
+};
+
+}  // namespace gpv
+
+struct gpv_context {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    // circular mask offset tables, radii 1..table_radius (short2 per pixel)
+    int table_radius = 0;
+    gpv::DevBuf offs;     // short2
+    gpv::DevBuf tab_off;  // int32 [table_radius + 1]
+    gpv::DevBuf tab_n;    // int32 [table_radius + 1]
+    std::vector<int32_t> h_tab_off, h_tab_n;
+    // solve workspace
+    gpv::DevBuf scratch;   // per-warp / per-block pixel arrays
+    gpv::DevBuf queue;     // work-queue counters
+    gpv::DevBuf desc_dev;  // staging for the host API
+    gpv::DevBuf out_dev;
+    gpv::DevBuf order_dev;
+    gpv::DevBuf hist_dev;
+    gpv::DevBuf eval_dev;
+    int mixed_blocks_per_sm = 0;
+};
+
+struct gpv_image {
+    gpv_context *ctx = nullptr;
+    int64_t h = 0, w = 0, ch = 0, cw = 0;
+    int32_t border = 0;
+    int64_t pitch32 = 0, pitch64 = 0;  // elements per coefficient row
+    float *c32 = nullptr;
+    double *c64 = nullptr;
+    double *rowpass = nullptr;  // FP64 row-pass intermediate (h, cw)
+    void *px_dev = nullptr;     // staging for host pixels
+    size_t px_bytes = 0;
+    uint32_t flags = 0;
+};
+
+struct gpv_mask {
+    gpv_context *ctx = nullptr;
+    int64_t h = 0, w = 0;
+    uint8_t *dev = nullptr;
+};
+
+namespace gpv {
+// prefilter.cu
+int prefilter_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s);
+// icgn.cu
+struct SolveLaunch {
+    const gpv_image *f, *g;
+    const gpv_subset_desc *desc;  // device
+    const int32_t *order;         // device or null
+    int64_t n;
+    const gpv_solve_params *prm;
+    const uint8_t *mask;
+    int64_t mh, mw;
+    gpv_subset_result *out;  // device
+    double *history;         // device or null
+    int max_radius;
+};
+int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s);
+int eval_launch(const gpv_image *img, const double *xy_dev, int64_t n, int precision, double *out_dev,
+                cudaStream_t s);
+int ensure_tables(gpv_context *ctx, int max_radius);
+int probe_fp32_peak(gpv_context *ctx, double *tflops);
+}  // namespace gpv

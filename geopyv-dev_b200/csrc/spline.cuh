@@ -1,0 +1,129 @@
+// spline.cuh -- bi-quintic B-spline basis and evaluation on the device.
+//
+// The interpolant is the one of Image::eval / Image::eval_grad
+// (src/image.rs:115-230): value = a(ty)^T * C_block * b(tx), with
+// a, b = Q^T [1, t, ..., t^5] and the 6x6 coefficient block starting at
+// C[yf + border - 2, xf + border - 2] after clamping (x, y) into
+// [0, w - 1e-9] x [0, h - 1e-9].
+//
+// The six weights are evaluated in a symmetric split about t = 1/2
+// (u = t - 1/2, v = u^2): w_k = e_k + o_k, w_{5-k} = e_k - o_k with e_k
+// even quartics in u and o_k odd quintics.  The coefficients below are
+// Q's columns re-expanded about t = 1/2 (exact rationals); this takes 23
+// operations per axis instead of the 36 multiply-adds of Q^T [1..t^5].
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gpv {
+
+template <typename T>
+__device__ __forceinline__ void basis(T t, T w[6]) {
+    const T u = t - T(0.5);
+    const T v = u * u;
+    const T e0 = fma(fma(v, T(1.0 / 48.0), T(1.0 / 96.0)), v, T(1.0 / 3840.0));
+    const T e1 = fma(fma(v, T(-1.0 / 16.0), T(7.0 / 32.0)), v, T(79.0 / 1280.0));
+    const T e2 = fma(fma(v, T(1.0 / 24.0), T(-11.0 / 48.0)), v, T(841.0 / 1920.0));
+    const T o0 = -u * fma(fma(v, T(1.0 / 120.0), T(1.0 / 48.0)), v, T(1.0 / 384.0));
+    const T o1 = -u * fma(fma(v, T(-1.0 / 24.0), T(1.0 / 16.0)), v, T(25.0 / 128.0));
+    const T o2 = -u * fma(fma(v, T(1.0 / 12.0), T(-7.0 / 24.0)), v, T(77.0 / 192.0));
+    w[0] = e0 + o0;
+    w[5] = e0 - o0;
+    w[1] = e1 + o1;
+    w[4] = e1 - o1;
+    w[2] = e2 + o2;
+    w[3] = e2 - o2;
+}
+
+// d/dt of the weights (Image::rows uses the derivative at the fractional
+// position itself, src/image.rs:210-230).
+template <typename T>
+__device__ __forceinline__ void dbasis(T t, T d[6]) {
+    const T u = t - T(0.5);
+    const T v = u * u;
+    const T two_u = u + u;
+    // de_k/du = 2u (q1 + 2 q2 v);  do_k/du = -(p0 + 3 p1 v + 5 p2 v^2)
+    const T de0 = two_u * fma(v, T(2.0 / 48.0), T(1.0 / 96.0));
+    const T de1 = two_u * fma(v, T(-2.0 / 16.0), T(7.0 / 32.0));
+    const T de2 = two_u * fma(v, T(2.0 / 24.0), T(-11.0 / 48.0));
+    const T do0 = -fma(fma(v, T(5.0 / 120.0), T(3.0 / 48.0)), v, T(1.0 / 384.0));
+    const T do1 = -fma(fma(v, T(-5.0 / 24.0), T(3.0 / 16.0)), v, T(25.0 / 128.0));
+    const T do2 = -fma(fma(v, T(5.0 / 12.0), T(-21.0 / 24.0)), v, T(77.0 / 192.0));
+    d[0] = de0 + do0;
+    d[5] = de0 - do0;
+    d[1] = de1 + do1;
+    d[4] = de1 - do1;
+    d[2] = de2 + do2;
+    d[3] = de2 - do2;
+}
+
+// Split a coordinate into an integer pixel index and a fraction in [0, 1]
+// with the reference clamp (src/image.rs:129-132): below 0 -> (0, 0), at or
+// beyond the last pixel -> (n - 1, 1 - 1e-9).  `base` is an exact integer offset
+// added to the small local coordinate `loc` (keeps FP32 fractions exact).
+template <typename T>
+__device__ __forceinline__ void split_clamped(int base, T loc, int n, int &i, T &t) {
+    const T fl = floor(loc);
+    i = base + (int)fl;
+    t = loc - fl;
+    if (i < 0) {
+        i = 0;
+        t = T(0);
+    } else if (i > n - 1) {
+        i = n - 1;
+        t = T(1) - T(1e-9);  // x clamped to n - 1e-9 (rounds to 1 in FP32)
+    }
+}
+
+// Value at a clamped position; p points at C[iy + border - 2][ix + border - 2].
+template <typename T, typename C>
+__device__ __forceinline__ T contract(const C *__restrict__ p, int64_t pitch, const T a[6], const T b[6]) {
+    T val = T(0);
+#pragma unroll
+    for (int r = 0; r < 6; r++) {
+        const C *row = p + r * pitch;
+        T s = T(row[0]) * b[0];
+#pragma unroll
+        for (int k = 1; k < 6; k++) s = fma(T(row[k]), b[k], s);
+        val = fma(a[r], s, val);
+    }
+    return val;
+}
+
+// Value and gradient (Image::eval_grad, src/image.rs:115-124, :155-178).
+template <typename T, typename C>
+__device__ __forceinline__ T contract_grad(const C *__restrict__ p, int64_t pitch, const T a[6], const T da[6],
+                                           const T b[6], const T db[6], T &gx, T &gy) {
+    T val = T(0), vx = T(0), vy = T(0);
+#pragma unroll
+    for (int r = 0; r < 6; r++) {
+        const C *row = p + r * pitch;
+        T s = T(0), q = T(0);
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const T c = T(row[k]);
+            s = fma(c, b[k], s);
+            q = fma(c, db[k], q);
+        }
+        val = fma(a[r], s, val);
+        vx = fma(a[r], q, vx);
+        vy = fma(da[r], s, vy);
+    }
+    gx = vx;
+    gy = vy;
+    return val;
+}
+
+// ---- warp reductions --------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ int warp_sum_int(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace gpv

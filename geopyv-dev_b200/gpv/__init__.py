@@ -1,0 +1,298 @@
+"""gpv -- Python host interface of the B200 subset-correlation library.
+
+Mirrors the reference package's Python classes for this path
+(geopyv_dev/__init__.py:299-385 ``Subset``, python/src/py_image.rs:41-64
+``Image``, python/src/py_mask.rs:89-154 ``Mask``) over the C ABI of
+``include/gpv.h``.  All arithmetic runs in the CUDA library; this module only
+marshals arguments.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import threading
+
+import numpy as np
+
+from . import _lib
+from ._lib import (DESC_DTYPE, RESULT_DTYPE, PREC_FP64, PREC_MIXED, SOLVE_ETA, STATUS, GpvError, SolveParams,
+                   check, lib, ptr)
+
+__all__ = ["Context", "Image", "Mask", "Subset", "solve_batch", "make_desc", "DESC_DTYPE", "RESULT_DTYPE",
+           "GpvError", "PREC_MIXED", "PREC_FP64", "STATUS", "version"]
+
+
+def version() -> str:
+    return lib().gpv_version().decode()
+
+
+class Context:
+    """One CUDA device, one stream and the solve workspace (gpv_context)."""
+
+    def __init__(self, device: int = 0):
+        h = ct.c_void_p()
+        check(lib().gpv_context_create(device, ct.byref(h)), "gpv_context_create")
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return lib().gpv_context_stream(self._h) or 0
+
+    def reserve(self, n_subsets: int, max_radius: int, max_iterations: int = 50) -> None:
+        check(lib().gpv_context_reserve(self._h, n_subsets, max_radius, max_iterations), "gpv_context_reserve")
+
+    def close(self) -> None:
+        if self._h:
+            lib().gpv_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default = {}
+_default_lock = threading.Lock()
+
+
+def default_context(device: int = 0) -> Context:
+    with _default_lock:
+        if device not in _default:
+            _default[device] = Context(device)
+        return _default[device]
+
+
+class Image:
+    """Device-resident bi-quintic B-spline coefficients of a greyscale image.
+
+    ``Image(image_gs=array, border=20)`` as python/src/py_image.rs:42-64 (the
+    coefficients are computed on the GPU: Image::from_array -> get_c,
+    src/image.rs:83-86, :252-327).  ``keep_f64`` keeps an FP64 copy of the
+    coefficients for the FP64 solver.
+    """
+
+    def __init__(self, filepath=None, image_gs=None, border: int = 20, keep_f64: bool = False, ctx: Context | None = None):
+        if filepath is not None and image_gs is not None:
+            raise ValueError("supply exactly one of `filepath` or `image_gs`, not both")
+        if filepath is not None:
+            raise NotImplementedError("loading image files is not part of this library; pass image_gs")
+        if image_gs is None:
+            raise ValueError("one of `filepath` or `image_gs` is required")
+        arr = np.asarray(image_gs)
+        if arr.ndim != 2:
+            raise ValueError("image_gs must be 2-D")
+        if arr.dtype not in _lib.DTYPES:
+            arr = arr.astype(np.float64)
+        arr = np.ascontiguousarray(arr)
+        self.ctx = ctx or default_context()
+        self.shape = arr.shape
+        self.border = border
+        self.dtype = arr.dtype
+        h = ct.c_void_p()
+        flags = _lib.IMAGE_KEEP_F64 if keep_f64 else 0
+        check(lib().gpv_image_create(self.ctx.handle, ptr(arr), _lib.DTYPES[arr.dtype], arr.shape[0], arr.shape[1],
+                                     border, flags, ct.byref(h)), "gpv_image_create")
+        self._h = h
+        self.keep_f64 = keep_f64
+
+    @property
+    def handle(self):
+        return self._h
+
+    def coef(self, f64: bool = False) -> np.ndarray:
+        """Coefficient array C, shape (h + 2 border, w + 2 border) (src/image.rs:48-51)."""
+        shp = (self.shape[0] + 2 * self.border, self.shape[1] + 2 * self.border)
+        if f64:
+            out = np.empty(shp, np.float64)
+            check(lib().gpv_image_coefficients_f64(self._h, ptr(out)), "gpv_image_coefficients_f64")
+        else:
+            out = np.empty(shp, np.float32)
+            check(lib().gpv_image_coefficients_f32(self._h, ptr(out)), "gpv_image_coefficients_f32")
+        return out
+
+    def eval(self, xy, grad: bool = False, precision: int = PREC_MIXED):
+        """Spline value (and gradient) at points (x = column, y = row): Image::eval / eval_grad."""
+        xy = np.ascontiguousarray(np.atleast_2d(xy), dtype=np.float64)
+        n = xy.shape[0]
+        val = np.empty(n)
+        g = np.empty((n, 2)) if grad else None
+        check(lib().gpv_image_eval(self._h, ptr(xy), n, precision, ptr(val), ptr(g)), "gpv_image_eval")
+        return (val, g) if grad else val
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gpv_image_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mask:
+    """Local (circular template) or global (binary image) mask.
+
+    ``Mask("local", shape="circle", size=25)`` as python/src/py_mask.rs:89-110;
+    ``Mask("global", binary=array)`` takes the binary mask image directly
+    (the reference rasterises it from boundary polygons, which is outside this
+    library).
+    """
+
+    def __init__(self, mask_type: str, shape: str | None = None, size: int = 25, binary=None, ctx: Context | None = None):
+        self.mask_type = mask_type
+        self._h = None
+        if mask_type == "local":
+            if shape is None:
+                raise ValueError("shape is required for mask_type='local'")
+            if shape != "circle":
+                raise NotImplementedError(f"local mask shape '{shape}': only 'circle' is supported")
+            if size <= 0:
+                raise RuntimeError("invalid input: radius must be > 0")
+            self.shape, self.size = shape, int(size)
+        elif mask_type == "global":
+            if binary is None:
+                raise ValueError("binary is required for mask_type='global'")
+            b = np.ascontiguousarray(binary, dtype=np.uint8)
+            self.binary = b
+            self.ctx = ctx or default_context()
+            h = ct.c_void_p()
+            check(lib().gpv_mask_create(self.ctx.handle, ptr(b), b.shape[0], b.shape[1], ct.byref(h)),
+                  "gpv_mask_create")
+            self._h = h
+        else:
+            raise ValueError(f"unknown mask_type '{mask_type}': expected 'local' or 'global'")
+
+    @property
+    def n_px(self) -> int:
+        r = self.size
+        y, x = np.mgrid[-r:r + 1, -r:r + 1]
+        return int(np.count_nonzero(x * x + y * y <= r * r))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().gpv_mask_destroy(self._h)
+        except Exception:
+            pass
+
+
+def make_desc(coords, radius, order, p0=None) -> np.ndarray:
+    """Structured gpv_subset_desc array from centres (n, 2), radii and orders."""
+    coords = np.atleast_2d(np.asarray(coords, dtype=np.float64))
+    n = coords.shape[0]
+    d = np.zeros(n, DESC_DTYPE)
+    d["coord"] = coords
+    d["radius"] = np.broadcast_to(np.asarray(radius, dtype=np.int32), (n,))
+    d["order"] = np.broadcast_to(np.asarray(order, dtype=np.int32), (n,))
+    if p0 is not None:
+        p0 = np.atleast_2d(np.asarray(p0, dtype=np.float64))
+        d["p0"][:, :p0.shape[1]] = p0
+    return d
+
+
+def _params(max_norm, max_iterations, tolerance, eta, precision, mask, history_buf):
+    return SolveParams(max_norm=max_norm, tolerance=tolerance, max_iterations=max_iterations,
+                       flags=(SOLVE_ETA if eta else 0), precision=precision, reserved=0,
+                       mask=(mask.handle if mask is not None else None),
+                       history=(history_buf.ctypes.data if history_buf is not None else None))
+
+
+def solve_batch(f_img: Image, g_img: Image, desc, max_norm=1e-5, max_iterations=50, tolerance=0.75, eta=False,
+                precision=PREC_MIXED, global_mask: Mask | None = None, history=False):
+    """Batched Subset::new + solve_icgn_result on the GPU; returns a RESULT_DTYPE array
+    (and the (n, max_iterations, 3) history of (norm, zncc, znssd) when asked)."""
+    desc = np.ascontiguousarray(desc, dtype=DESC_DTYPE)
+    out = np.zeros(desc.size, RESULT_DTYPE)
+    hist = np.zeros((desc.size, max(max_iterations, 1), 3)) if history else None
+    prm = _params(max_norm, max_iterations, tolerance, eta, precision, global_mask, hist)
+    check(lib().gpv_solve_batch(f_img.ctx.handle, f_img.handle, g_img.handle, ptr(desc), desc.size,
+                                ct.byref(prm), ptr(out)), "gpv_solve_batch")
+    return (out, hist) if history else out
+
+
+class Subset:
+    """One subset, solved on the GPU (geopyv_dev/__init__.py:299-385,
+    python/src/py_subset.rs:159-237).  Results are read back as attributes
+    (``p``, ``c_zncc``, ``c_znssd``, ``iterations``, ``converged``,
+    ``quality_ok``, ``eta_omitted``, ``history``)."""
+
+    def __init__(self, coord, local_mask: Mask, f_img: Image, g_img: Image, subset_order: int = 1,
+                 global_mask: Mask | None = None):
+        if subset_order > 2 or subset_order < 0:
+            raise ValueError(f"subset_order must be 0, 1, or 2, got {subset_order}")
+        if not isinstance(local_mask, Mask) or local_mask.mask_type != "local":
+            raise TypeError("local_mask must be a Mask")
+        self.coord = [float(coord[0]), float(coord[1])]
+        self.local_mask, self.global_mask = local_mask, global_mask
+        self.f_img, self.g_img = f_img, g_img
+        self.subset_order = subset_order
+        self._result = None
+        self._history = None
+        self.solved = False
+
+    def solve(self, p_0=None, solver=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED):
+        if solver not in (None, "icgn"):
+            raise NotImplementedError("only solver='icgn' runs on the GPU")
+        self.solve_icgn(p_0=p_0, max_norm=max_norm, max_iterations=max_iterations, tolerance=tolerance,
+                        precision=precision)
+
+    def solve_icgn(self, p_0=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED):
+        m = {0: 2, 1: 6, 2: 12}[self.subset_order]
+        p0 = np.zeros(m)
+        if p_0 is not None:  # resized to the order's length (src/subset.rs:1134-1136)
+            v = np.asarray(p_0, dtype=np.float64).ravel()[:m]
+            p0[:v.size] = v
+        d = make_desc([self.coord], self.local_mask.size, self.subset_order, p0[None, :])
+        out, hist = solve_batch(self.f_img, self.g_img, d, max_norm=max_norm, max_iterations=max_iterations,
+                                tolerance=tolerance, eta=True, precision=precision, global_mask=self.global_mask,
+                                history=True)
+        r = out[0]
+        st = int(r["status"])
+        if st in (1, 2):  # Subset::new errors (src/subset.rs:853-892) -> RuntimeError (python/src/lib.rs:18-38)
+            raise RuntimeError("invalid input: " + ("effective mask coords is empty" if st == 1
+                                                    else "reference subset is featureless (delta_f = 0)"))
+        if st in (3, 4):  # the reference panics (src/subset.rs:520,595,1143)
+            raise RuntimeError("ICGN Hessian singular" if st == 3 else "W_delta singular")
+        self._result = r
+        k = int(r["iterations"])
+        self._history = [(i + 1, *hist[0, i]) for i in range(k)]
+        self.solved = True
+
+    def _get(self, key):
+        if self._result is None:
+            raise RuntimeError("Subset has not been solved; call solve() first")
+        return self._result[key]
+
+    @property
+    def p(self):
+        m = {0: 2, 1: 6, 2: 12}[self.subset_order]
+        return np.array(self._get("p")[:m])
+
+    c_zncc = property(lambda s: float(s._get("c_zncc")))
+    c_znssd = property(lambda s: float(s._get("c_znssd")))
+    iterations = property(lambda s: int(s._get("iterations")))
+    converged = property(lambda s: bool(s._get("converged")))
+    quality_ok = property(lambda s: bool(s._get("quality_ok")))
+    f_m = property(lambda s: float(s._get("f_m")))
+    delta_f = property(lambda s: float(s._get("delta_f")))
+    sssig = property(lambda s: float(s._get("sssig")))
+    sigma_intensity = property(lambda s: float(s._get("sigma")))
+    n_px = property(lambda s: int(s._get("n_px")))
+    history = property(lambda s: s._history)
+
+    @property
+    def eta_omitted(self):
+        r = self._result
+        return (float(r["eta_u"]), float(r["eta_v"])) if r is not None and r["has_eta"] else None

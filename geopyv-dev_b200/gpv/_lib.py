@@ -1,0 +1,108 @@
+"""ctypes binding of libgpv_b200.so (the C ABI declared in include/gpv.h).
+
+The library is built in-tree by ``geopyv-dev_b200/build.py``.  There is no
+fallback: if the shared object is missing or cannot be loaded, importing the
+package raises.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpv_b200.so")
+
+# Record layouts of include/gpv.h
+DESC_DTYPE = np.dtype([("coord", "<f8", (2,)), ("p0", "<f8", (12,)), ("order", "<i4"), ("radius", "<i4")])
+RESULT_DTYPE = np.dtype([
+    ("p", "<f8", (12,)), ("c_zncc", "<f8"), ("c_znssd", "<f8"), ("norm", "<f8"),
+    ("eta_u", "<f8"), ("eta_v", "<f8"), ("f_m", "<f8"), ("delta_f", "<f8"), ("sssig", "<f8"),
+    ("sigma", "<f8"), ("iterations", "<i4"), ("converged", "<i4"), ("quality_ok", "<i4"),
+    ("status", "<i4"), ("n_px", "<i4"), ("has_eta", "<i4"),
+])
+assert DESC_DTYPE.itemsize == 120 and RESULT_DTYPE.itemsize == 192
+
+
+class SolveParams(ct.Structure):
+    _fields_ = [("max_norm", ct.c_double), ("tolerance", ct.c_double), ("max_iterations", ct.c_int32),
+                ("flags", ct.c_int32), ("precision", ct.c_int32), ("reserved", ct.c_int32),
+                ("mask", ct.c_void_p), ("history", ct.c_void_p)]
+
+
+# enums
+GPV_U8, GPV_U16, GPV_F32, GPV_F64 = 1, 2, 3, 4
+PREC_MIXED, PREC_FP64 = 0, 1
+SOLVE_ETA, SOLVE_HISTORY = 1, 2
+IMAGE_KEEP_F64 = 1
+STATUS = {0: "OK", 1: "EMPTY_MASK", 2: "FEATURELESS", 3: "SINGULAR_H", 4: "SINGULAR_WDELTA", 5: "NONFINITE",
+          6: "TIMEOUT", 7: "CANCELLED", 8: "INVALID_SUBSET"}
+DTYPES = {np.dtype(np.uint8): GPV_U8, np.dtype(np.uint16): GPV_U16, np.dtype(np.float32): GPV_F32,
+          np.dtype(np.float64): GPV_F64}
+
+# Every entry point of include/gpv.h: name -> (restype, argtypes)
+P, I32, I64, U32, SZ, DBL = ct.c_void_p, ct.c_int32, ct.c_int64, ct.c_uint32, ct.c_size_t, ct.c_double
+SIGNATURES = {
+    "gpv_version": (ct.c_char_p, []),
+    "gpv_abi_version": (ct.c_int, []),
+    "gpv_last_error": (SZ, [ct.c_char_p, SZ]),
+    "gpv_context_create": (ct.c_int, [ct.c_int, P]),
+    "gpv_context_destroy": (ct.c_int, [P]),
+    "gpv_context_stream": (P, [P]),
+    "gpv_context_reserve": (ct.c_int, [P, I64, I32, I32]),
+    "gpv_image_create": (ct.c_int, [P, P, I32, I64, I64, I32, U32, P]),
+    "gpv_image_create_device": (ct.c_int, [P, P, I32, I64, I64, I32, U32, P]),
+    "gpv_image_update_device": (ct.c_int, [P, P, I32]),
+    "gpv_image_update": (ct.c_int, [P, P, I32]),
+    "gpv_image_destroy": (ct.c_int, [P]),
+    "gpv_image_shape": (ct.c_int, [P, P, P, P]),
+    "gpv_image_coefficients_f32": (ct.c_int, [P, P]),
+    "gpv_image_coefficients_f64": (ct.c_int, [P, P]),
+    "gpv_image_eval": (ct.c_int, [P, P, I64, I32, P, P]),
+    "gpv_mask_create": (ct.c_int, [P, P, I64, I64, P]),
+    "gpv_mask_destroy": (ct.c_int, [P]),
+    "gpv_solve_batch": (ct.c_int, [P, P, P, P, I64, P, P]),
+    "gpv_solve_batch_device": (ct.c_int, [P, P, P, P, P, I64, P, P, P]),
+    "gpv_probe_fp32_peak": (ct.c_int, [P, P]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises OSError when it is missing: no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing; build it with `python geopyv-dev_b200/build.py`")
+        L = ct.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class GpvError(RuntimeError):
+    """A failed library call (the message is gpv_last_error())."""
+
+
+def last_error() -> str:
+    buf = ct.create_string_buffer(1024)
+    lib().gpv_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != 0:
+        raise GpvError(f"{what} failed ({rc}): {last_error()}")
+
+
+def ptr(a) -> ct.c_void_p | None:
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return ct.c_void_p(a)
+    return ct.c_void_p(a.ctypes.data)

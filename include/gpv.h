@@ -1,0 +1,173 @@
+/*
+ * gpv.h -- C ABI of libgpv_b200, the B200 (sm_100a) subset-correlation
+ * library: bi-quintic B-spline prefilter + batched ICGN subset solves.
+ *
+ * Each entry point replaces a call of the reference geopyv-dev crate (Rust)
+ * on its hot path; the replaced interface is cited beside it (paths within
+ * the geopyv-dev repository).  Plain C types only; every pointer is a host
+ * pointer unless its name ends in `_dev`.  No entry point aborts: failures
+ * return a negative gpv_err and leave a message for gpv_last_error().
+ * Per-subset failures are reported in gpv_subset_result.status, never as
+ * an API error (the reference returns Err / panics per subset instead).
+ */
+#ifndef GPV_H
+#define GPV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPV_ABI_VERSION 1
+
+/* ---- API return codes -------------------------------------------------- */
+typedef enum {
+    GPV_SUCCESS = 0,
+    GPV_ERR_INVALID = -1,   /* bad argument (src/error.rs:5-40 InvalidInput) */
+    GPV_ERR_CUDA = -2,      /* CUDA runtime error                            */
+    GPV_ERR_NOMEM = -3,     /* device allocation failed / admission refused  */
+    GPV_ERR_CANCELLED = -4, /* src/error.rs Cancelled (progress observer)    */
+    GPV_ERR_TIMEOUT = -5,   /* bounded wait expired                          */
+    GPV_ERR_NOT_FOUND = -6  /* unknown request id                            */
+} gpv_err;
+
+/* ---- per-subset status (gpv_subset_result.status) ---------------------- */
+typedef enum {
+    GPV_OK = 0,
+    GPV_EMPTY_MASK = 1,       /* src/subset.rs:853-856  Err(InvalidInput)   */
+    GPV_FEATURELESS = 2,      /* src/subset.rs:888-892  Err(InvalidInput)   */
+    GPV_SINGULAR_H = 3,       /* src/subset.rs:1143     panic               */
+    GPV_SINGULAR_WDELTA = 4,  /* src/subset.rs:520,595  panic               */
+    GPV_NONFINITE = 5,        /* increment or norm not finite               */
+    GPV_TIMEOUT = 6,
+    GPV_CANCELLED = 7,
+    GPV_INVALID_SUBSET = 8    /* order not in {0,1,2} or radius < 1         */
+} gpv_status;
+
+/* ---- pixel types ------------------------------------------------------- */
+typedef enum { GPV_U8 = 1, GPV_U16 = 2, GPV_F32 = 3, GPV_F64 = 4 } gpv_dtype;
+
+/* ---- precision of the solve -------------------------------------------- */
+typedef enum {
+    GPV_PREC_MIXED = 0, /* FP32 interpolation/warp/residual, FP64 reductions,
+                           Hessian inverse and warp composition; warp per subset */
+    GPV_PREC_FP64 = 1   /* FP64 throughout, one subset per thread block      */
+} gpv_precision;
+
+/* gpv_solve_params.flags */
+#define GPV_SOLVE_ETA 1u     /* omitted-mode diagnostic (src/subset.rs:748-820) */
+#define GPV_SOLVE_HISTORY 2u /* per-iteration (norm, zncc, znssd) history       */
+
+/* gpv_image_create flags */
+#define GPV_IMAGE_KEEP_F64 1u /* also keep FP64 coefficients (needed by GPV_PREC_FP64) */
+
+typedef struct gpv_context gpv_context;
+typedef struct gpv_image gpv_image;
+typedef struct gpv_mask gpv_mask;
+typedef struct gpv_server gpv_server;
+
+/* One subset to solve (src/subset.rs:836-843 Subset::new arguments +
+ * src/subset.rs:992-999 p_0).  Layout fixed: 120 bytes. */
+typedef struct {
+    double coord[2];  /* centre [x = column, y = row]                         */
+    double p0[12];    /* initial warp; first 2/6/12 used (p_0 resize, :1134-1136) */
+    int32_t order;    /* 0, 1 or 2 (src/subset.rs:16-20)                       */
+    int32_t radius;   /* circular local mask radius (src/masks.rs:69-109)      */
+} gpv_subset_desc;
+
+/* Solver settings (src/subset.rs:992-999; python/src/py_subset.rs:217
+ * defaults max_norm=1e-3, max_iterations=50, tolerance=0.75). */
+typedef struct {
+    double max_norm;
+    double tolerance;
+    int32_t max_iterations;
+    int32_t flags;      /* GPV_SOLVE_* */
+    int32_t precision;  /* gpv_precision */
+    int32_t reserved;
+    const gpv_mask *mask; /* global mask (src/masks.rs:199-263) or NULL */
+    double *history;      /* host, n * max_iterations * 3 doubles, or NULL */
+} gpv_solve_params;
+
+/* SolveResult fields (src/subset.rs:145-191) + Subset scalars.  192 bytes. */
+typedef struct {
+    double p[12];
+    double c_zncc, c_znssd, norm;
+    double eta_u, eta_v;
+    double f_m, delta_f, sssig, sigma;
+    int32_t iterations, converged, quality_ok, status;
+    int32_t n_px, has_eta;
+} gpv_subset_result;
+
+/* ---- library ----------------------------------------------------------- */
+const char *gpv_version(void);
+int gpv_abi_version(void);
+/* Copies the calling thread's last error message; returns its length. */
+size_t gpv_last_error(char *buf, size_t len);
+
+/* ---- context: one device, one stream, reusable workspace ---------------- */
+int gpv_context_create(int device, gpv_context **out);
+int gpv_context_destroy(gpv_context *ctx);
+/* The context's CUDA stream, as a cudaStream_t cast to void*. */
+void *gpv_context_stream(gpv_context *ctx);
+/* Pre-size the solve workspace so that later solves of up to n_subsets
+ * subsets of radius <= max_radius allocate nothing (graph-capturable). */
+int gpv_context_reserve(gpv_context *ctx, int64_t n_subsets, int32_t max_radius, int32_t max_iterations);
+
+/* ---- image: device-resident coefficients --------------------------------
+ * Replaces Image::from_array(image_gs, border) -> get_c
+ * (src/image.rs:83-86, :252-327; python/src/py_image.rs:42-64).
+ * px: host pixels (h, w) row-major of `dtype`; border >= 3 (default 20). */
+int gpv_image_create(gpv_context *ctx, const void *px, int32_t dtype, int64_t h, int64_t w, int32_t border,
+                     uint32_t flags, gpv_image **out);
+/* Same, pixels already on the device (async on the context stream). */
+int gpv_image_create_device(gpv_context *ctx, const void *px_dev, int32_t dtype, int64_t h, int64_t w,
+                            int32_t border, uint32_t flags, gpv_image **out);
+/* Re-prefilter new pixels of the same shape into an existing image
+ * (sequence frames: src/sequence.rs:693-694,914), no allocation. */
+int gpv_image_update_device(gpv_image *img, const void *px_dev, int32_t dtype);
+/* Same from host pixels (copied through the image's staging buffer; fast
+ * when px is page-locked).  Synchronous. */
+int gpv_image_update(gpv_image *img, const void *px, int32_t dtype);
+int gpv_image_destroy(gpv_image *img);
+int gpv_image_shape(const gpv_image *img, int64_t *h, int64_t *w, int32_t *border);
+/* Download coefficients C (h+2b, w+2b) row-major: FP32 always, FP64 if kept. */
+int gpv_image_coefficients_f32(const gpv_image *img, float *out);
+int gpv_image_coefficients_f64(const gpv_image *img, double *out);
+/* Value (+ gradient) of the spline at n points (x, y) -- Image::eval /
+ * Image::eval_grad (src/image.rs:115-178), evaluated on the device in the
+ * given precision.  grad may be NULL. */
+int gpv_image_eval(const gpv_image *img, const double *xy, int64_t n, int32_t precision, double *val,
+                   double *grad);
+
+/* ---- global mask: LocalMask::mask_update (src/masks.rs:199-263) --------- */
+int gpv_mask_create(gpv_context *ctx, const uint8_t *mask, int64_t h, int64_t w, gpv_mask **out);
+int gpv_mask_destroy(gpv_mask *m);
+
+/* ---- batched subset solve ----------------------------------------------
+ * Replaces, per subset, Subset::new + Subset::solve_icgn_result
+ * (src/subset.rs:836-919, :1117-1219) as called from
+ * Mesh::solve_one_with_tolerance (src/mesh.rs:1025-1040) and
+ * PySubset::solve_icgn (python/src/py_subset.rs:217-237).
+ * Host arrays in and out; synchronous. */
+int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc,
+                    int64_t n, const gpv_solve_params *params, gpv_subset_result *out);
+/* Device arrays in and out, asynchronous on `stream` (a cudaStream_t, or
+ * NULL for the context stream).  work_order_dev (optional, int32[n]) is the
+ * order in which subsets are taken from the work queue (largest first is
+ * best); history (params->history) must then be a device pointer or NULL.
+ * Allocates nothing once gpv_context_reserve covers the call. */
+int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image *g,
+                           const gpv_subset_desc *desc_dev, const int32_t *work_order_dev, int64_t n,
+                           const gpv_solve_params *params, gpv_subset_result *out_dev, void *stream);
+
+/* ---- calibration (no counterpart in the reference) ----------------------
+ * Measured FP32 FMA throughput of this device (TFLOP/s, 2 FLOP per FMA) from
+ * a register-only FMA kernel: the denominator of the interpolation roofline. */
+int gpv_probe_fp32_peak(gpv_context *ctx, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPV_H */
