@@ -86,6 +86,11 @@ __device__ __forceinline__ T mu_val(int mu, T dx, T dy) {
     }
 }
 
+// Flatness (Subset::new, src/subset.rs:888-892, rejects delta_f == 0): the
+// prefilter's rounding leaves an exactly flat subset with delta_f ~ 1e-12 (FP64)
+// or ~1e-4 (FP32) instead of 0, so a subset is featureless when
+// sigma_f = delta_f / sqrt(n) <= 1e-6 max(1, |f_m|) -- in the oracle too.
+
 // Global-mask test of LocalMask::mask_update (src/masks.rs:199-263): the
 // template pixel maps to image pixel trunc(centre) + offset; the extracted
 // window always stops one short of the last mask row / column.
@@ -491,7 +496,7 @@ __device__ void mixed_subset(const KArgs &A, int idx, const gpv_subset_desc &d, 
         if (lane == 0) { sm.A[j] = av; sm.S[j] = sv; }
     }
     const double df = sqrt(saa);
-    if (df == 0.0) {
+    if (!(sqrt(saa / dn) > 1e-6 * fmax(1.0, fabs(fm)))) {  // flat subset (see featureless_test)
         if (lane == 0) write_failed(A, idx, d, M, GPV_FEATURELESS, n, fm, df);
         return;
     }
@@ -865,7 +870,7 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
     }
     ss = block_sum1(ss, sm);
     const double df = sqrt(ss);
-    if (df == 0.0) {
+    if (!(sqrt(ss / dn) > 1e-6 * fmax(1.0, fabs(fm)))) {  // flat subset
         if (tid == 0) write_failed(A, idx, d, M, GPV_FEATURELESS, n, fm, df);
         return;
     }

@@ -3,10 +3,13 @@ workloads (the generator model is stated in csrc/synth.c).
 
     C1  1024^2 u8, rigid (0.35, -0.20) px, r=25 on a 20 px grid, order 1
     C2  4096^2 u16 (12-bit, x16), 1% uniaxial strain + 0.5 deg rotation +
-        1e-6 px^-1 quadratic, r=30 on a 10 px grid, order 2
+        1e-6 px^-1 quadratic, r=30 on a 10 px grid, order 2, p0 = field
+        translation +- 0.3 px and field gradient (a neighbour preconditioner's
+        seed; the displacement reaches ~30 px at the corners)
     C3  2048^2 u8, u = 2 tanh((y-1024)/40) + 0.2% background strain, 50k
         centres (coarse grid refined x4 within 150 px of the band), radii
-        log-uniform in [15, 60], orders 1/2 70/30, p0 = field +- 0.3 px
+        log-uniform in [15, 60], orders 1/2 70/30, p0 = field translation
+        +- 0.3 px and field gradient
     C4  2048^2 u8 frames, simple shear rising linearly to 5% by frame 200,
         20k subsets r=25, seeded from the previous frame
     C5  Poisson request stream (see gpv.serve)
@@ -91,6 +94,29 @@ def displacement(field: Field, xy) -> np.ndarray:
     return out
 
 
+def gradient(field: Field, xy) -> np.ndarray:
+    """Analytic displacement gradient [du/dx, dv/dx, du/dy, dv/dy] at points (warp slots 2..5)."""
+    xy = np.atleast_2d(np.asarray(xy, dtype=np.float64))
+    dx, dy = xy[:, 0] - field.xc, xy[:, 1] - field.yc
+    a, q = list(field.a), list(field.q)
+    ux = a[0] + 2 * q[0] * dx + q[1] * dy
+    uy = a[1] + q[1] * dx + 2 * q[2] * dy
+    vx = a[2] + 2 * q[3] * dx + q[4] * dy
+    vy = a[3] + q[4] * dx + 2 * q[5] * dy
+    if field.band_w != 0.0:
+        uy = uy + field.band_amp / field.band_w / np.cosh((xy[:, 1] - field.band_y) / field.band_w) ** 2
+    return np.stack([ux, vx, uy, vy], 1)
+
+
+def seeded_p0(field: Field, xy, rng, jitter=0.3) -> np.ndarray:
+    """Initial warps as a neighbour-based preconditioner would give them: the
+    field's translation perturbed by +-jitter px, and its gradient."""
+    p0 = np.zeros((len(xy), 12))
+    p0[:, :2] = displacement(field, xy) + rng.uniform(-jitter, jitter, (len(xy), 2))
+    p0[:, 2:6] = gradient(field, xy)
+    return p0
+
+
 def pair(h, w, field: Field, seed, dtype=np.uint8, scale=1.0, sigma=2.0):
     """(reference, target) quantised images of one seeded speckle pair."""
     r0 = speckle(h, w, seed, scale)
@@ -138,7 +164,7 @@ def workload(config: int, scale_down: int = 1, seed_frame: int = 0):
         xy = grid(n, n, 10, r + 3 + 0.012 * n)
         order = np.full(len(xy), 2, np.int32)
         radius = np.full(len(xy), r, np.int32)
-        p0 = np.zeros((len(xy), 12))
+        p0 = seeded_p0(fld, xy, np.random.default_rng(seed))
         name = f"C2 affine+quadratic {n}x{n} u16 r=30 grid10 order2"
     elif config == 3:
         n = 2048 // scale_down
@@ -156,9 +182,7 @@ def workload(config: int, scale_down: int = 1, seed_frame: int = 0):
             xy = xy[np.sort(rng.choice(len(xy), target, replace=False))]
         radius = np.exp(rng.uniform(math.log(15), math.log(60), len(xy))).round().astype(np.int32)
         order = np.where(rng.uniform(size=len(xy)) < 0.7, 1, 2).astype(np.int32)
-        uv = displacement(fld, xy)
-        p0 = np.zeros((len(xy), 12))
-        p0[:, :2] = uv + rng.uniform(-0.3, 0.3, (len(xy), 2))
+        p0 = seeded_p0(fld, xy, rng)
         name = f"C3 shear band {n}x{n} u8 r=15..60 mixed order"
     elif config == 4:
         n = 2048 // scale_down

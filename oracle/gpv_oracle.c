@@ -616,7 +616,11 @@ static int subset_new(const spline *F, const double coord[2], int64_t radius, co
     double ss = 0.0;
     for (int64_t i = 0; i < n; i++) ss += (s->f[i] - s->f_m) * (s->f[i] - s->f_m);
     s->delta_f = sqrt(ss);
-    if (s->delta_f == 0.0) return ST_FEATURELESS;
+    /* Subset::new rejects delta_f == 0 (src/subset.rs:888-892).  The FFT
+     * prefilter leaves an exactly flat subset with delta_f ~ 1e-12 instead of
+     * 0, so flatness is tested as sigma_f <= 1e-6 max(1, |f_m|) -- the same
+     * test in every implementation of this library. */
+    if (!(sqrt(ss / (double)n) > 1e-6 * fmax(1.0, fabs(s->f_m)))) return ST_FEATURELESS;
     double sg = 0.0;
     for (int64_t i = 0; i < n; i++) sg += 0.5 * (s->grad[2 * i] * s->grad[2 * i] + s->grad[2 * i + 1] * s->grad[2 * i + 1]);
     s->sssig = sg;

@@ -8,7 +8,7 @@ seeded synthetic speckle pairs:
   * mixed form (FP32 interpolation): displacement within 1e-3 px and
     strain terms within 1e-5 (the stated parity bar), ZNCC within 1e-5,
     identical converged / quality flags; iteration counts may differ by one
-    on at most 2% of subsets (a borderline norm near max_norm).
+    on at most 2% of subsets (at least one) -- a borderline norm near max_norm.
 """
 import numpy as np
 import pytest
@@ -32,7 +32,6 @@ def _desc(gpv_mod, W):
 
 
 def _compare(res, ref, exact, label):
-    m = ref["order"] if "order" in ref.dtype.names else None
     ok = (ref["status"] == 0)
     assert np.array_equal(res["status"], ref["status"]), label
     assert np.array_equal(res["n_px"], ref["n_px"]), label
@@ -47,7 +46,7 @@ def _compare(res, ref, exact, label):
         assert dp[ok][:, 2:6].max() <= 1e-5, label
         assert np.abs(res["c_zncc"] - ref["c_zncc"])[ok].max() < 1e-5, label
         it_diff = np.abs(res["iterations"].astype(int) - ref["iterations"])
-        assert it_diff.max() <= 1 and (it_diff > 0).mean() <= 0.02, label
+        assert it_diff.max() <= 1 and (it_diff > 0).sum() <= max(1, int(np.ceil(0.02 * len(it_diff)))), label
     assert np.array_equal(res["converged"], ref["converged"]), label
     assert np.array_equal(res["quality_ok"], ref["quality_ok"]), label
 
@@ -135,6 +134,8 @@ def test_failure_statuses(oracle, gpv_mod):
     flat = np.full((80, 80), 90, np.uint8)
     F = gpv_mod.Image(image_gs=flat, border=BORDER, keep_f64=True)
     d = gpv_mod.make_desc([[40.0, 40.0]], 10, 1)
+    C = oracle.get_c(flat.astype(np.float64), BORDER)
+    assert oracle.solve_batch(C, C, flat.shape, BORDER, d)["status"][0] == 2
     for prec in (gpv_mod.PREC_FP64, gpv_mod.PREC_MIXED):
         r = gpv_mod.solve_batch(F, F, d, precision=prec)
         assert r["status"][0] == 2 and r["quality_ok"][0] == 0  # FEATURELESS
