@@ -126,6 +126,8 @@ int gpv_context_create(int device, gpv_context **out) {
     ctx->device = device;
     cudaError_t e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) e = cudaStreamCreateWithFlags(&ctx->aux[k], cudaStreamNonBlocking);
+    for (int k = 0; k < 3 && e == cudaSuccess; k++) e = cudaEventCreateWithFlags(&ctx->ev[k], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         set_error(std::string("context: ") + cudaGetErrorString(e));
         delete ctx;
@@ -140,8 +142,12 @@ int gpv_context_destroy(gpv_context *ctx) {
     DeviceGuard dg(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->offs, &ctx->tab_off, &ctx->tab_n, &ctx->scratch, &ctx->queue, &ctx->desc_dev, &ctx->out_dev,
-                      &ctx->order_dev, &ctx->hist_dev, &ctx->eval_dev})
+                      &ctx->order_dev, &ctx->hist_dev, &ctx->eval_dev, &ctx->tile_ws})
         b->release();
+    for (int k = 0; k < 2; k++)
+        if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
+    for (int k = 0; k < 3; k++)
+        if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GPV_SUCCESS;
@@ -347,6 +353,7 @@ int gpv_context_reserve(gpv_context *ctx, int64_t n_subsets, int32_t max_radius,
     if (int rc = ctx->desc_dev.ensure(sizeof(gpv_subset_desc) * (size_t)n_subsets)) return rc;
     if (int rc = ctx->out_dev.ensure(sizeof(gpv_subset_result) * (size_t)n_subsets)) return rc;
     if (int rc = ctx->order_dev.ensure(sizeof(int32_t) * (size_t)n_subsets)) return rc;
+    if (int rc = ctx->tile_ws.ensure(sizeof(int32_t) * (32 + (size_t)n_subsets))) return rc;
     (void)max_iterations;
     return GPV_SUCCESS;
 }

@@ -1,0 +1,743 @@
+// icgn_tile.cu -- mixed-precision ICGN, one thread block per subset, the
+// subset's coefficient window staged in shared memory.
+//
+// Same algorithm and numerics as the warp-per-subset kernel (icgn.cu) --
+// Subset::new + solve_icgn_result, src/subset.rs:836-919, 1117-1219 -- with
+// a different execution layout:
+//  * 4 warps solve one subset; pixels are dealt round-robin in the row-major
+//    order of the circular template, so each warp covers 32 neighbouring
+//    pixels of a template row and the 6x6 windows of its lanes overlap.
+//  * The block of coefficients the subset can touch is copied once into
+//    shared memory with 16-byte vector loads (f's window for the setup, g's
+//    for the iterations) with a margin of kMargin px.  Every iteration checks
+//    (from the warp parameters, conservatively) that the warped subset still
+//    lies inside the staged block and re-stages when it does not; a subset
+//    whose block exceeds the shared-memory capacity reads global memory for
+//    that iteration.  Window indices are clamped, so no access can leave the
+//    staged block whatever the warp.
+//  * One kernel per warp order (fewer registers, smaller code); the batch is
+//    partitioned by order on the device and the three kernels run on three
+//    streams so each one's tail overlaps the next one's start.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+
+#include "icgn_common.cuh"
+
+namespace gpv {
+namespace {
+
+constexpr int kMaxTileWarps = 8;  // blocks of 128 or 256 threads
+constexpr int kMargin = 4;
+
+struct TileSmem {
+    double mom[3 * 15];
+    double H[144];
+    double Hinv[144];
+    double aug[288];
+    double A[12], S[12];
+    double p[12], pprev[12], dp[12], grad[12];
+    double red[kMaxTileWarps][16];
+    double tot[16];
+    double misc[8];
+    int flag[4];
+    int item;
+    int win_r0, win_c0, win_h, win_w, win_ok;
+};
+
+struct TileArgs {
+    KArgs k;
+    const int32_t *seg;  // [start, count] of this order's segment in k.order
+    int *queue;          // this kernel's work-queue counter
+    int win_cap;         // floats of dynamic shared memory for the window
+};
+
+// Copy coefficient rows [r0, r0+wh) x cols [c0, c0+ww) (c0, ww multiples of 4)
+// into win (row pitch ww).  Out-of-range rows / columns are clamped.
+template <int NT>
+__device__ __forceinline__ void stage(const float *__restrict__ C, int64_t pitch, int ch, int r0, int c0, int wh,
+                                      int ww, float *win) {
+    const int nv = ww >> 2;
+    for (int idx = threadIdx.x; idx < wh * nv; idx += NT) {
+        const int rr = idx / nv, cc = (idx - rr * nv) << 2;
+        int row = r0 + rr;
+        row = row < 0 ? 0 : (row > ch - 1 ? ch - 1 : row);
+        int col = c0 + cc;
+        col = col < 0 ? 0 : (col > (int)pitch - 4 ? (int)pitch - 4 : col);
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(C + (int64_t)row * pitch + col));
+        *reinterpret_cast<float4 *>(win + rr * ww + cc) = v;
+    }
+}
+
+// Plan a window covering pixel indices [xlo, xhi] x [ylo, yhi] (already
+// clamped to the image) plus kMargin; returns false if it does not fit.
+__device__ __forceinline__ bool plan_window(int xlo, int xhi, int ylo, int yhi, int border, int cap, int &r0, int &c0,
+                                            int &wh, int &ww) {
+    for (int m = kMargin; m >= 0; m -= kMargin) {
+        const int clo = xlo + border - 2 - m, chi = xhi + border + 3 + m;
+        c0 = clo >= 0 ? (clo & ~3) : -(((-clo) + 3) & ~3);
+        ww = ((chi + 1 - c0) + 3) & ~3;
+        r0 = ylo + border - 2 - m;
+        wh = yhi + border + 3 + m + 1 - r0;
+        if (ww * wh <= cap) return true;
+        if (m == 0) break;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool window_covers(const TileSmem &sm, int xlo, int xhi, int ylo, int yhi, int border) {
+    if (!sm.win_ok) return false;
+    return xlo + border - 2 >= sm.win_c0 && xhi + border + 3 < sm.win_c0 + sm.win_w && ylo + border - 2 >= sm.win_r0 &&
+           yhi + border + 3 < sm.win_r0 + sm.win_h;
+}
+
+// Sum K per-thread values over the block into sm.tot[0..K) (FP64).
+template <int NT, int K>
+__device__ __forceinline__ void block_reduce(const double (&v)[K], TileSmem &sm) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const double s = warp_sum(v[k]);
+        if (lane == 0) sm.red[wid][k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < NT / 32; w++) s += sm.red[w][threadIdx.x];
+        sm.tot[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+template <int NT>
+__device__ __forceinline__ double block_sum1(double v, TileSmem &sm) {
+    const double a[1] = {v};
+    block_reduce<NT, 1>(a, sm);
+    return sm.tot[0];
+}
+
+// Pixel extent (in image pixels, clamped) touched by the warp p of a radius-r
+// subset centred at (cx, cy), conservatively.
+template <int ORDER>
+__device__ void warp_extent(const double *p, double cx, double cy, int r, int w, int h, int &xlo, int &xhi, int &ylo,
+                            int &yhi) {
+    double ex = r, ey = r;
+    if (ORDER >= 1) {
+        ex = r * (fabs(1.0 + p[2]) + fabs(p[4]));
+        ey = r * (fabs(p[3]) + fabs(1.0 + p[5]));
+    }
+    if (ORDER == 2) {
+        const double rr = 0.5 * (double)r * r;
+        ex += rr * (fabs(p[6 % 12]) + 2.0 * fabs(p[8 % 12]) + fabs(p[10 % 12]));
+        ey += rr * (fabs(p[7 % 12]) + 2.0 * fabs(p[9 % 12]) + fabs(p[11 % 12]));
+    }
+    const double X0 = cx + p[0], Y0 = cy + p[1];
+    double a = floor(X0 - ex) - 1.0, b = floor(X0 + ex) + 1.0, c = floor(Y0 - ey) - 1.0, d = floor(Y0 + ey) + 1.0;
+    if (!(isfinite(a) && isfinite(b) && isfinite(c) && isfinite(d))) {
+        xlo = 0; xhi = w - 1; ylo = 0; yhi = h - 1;  // plans a window that cannot fit: global path
+        return;
+    }
+    xlo = (int)fmax(0.0, fmin(a, (double)(w - 1)));
+    xhi = (int)fmax(0.0, fmin(b, (double)(w - 1)));
+    ylo = (int)fmax(0.0, fmin(c, (double)(h - 1)));
+    yhi = (int)fmax(0.0, fmin(d, (double)(h - 1)));
+}
+
+// Per-pixel record kept between the setup and the iterations: f, df/dx,
+// df/dy and the template offset (dx, dy) packed as two int16 in the last
+// word.  f = NaN marks a pixel removed by the global mask.
+__device__ __forceinline__ float4 pack_px(float f, float gx, float gy, int dx, int dy) {
+    return make_float4(f, gx, gy, __int_as_float((dx & 0xffff) | (dy << 16)));
+}
+__device__ __forceinline__ void unpack_off(float w, float &dx, float &dy) {
+    const int v = __float_as_int(w);
+    dx = (float)(int)(short)(v & 0xffff);
+    dy = (float)(v >> 16);
+}
+
+template <int ORDER, int NT>
+__device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d, float4 *S4, float *Sg, float *win,
+                            TileSmem &sm) {
+    const KArgs &A = T.k;
+    using O = Ord<ORDER>;
+    constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int r = d.radius;
+    const int npx_t = A.tab_n[r];
+    const short2 *po = A.offs + A.tab_off[r];
+    const double cx = d.coord[0], cy = d.coord[1];
+    const int cxi = (int)cx, cyi = (int)cy;
+    const double fxd = floor(cx), fyd = floor(cy);
+    const int bx = (int)fxd, by = (int)fyd;
+    const float fx = (float)(cx - fxd), fy = (float)(cy - fyd);
+    const int B = A.border, ch = A.h + 2 * B;
+
+    // ---- stage f's window ------------------------------------------------
+    {
+        // +-1: an FP32 fraction can round up to the next integer
+        const int xlo = max(0, min(bx - r - 1, A.w - 1)), xhi = max(0, min(bx + r + 1, A.w - 1));
+        const int ylo = max(0, min(by - r - 1, A.h - 1)), yhi = max(0, min(by + r + 1, A.h - 1));
+        int r0, c0, wh, ww;
+        const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, r0, c0, wh, ww);
+        if (ok) stage<NT>(A.f32, A.pitch32, ch, r0, c0, wh, ww, win);
+        if (tid == 0) {
+            sm.win_ok = 0;  // g must be staged before the iterations
+            sm.win_r0 = r0; sm.win_c0 = c0; sm.win_h = wh; sm.win_w = ww;
+            sm.flag[2] = ok;
+        }
+        __syncthreads();
+    }
+    const bool f_staged = sm.flag[2] != 0;
+    const int fr0 = sm.win_r0, fc0 = sm.win_c0, fwh = sm.win_h, fww = sm.win_w;
+    // interior subset: every template pixel sits at integer offsets from
+    // (cx, cy) inside the image, so all share one fraction and one basis
+    const bool interior = f_staged && bx - r >= 0 && bx + r <= A.w - 1 && by - r >= 0 && by + r <= A.h - 1;
+
+    // ---- setup pass 1: f, grad f, sum f, SSSIG --------------------------
+    double sum_f = 0.0, sssig = 0.0, cnt = 0.0;
+    {
+        float a0[6], da0[6], b0[6], db0[6];
+        basis(fy, a0); dbasis(fy, da0);
+        basis(fx, b0); dbasis(fx, db0);
+        for (int i = tid; i < npx_t; i += NT) {
+            const short2 o = po[i];
+            if (!mask_ok(A, cxi, cyi, o.x, o.y)) {
+                S4[i] = pack_px(__int_as_float(0x7fc00000), 0.f, 0.f, o.x, o.y);
+                continue;
+            }
+            float gx, gy, f;
+            if (interior) {
+                const int wx = bx + o.x + B - 2 - fc0, wy = by + o.y + B - 2 - fr0;
+                f = contract_grad<float>(win + wy * fww + wx, fww, a0, da0, b0, db0, gx, gy);
+            } else {
+                int ix, iy;
+                float tx, ty;
+                split_clamped(bx, fx + (float)o.x, A.w, ix, tx);
+                split_clamped(by, fy + (float)o.y, A.h, iy, ty);
+                float a[6], da[6], b[6], db[6];
+                basis(ty, a); dbasis(ty, da);
+                basis(tx, b); dbasis(tx, db);
+                if (f_staged) {
+                    const int wx = min(max(ix + B - 2 - fc0, 0), fww - 6), wy = min(max(iy + B - 2 - fr0, 0), fwh - 6);
+                    f = contract_grad<float>(win + wy * fww + wx, fww, a, da, b, db, gx, gy);
+                } else {
+                    const float *F = A.f32 + (int64_t)(iy + B - 2) * A.pitch32 + (ix + B - 2);
+                    f = contract_grad<float>(F, A.pitch32, a, da, b, db, gx, gy);
+                }
+            }
+            S4[i] = pack_px(f, gx, gy, o.x, o.y);
+            sum_f += (double)f;
+            sssig += 0.5 * ((double)gx * gx + (double)gy * gy);
+            cnt += 1.0;
+        }
+    }
+    {
+        const double v[3] = {sum_f, sssig, cnt};
+        block_reduce<NT, 3>(v, sm);
+    }
+    const double tot_f = sm.tot[0], tot_sssig = sm.tot[1];
+    const int n = (int)sm.tot[2];
+    if (n == 0) {
+        if (tid == 0) write_failed(A, idx, d, M, GPV_EMPTY_MASK, 0, 0.0, 0.0);
+        return;
+    }
+    const double dn = (double)n;
+    const double fm = tot_f / dn;
+    const float fmf = (float)fm;
+
+    // ---- setup pass 1b: gradient moments (Hessian) -------------------------
+    {
+        float mom[3][NMOM];
+#pragma unroll
+        for (int p = 0; p < 3; p++)
+#pragma unroll
+            for (int q = 0; q < NMOM; q++) mom[p][q] = 0.f;
+        for (int i = tid; i < npx_t; i += NT) {
+            const float4 rec = S4[i];
+            if (rec.x != rec.x) continue;
+            float dx, dy;
+            unpack_off(rec.w, dx, dy);
+            const float gx = rec.y, gy = rec.z;
+            float pxp[5], pyp[5];
+            pxp[0] = 1.f; pyp[0] = 1.f;
+#pragma unroll
+            for (int e = 1; e <= 2 * O::DEG; e++) { pxp[e] = pxp[e - 1] * dx; pyp[e] = pyp[e - 1] * dy; }
+            const float gg[3] = {gx * gx, gx * gy, gy * gy};
+#pragma unroll
+            for (int dgr = 0; dgr <= 2 * O::DEG; dgr++)
+#pragma unroll
+                for (int bb = 0; bb <= dgr; bb++) {
+                    const float mono = pxp[dgr - bb] * pyp[bb];
+#pragma unroll
+                    for (int p = 0; p < 3; p++)
+                        mom[p][mom_idx(dgr - bb, bb)] = fmaf(gg[p], mono, mom[p][mom_idx(dgr - bb, bb)]);
+                }
+        }
+#pragma unroll
+        for (int q0 = 0; q0 < 3 * NMOM; q0 += 15) {
+            double v[15];
+#pragma unroll
+            for (int j = 0; j < 15; j++) {
+                const int q = q0 + j;
+                v[j] = q < 3 * NMOM ? (double)mom[q / NMOM][q % NMOM] : 0.0;
+            }
+            block_reduce<NT, 15>(v, sm);
+            if (tid < 15 && q0 + tid < 3 * NMOM) sm.mom[q0 + tid] = sm.tot[tid];
+        }
+    }
+
+    // ---- setup pass 2: delta_f, A_j, S_j --------------------------------
+    double sa, saa;
+    {
+        double acc[2 + 2 * M];
+#pragma unroll
+        for (int j = 0; j < 2 + 2 * M; j++) acc[j] = 0.0;
+        for (int i = tid; i < npx_t; i += NT) {
+            const float4 rec = S4[i];
+            if (rec.x != rec.x) continue;
+            float dxf, dyf;
+            unpack_off(rec.w, dxf, dyf);
+            const double a = (double)rec.x - fm;
+            const double gx = rec.y, gy = rec.z, dx = dxf, dy = dyf;
+            acc[0] += a;
+            acc[1] += a * a;
+#pragma unroll
+            for (int mu = 0; mu < NMU; mu++) {
+                const double mv = mu_val<double>(mu, dx, dy);
+                acc[2 + 2 * mu] += gx * mv * a;
+                acc[3 + 2 * mu] += gy * mv * a;
+                acc[2 + M + 2 * mu] += gx * mv;
+                acc[3 + M + 2 * mu] += gy * mv;
+            }
+        }
+        constexpr int K1 = (2 + 2 * M + 1) / 2, K2 = 2 + 2 * M - K1;
+        double v1[K1], v2[K2];
+#pragma unroll
+        for (int j = 0; j < K1; j++) v1[j] = acc[j];
+#pragma unroll
+        for (int j = 0; j < K2; j++) v2[j] = acc[K1 + j];
+        block_reduce<NT, K1>(v1, sm);
+        double *dst = sm.aug;  // scratch until the Hessian is inverted
+        if (tid < K1) dst[tid] = sm.tot[tid];
+        block_reduce<NT, K2>(v2, sm);
+        if (tid < K2) dst[K1 + tid] = sm.tot[tid];
+        __syncthreads();
+        sa = dst[0];
+        saa = dst[1];
+        if (tid < M) {
+            sm.A[tid] = dst[2 + tid];
+            sm.S[tid] = dst[2 + M + tid];
+        }
+        __syncthreads();
+    }
+    const double df = sqrt(saa);
+    if (!(sqrt(saa / dn) > 1e-6 * fmax(1.0, fabs(fm)))) {  // flat subset
+        if (tid == 0) write_failed(A, idx, d, M, GPV_FEATURELESS, n, fm, df);
+        return;
+    }
+    if (wid == 0) {
+        assemble_hessian<ORDER>(sm.mom, sm.H, lane);
+        const bool ok = spd_inverse_warp<M>(sm.H, sm.aug, sm.Hinv, lane);
+        if (lane == 0) sm.flag[0] = ok;
+    }
+    __syncthreads();
+    if (!sm.flag[0]) {
+        if (tid == 0) {
+            write_failed(A, idx, d, M, GPV_SINGULAR_H, n, fm, df);
+            A.out[idx].sssig = tot_sssig;
+            A.out[idx].sigma = sqrt(saa / dn);
+        }
+        return;
+    }
+
+    // ---- ICGN iterations --------------------------------------------------
+    const double size = sqrt(dn);
+    if (tid < M) {
+        sm.p[tid] = d.p0[tid];
+        sm.pprev[tid] = d.p0[tid];
+    }
+    __syncthreads();
+    int iters = 0, status = GPV_OK;
+    bool converged = false;
+    double c_zncc = 0.0, c_znssd = 4.0, last_norm = 0.0, gm_last = 0.0, dg_last = 0.0;
+    for (int it = 1; it <= A.max_iter; it++) {
+        // (re)stage g's window when the warped subset has left it
+        {
+            int xlo, xhi, ylo, yhi;
+            warp_extent<ORDER>(sm.p, cx, cy, r, A.w, A.h, xlo, xhi, ylo, yhi);
+            if (!window_covers(sm, xlo, xhi, ylo, yhi, B)) {
+                int r0, c0, wh, ww;
+                const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, r0, c0, wh, ww);
+                __syncthreads();  // nobody still reads the old window
+                if (ok) stage<NT>(A.g32, A.pitch32, ch, r0, c0, wh, ww, win);
+                if (tid == 0) {
+                    sm.win_ok = ok;
+                    sm.win_r0 = r0; sm.win_c0 = c0; sm.win_h = wh; sm.win_w = ww;
+                }
+                __syncthreads();
+            }
+        }
+        const bool staged = sm.win_ok != 0;
+        const int gr0 = sm.win_r0, gc0 = sm.win_c0, gwh = sm.win_h, gww = sm.win_w;
+        const double X0 = cx + sm.p[0], Y0 = cy + sm.p[1];
+        const double bxd = floor(X0), byd = floor(Y0);
+        const int wbx = (int)bxd, wby = (int)byd;
+        const float ox = (float)(X0 - bxd), oy = (float)(Y0 - byd);
+        float ux = 0.f, uy = 0.f, vx = 0.f, vy = 0.f, uxx = 0.f, uxy = 0.f, uyy = 0.f, vxx = 0.f, vxy = 0.f, vyy = 0.f;
+        if (ORDER >= 1) { ux = (float)sm.p[2]; vx = (float)sm.p[3]; uy = (float)sm.p[4]; vy = (float)sm.p[5]; }
+        if (ORDER == 2) {
+            uxx = (float)(0.5 * sm.p[6 % M]); vxx = (float)(0.5 * sm.p[7 % M]); uxy = (float)sm.p[8 % M];
+            vxy = (float)sm.p[9 % M]; uyy = (float)(0.5 * sm.p[10 % M]); vyy = (float)(0.5 * sm.p[11 % M]);
+        }
+        // window-relative base: sample (ix, iy) reads win[(iy + B-2 - r0) * ww + (ix + B-2 - c0)]
+        const int offx = B - 2 - gc0, offy = B - 2 - gr0;
+        double s1 = 0.0, s2 = 0.0, sfg = 0.0;
+        float pb[M];
+#pragma unroll
+        for (int j = 0; j < M; j++) pb[j] = 0.f;
+        for (int base = 0; base < npx_t; base += NT * kChunk) {
+            float p1 = 0.f, p2 = 0.f, pfg = 0.f;
+#pragma unroll 2
+            for (int c = 0; c < kChunk; c++) {
+                const int i = base + c * NT + tid;
+                if (i < npx_t) {
+                    const float4 rec = S4[i];
+                    const float fv = rec.x;
+                    if (fv == fv) {
+                        float dx, dy;
+                        unpack_off(rec.w, dx, dy);
+                        float lx = fmaf(uy, dy, fmaf(ux, dx, ox)) + dx;
+                        float ly = fmaf(vy, dy, fmaf(vx, dx, oy)) + dy;
+                        float dxx = 0.f, dxy = 0.f, dyy = 0.f;
+                        if (ORDER == 2) {
+                            dxx = dx * dx; dxy = dx * dy; dyy = dy * dy;
+                            lx += fmaf(uxx, dxx, fmaf(uxy, dxy, uyy * dyy));
+                            ly += fmaf(vxx, dxx, fmaf(vxy, dxy, vyy * dyy));
+                        }
+                        int ix, iy;
+                        float tx, ty;
+                        split_clamped(wbx, lx, A.w, ix, tx);
+                        split_clamped(wby, ly, A.h, iy, ty);
+                        float a[6], b[6];
+                        basis(ty, a);
+                        basis(tx, b);
+                        float g;
+                        if (staged) {
+                            const int wx = min(max(ix + offx, 0), gww - 6), wy = min(max(iy + offy, 0), gwh - 6);
+                            g = contract<float>(win + wy * gww + wx, gww, a, b);
+                        } else {
+                            g = contract<float>(A.g32 + (int64_t)(iy + B - 2) * A.pitch32 + (ix + B - 2), A.pitch32, a, b);
+                        }
+                        const float gc = g - fmf;
+                        p1 += gc;
+                        p2 = fmaf(gc, gc, p2);
+                        pfg = fmaf(fv - fmf, gc, pfg);
+                        const float gxg = rec.y * gc, gyg = rec.z * gc;
+                        pb[0] += gxg;
+                        pb[1] += gyg;
+                        if (ORDER >= 1) {
+                            pb[2 % M] = fmaf(gxg, dx, pb[2 % M]); pb[3 % M] = fmaf(gyg, dx, pb[3 % M]);
+                            pb[4 % M] = fmaf(gxg, dy, pb[4 % M]); pb[5 % M] = fmaf(gyg, dy, pb[5 % M]);
+                        }
+                        if (ORDER == 2) {
+                            const float hxx = 0.5f * dxx, hyy = 0.5f * dyy;
+                            pb[6 % M] = fmaf(gxg, hxx, pb[6 % M]); pb[7 % M] = fmaf(gyg, hxx, pb[7 % M]);
+                            pb[8 % M] = fmaf(gxg, dxy, pb[8 % M]); pb[9 % M] = fmaf(gyg, dxy, pb[9 % M]);
+                            pb[10 % M] = fmaf(gxg, hyy, pb[10 % M]); pb[11 % M] = fmaf(gyg, hyy, pb[11 % M]);
+                        }
+                    }
+                }
+            }
+            s1 += (double)p1;
+            s2 += (double)p2;
+            sfg += (double)pfg;
+        }
+        {
+            double v[3 + M];
+            v[0] = s1; v[1] = s2; v[2] = sfg;
+#pragma unroll
+            for (int j = 0; j < M; j++) v[3 + j] = (double)pb[j];
+            block_reduce<NT, 3 + M>(v, sm);
+        }
+        // uniform FP64 update by warp 0
+        const double gmt = sm.tot[0] / dn;
+        const double dg2 = sm.tot[1] - sm.tot[0] * gmt;
+        const double dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
+        const double sab = sm.tot[2] - gmt * sa;
+        const double znssd = 2.0 - 2.0 * sab / (df * dg);
+        const double ratio = df / dg;
+        gm_last = fm + gmt;
+        dg_last = dg;
+        if (wid == 0) {
+            if (lane < M) sm.grad[lane] = sm.A[lane] - ratio * (sm.tot[3 + lane] - gmt * sm.S[lane]);
+            __syncwarp();
+            if (lane < M) {
+                double acc = 0.0;
+#pragma unroll
+                for (int k = 0; k < M; k++) acc = fma(sm.Hinv[lane * M + k], sm.grad[k], acc);
+                sm.dp[lane] = -acc;
+                sm.pprev[lane] = sm.p[lane];
+            }
+            __syncwarp();
+            if (lane == 0) {
+                double pn[12], dpl[12], pl[12];
+#pragma unroll
+                for (int k = 0; k < 12; k++) {
+                    dpl[k] = sm.dp[k % M];
+                    pl[k] = sm.p[k % M];
+                }
+                bool ok = true;
+                if (ORDER == 0) {
+                    pn[0] = pl[0] - dpl[0];
+                    pn[1] = pl[1] - dpl[1];
+                } else if (ORDER == 1) {
+                    ok = compose1(pl, dpl, pn);
+                } else {
+                    ok = compose2_regs(pl, dpl, pn);
+                }
+                if (ok) {
+#pragma unroll
+                    for (int k = 0; k < M; k++) sm.p[k] = pn[k];
+                }
+                sm.flag[1] = ok;
+                sm.misc[1] = conv_norm<M>(dpl, size);
+            }
+        }
+        __syncthreads();
+        if (!sm.flag[1]) {
+            status = GPV_SINGULAR_WDELTA;  // p keeps the last valid warp
+            break;
+        }
+        const double nrm = sm.misc[1];
+        c_znssd = znssd;
+        c_zncc = 1.0 - znssd / 2.0;
+        iters = it;
+        last_norm = nrm;
+        if (tid == 0) write_history(A, idx, it, nrm, c_zncc, c_znssd);
+        if (!isfinite(nrm)) { status = GPV_NONFINITE; break; }
+        if (nrm < A.max_norm) { converged = true; break; }
+    }
+
+    // ---- eta diagnostic at the last sampled warp (optional) -----------------
+    double eu = 0.0, ev = 0.0;
+    const bool want_eta = (A.flags & GPV_SOLVE_ETA) && iters > 0 && status == GPV_OK;
+    if (want_eta) {
+        const double *pprev = sm.pprev;
+        const double X0 = cx + pprev[0], Y0 = cy + pprev[1];
+        const double bxd = floor(X0), byd = floor(Y0);
+        const int wbx = (int)bxd, wby = (int)byd;
+        const double ox = X0 - bxd, oy = Y0 - byd;
+        for (int i = tid; i < npx_t; i += NT) {
+            const float4 rec = S4[i];
+            if (rec.x != rec.x) continue;
+            float dxf, dyf;
+            unpack_off(rec.w, dxf, dyf);
+            const double dx = dxf, dy = dyf;
+            double lx = ox + dx, ly = oy + dy;
+            if (ORDER >= 1) {
+                lx += pprev[2] * dx + pprev[4] * dy;
+                ly += pprev[3] * dx + pprev[5] * dy;
+            }
+            if (ORDER == 2) {
+                lx += 0.5 * pprev[6 % M] * dx * dx + pprev[8 % M] * dx * dy + 0.5 * pprev[10 % M] * dy * dy;
+                ly += 0.5 * pprev[7 % M] * dx * dx + pprev[9 % M] * dx * dy + 0.5 * pprev[11 % M] * dy * dy;
+            }
+            int ix, iy;
+            float tx, ty;
+            split_clamped(wbx, (float)lx, A.w, ix, tx);
+            split_clamped(wby, (float)ly, A.h, iy, ty);
+            float a[6], b[6];
+            basis(ty, a);
+            basis(tx, b);
+            Sg[i] = contract<float>(A.g32 + (int64_t)(iy + B - 2) * A.pitch32 + (ix + B - 2), A.pitch32, a, b);
+        }
+        __syncthreads();
+        auto load = [&](int i, double &f, double &gx, double &gy, double &g, double &dx, double &dy) -> bool {
+            const float4 rec = S4[i];
+            if (rec.x != rec.x) return false;
+            float dxf, dyf;
+            unpack_off(rec.w, dxf, dyf);
+            f = rec.x; gx = rec.y; gy = rec.z; g = Sg[i]; dx = dxf; dy = dyf;
+            return true;
+        };
+        auto red = [&](double v) { return block_sum1<NT>(v, sm); };
+        eta_sums<ORDER>(npx_t, tid, NT, dn, fm, df, gm_last, dg_last, load, red, eu, ev);
+    }
+    if (tid == 0) {
+        gpv_subset_result *o = A.out + idx;
+#pragma unroll
+        for (int k = 0; k < 12; k++) o->p[k] = k < M ? sm.p[k % M] : 0.0;
+        o->c_zncc = c_zncc;
+        o->c_znssd = c_znssd;
+        o->norm = last_norm;
+        o->eta_u = eu;
+        o->eta_v = ev;
+        o->f_m = fm;
+        o->delta_f = df;
+        o->sssig = tot_sssig;
+        o->sigma = sqrt(saa / dn);
+        o->iterations = iters;
+        o->converged = converged;
+        o->quality_ok = converged && c_zncc >= A.tolerance;
+        o->status = status;
+        o->n_px = n;
+        o->has_eta = want_eta;
+    }
+}
+
+// Scratch per block: n_max float4 records + n_max floats (eta resample).
+template <int ORDER, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT) icgn_tile(TileArgs T) {
+    extern __shared__ float4 win4[];
+    float *win = reinterpret_cast<float *>(win4);
+    __shared__ TileSmem sm;
+    const KArgs &A = T.k;
+    const int64_t nmax = A.scratch_stride / 5;
+    float *base = reinterpret_cast<float *>(A.scratch) + (int64_t)blockIdx.x * A.scratch_stride;
+    float4 *S4 = reinterpret_cast<float4 *>(base);
+    float *Sg = base + 4 * nmax;
+    const int start = T.seg[0], count = T.seg[1];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) sm.item = atomicAdd(T.queue, 1);
+        __syncthreads();
+        const int item = sm.item;
+        if (item >= count) break;
+        const int idx = A.order[start + item];
+        const gpv_subset_desc d = A.desc[idx];
+        if (d.radius < 1 || d.radius > A.max_radius) {
+            if (threadIdx.x == 0) write_failed(A, idx, d, 12, GPV_INVALID_SUBSET, 0, 0.0, 0.0);
+            continue;
+        }
+        tile_subset<ORDER, NT>(T, idx, d, S4, Sg, win, sm);
+    }
+}
+
+// Split the work list by warp order: seg[2k], seg[2k+1] = start, count of
+// order 2 - k (order 2 first); order_out holds the segments back to back.
+// Subsets with an order outside {0, 1, 2} are failed here.
+__global__ void count_orders(const gpv_subset_desc *desc, const int32_t *order_in, int n, int32_t *cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int o = -1;
+    if (i < n) o = desc[order_in ? order_in[i] : i].order;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const unsigned m = __ballot_sync(0xffffffffu, o == 2 - k);
+        if ((threadIdx.x & 31) == 0 && m) atomicAdd(cnt + k, __popc(m));
+    }
+}
+
+__global__ void scatter_orders(const gpv_subset_desc *desc, const int32_t *order_in, int n, const int32_t *cnt,
+                               int32_t *fill, int32_t *order_out, int32_t *seg, gpv_subset_result *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    int idx = -1, o = -1;
+    if (i < n) {
+        idx = order_in ? order_in[i] : i;
+        o = desc[idx].order;
+    }
+    const int start[3] = {0, cnt[0], cnt[0] + cnt[1]};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const unsigned m = __ballot_sync(0xffffffffu, o == 2 - k);
+        if (!m) continue;
+        int base = 0;
+        const int leader = __ffs(m) - 1;
+        if (lane == leader) base = atomicAdd(fill + k, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (o == 2 - k) order_out[start[k] + base + __popc(m & ((1u << lane) - 1))] = idx;
+    }
+    if (i < n && (o < 0 || o > 2)) {
+        const gpv_subset_desc d = desc[idx];
+        write_failed_any(out, idx, d, GPV_INVALID_SUBSET);
+    }
+    if (i == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            seg[2 * k] = start[k];
+            seg[2 * k + 1] = cnt[k];
+        }
+    }
+}
+
+template <int NT>
+const void *tile_kernel(int order) {
+    return order == 2 ? (const void *)icgn_tile<2, NT> : (order == 1 ? (const void *)icgn_tile<1, NT>
+                                                                     : (const void *)icgn_tile<0, NT>);
+}
+
+template <int NT>
+void tile_launch_one(int order, int blocks, size_t smem, cudaStream_t s, const TileArgs &T) {
+    if (order == 2) icgn_tile<2, NT><<<blocks, NT, smem, s>>>(T);
+    else if (order == 1) icgn_tile<1, NT><<<blocks, NT, smem, s>>>(T);
+    else icgn_tile<0, NT><<<blocks, NT, smem, s>>>(T);
+}
+
+}  // namespace
+
+// Threads per block of the tiled kernel for subsets of radius r: the
+// autotuned choice when one was recorded for this radius class, else a
+// size rule (GPV_TILE_THREADS overrides).
+int tile_threads_for(gpv_context *ctx, int max_radius);
+
+// Launch the three per-order kernels.
+int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
+    int32_t *ws = static_cast<int32_t *>(ctx->tile_ws.ptr);
+    int32_t *cnt = ws, *fill = ws + 4, *seg = ws + 8, *queues = ws + 16, *order_out = ws + 32;
+    GPV_CUDA_TRY(cudaMemsetAsync(ws, 0, 32 * sizeof(int32_t), s));
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    count_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, cnt);
+    scatter_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, cnt, fill, order_out, seg, K.out);
+    GPV_CUDA_TRY(cudaGetLastError());
+    const int nt = tile_threads_for(ctx, K.max_radius);
+    // window capacity: a radius-max_radius subset stretched by 6%, plus margins
+    const int rw = (int)std::ceil(1.06 * K.max_radius) + 2;
+    const int side = 2 * rw + 6 + 2 * kMargin + 4;
+    const int cap = side * side;
+    const size_t smem = sizeof(float) * cap;
+    TileArgs T;
+    T.k = K;
+    T.k.order = order_out;
+    T.win_cap = cap;
+    GPV_CUDA_TRY(cudaEventRecord(ctx->ev[0], s));
+    cudaStream_t st[3] = {s, ctx->aux[0], ctx->aux[1]};
+    int total_blocks = 0;
+    for (int k = 0; k < 3; k++) {
+        int per_sm = 0;
+        const void *fn = nt == 256 ? tile_kernel<256>(2 - k) : tile_kernel<128>(2 - k);
+        GPV_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, smem));
+        if (per_sm < 1) { set_error("subset window does not fit in shared memory"); return GPV_ERR_INVALID; }
+        total_blocks = std::max(total_blocks, per_sm * ctx->num_sms);
+    }
+    // scratch: one slot per resident block of each of the three kernels
+    const int64_t nmax = (int64_t)(ctx->h_tab_n[K.max_radius] + 31) / 32 * 32;
+    const int64_t stride = 5 * nmax;  // float4 record + eta sample per pixel
+    if (int rc = ctx->scratch.ensure((size_t)3 * total_blocks * stride * sizeof(float))) return rc;
+    for (int k = 0; k < 3; k++) {
+        if (k > 0) GPV_CUDA_TRY(cudaStreamWaitEvent(st[k], ctx->ev[0], 0));
+        TileArgs Tk = T;
+        Tk.seg = seg + 2 * k;
+        Tk.queue = queues + k;
+        Tk.k.scratch = static_cast<float *>(ctx->scratch.ptr) + (int64_t)k * total_blocks * stride;
+        Tk.k.scratch_stride = stride;
+        if (nt == 256) tile_launch_one<256>(2 - k, total_blocks, smem, st[k], Tk);
+        else tile_launch_one<128>(2 - k, total_blocks, smem, st[k], Tk);
+        GPV_CUDA_TRY(cudaGetLastError());
+    }
+    for (int k = 1; k < 3; k++) {
+        GPV_CUDA_TRY(cudaEventRecord(ctx->ev[k], st[k]));
+        GPV_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev[k], 0));
+    }
+    return GPV_SUCCESS;
+}
+
+int tile_threads_for(gpv_context *ctx, int max_radius) {
+    if (const char *v = getenv("GPV_TILE_THREADS")) return atoi(v) == 256 ? 256 : 128;
+    const int cls = max_radius <= 20 ? 0 : (max_radius <= 40 ? 1 : 2);
+    if (ctx->tuned_threads[cls]) return ctx->tuned_threads[cls];
+    return max_radius > 40 ? 256 : 128;
+}
+
+}  // namespace gpv

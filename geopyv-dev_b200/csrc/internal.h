@@ -59,7 +59,11 @@ struct gpv_context {
     gpv::DevBuf order_dev;
     gpv::DevBuf hist_dev;
     gpv::DevBuf eval_dev;
+    gpv::DevBuf tile_ws;               // order partition + per-kernel queues
+    cudaStream_t aux[2] = {nullptr, nullptr};  // extra streams for the per-order kernels
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     int mixed_blocks_per_sm = 0;
+    int tuned_threads[3] = {0, 0, 0};  // autotuned threads per block by radius class
 };
 
 struct gpv_image {
