@@ -273,6 +273,9 @@ def run_ours(args, world, rank, local):
         if es1 is not None:
             es1.record(stream)
 
+    tuned = [0, 0, 0]
+    if prec == gpv.PREC_MIXED and not os.environ.get("GPV_TILE_THREADS"):
+        tuned = gpv.autotune(F, G, desc, sample_per_class=2048)
     peak_buf = ct.c_double(0.0)
     _lib.check(L.gpv_probe_fp32_peak(ctx.handle, ct.byref(peak_buf)), "probe")
     fp32_peak = peak_buf.value
@@ -372,7 +375,8 @@ def run_ours(args, world, rank, local):
                    "max_iterations": 50, "precision": args.precision,
                    "step": "prefilter(f)+prefilter(g)+batched ICGN solve",
                    "l2": "inputs larger than L2: 2 x 4136^2 FP32 coefficients + FP64 row pass (~410 MB) rewritten each step",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "tuned_threads_per_subset": {"r<=20": tuned[0], "r21-40": tuned[1], "r>40": tuned[2]}},
         "solve_ms": solve_avg_ms, "prefilter_ms": t_max / args.steps - solve_avg_ms,
         "samples_per_s": world * samples * args.steps / (t_max * 1e-3),
         "iterations_mean": float(np.mean(res["iterations"])),

@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -41,6 +43,7 @@ void DevBuf::release() {
 struct short2_h {
     int16_t x, y;
 };
+constexpr int16_t kSlotEmpty = -32768;  // padding slot of a template row (see icgn_tile.cu)
 
 // Circular local masks for radii 1..max_radius in the scan order of
 // LocalMask::circle (src/masks.rs:69-109): rows y = -r..r, columns x = -r..r,
@@ -51,23 +54,44 @@ int ensure_tables(gpv_context *ctx, int max_radius) {
         set_error("radius above 4000 is not supported");
         return GPV_ERR_INVALID;
     }
-    std::vector<short2_h> offs;
-    std::vector<int32_t> toff(max_radius + 1, 0), tn(max_radius + 1, 0);
+    std::vector<short2_h> offs, slots;
+    std::vector<int32_t> toff(max_radius + 1, 0), tn(max_radius + 1, 0), soff(max_radius + 1, 0),
+        sn(max_radius + 1, 0);
     for (int r = 1; r <= max_radius; r++) {
         toff[r] = (int32_t)offs.size();
-        for (int y = -r; y <= r; y++)
+        soff[r] = (int32_t)slots.size();
+        for (int y = -r; y <= r; y++) {
+            int row = 0;
             for (int x = -r; x <= r; x++)
-                if (x * x + y * y <= r * r) offs.push_back({(int16_t)x, (int16_t)y});
+                if (x * x + y * y <= r * r) {
+                    offs.push_back({(int16_t)x, (int16_t)y});
+                    slots.push_back({(int16_t)x, (int16_t)y});
+                    row++;
+                }
+            // pad the template row to whole warps: a warp never straddles two rows
+            while (row % 32) {
+                slots.push_back({kSlotEmpty, (int16_t)y});
+                row++;
+            }
+        }
         tn[r] = (int32_t)offs.size() - toff[r];
+        sn[r] = (int32_t)slots.size() - soff[r];
     }
     if (int rc = ctx->offs.ensure(offs.size() * sizeof(short2_h))) return rc;
-    if (int rc = ctx->tab_off.ensure(toff.size() * sizeof(int32_t))) return rc;
-    if (int rc = ctx->tab_n.ensure(tn.size() * sizeof(int32_t))) return rc;
+    if (int rc = ctx->slots.ensure(slots.size() * sizeof(short2_h))) return rc;
+    if (int rc = ctx->tab_off.ensure(2 * toff.size() * sizeof(int32_t))) return rc;
+    if (int rc = ctx->tab_n.ensure(2 * tn.size() * sizeof(int32_t))) return rc;
     GPV_CUDA_TRY(cudaMemcpy(ctx->offs.ptr, offs.data(), offs.size() * sizeof(short2_h), cudaMemcpyHostToDevice));
-    GPV_CUDA_TRY(cudaMemcpy(ctx->tab_off.ptr, toff.data(), toff.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-    GPV_CUDA_TRY(cudaMemcpy(ctx->tab_n.ptr, tn.data(), tn.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    GPV_CUDA_TRY(cudaMemcpy(ctx->slots.ptr, slots.data(), slots.size() * sizeof(short2_h), cudaMemcpyHostToDevice));
+    // tab_off / tab_n: compact template tables, then the padded slot tables
+    std::vector<int32_t> to2(toff), tn2(tn);
+    to2.insert(to2.end(), soff.begin(), soff.end());
+    tn2.insert(tn2.end(), sn.begin(), sn.end());
+    GPV_CUDA_TRY(cudaMemcpy(ctx->tab_off.ptr, to2.data(), to2.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    GPV_CUDA_TRY(cudaMemcpy(ctx->tab_n.ptr, tn2.data(), tn2.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     ctx->h_tab_off = toff;
     ctx->h_tab_n = tn;
+    ctx->h_slot_n = sn;
     ctx->table_radius = max_radius;
     return GPV_SUCCESS;
 }
@@ -101,6 +125,8 @@ using namespace gpv;
 
 extern "C" {
 
+static void tune_cache_load(gpv_context *ctx);
+
 const char *gpv_version(void) { return "gpv-b200 0.1.0 (sm_100a)"; }
 
 int gpv_abi_version(void) { return GPV_ABI_VERSION; }
@@ -133,6 +159,7 @@ int gpv_context_create(int device, gpv_context **out) {
         delete ctx;
         return GPV_ERR_CUDA;
     }
+    tune_cache_load(ctx);
     *out = ctx;
     return GPV_SUCCESS;
 }
@@ -141,7 +168,7 @@ int gpv_context_destroy(gpv_context *ctx) {
     if (!ctx) return GPV_SUCCESS;
     DeviceGuard dg(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (DevBuf *b : {&ctx->offs, &ctx->tab_off, &ctx->tab_n, &ctx->scratch, &ctx->queue, &ctx->desc_dev, &ctx->out_dev,
+    for (DevBuf *b : {&ctx->offs, &ctx->slots, &ctx->tab_off, &ctx->tab_n, &ctx->scratch, &ctx->queue, &ctx->desc_dev, &ctx->out_dev,
                       &ctx->order_dev, &ctx->hist_dev, &ctx->eval_dev, &ctx->tile_ws})
         b->release();
     for (int k = 0; k < 2; k++)
@@ -469,6 +496,88 @@ int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image
     L.max_radius = ctx->table_radius;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
     return solve_launch(ctx, L, s);
+}
+
+static int check_pair(const gpv_image *f, const gpv_image *g, const gpv_solve_params *prm);
+static int radius_class(int r) { return r <= 20 ? 0 : (r <= 40 ? 1 : 2); }
+
+static void tune_cache_load(gpv_context *ctx) {
+    const char *path = getenv("GPV_TUNE_CACHE");
+    if (!path) return;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) return;
+    FILE *fh = fopen(path, "r");
+    if (!fh) return;
+    char line[512];
+    while (fgets(line, sizeof line, fh)) {
+        char name[256];
+        int cls = -1, nt = 0;
+        if (sscanf(line, "%255[^|]|%d|%d", name, &cls, &nt) == 3 && cls >= 0 && cls < 3 &&
+            strcmp(name, prop.name) == 0 && (nt == 128 || nt == 256))
+            ctx->tuned_threads[cls] = nt;  // later lines win
+    }
+    fclose(fh);
+}
+
+int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc, int64_t n,
+                 const gpv_solve_params *prm, int32_t sample_per_class, int32_t *threads_out) {
+    if (!ctx || !desc || n <= 0 || sample_per_class < 1) { set_error("invalid autotune arguments"); return GPV_ERR_INVALID; }
+    if (int rc = check_pair(f, g, prm)) return rc;
+    std::vector<std::vector<gpv_subset_desc>> cls(3);
+    for (int64_t i = 0; i < n; i++) {
+        const int r = desc[i].radius;
+        if (r < 1 || r > 4000 || desc[i].order < 0 || desc[i].order > 2) continue;
+        cls[radius_class(r)].push_back(desc[i]);
+    }
+    gpv_solve_params p = *prm;
+    p.precision = GPV_PREC_MIXED;
+    p.history = nullptr;
+    p.flags &= ~GPV_SOLVE_ETA;
+    static const int cand[2] = {128, 256};
+    for (int c = 0; c < 3; c++) {
+        if (threads_out) threads_out[c] = 0;
+        if (cls[c].empty()) continue;
+        // an even sample of the class
+        std::vector<gpv_subset_desc> smp;
+        const size_t k = std::min<size_t>(cls[c].size(), (size_t)sample_per_class);
+        for (size_t j = 0; j < k; j++) smp.push_back(cls[c][j * cls[c].size() / k]);
+        std::vector<gpv_subset_result> out(smp.size());
+        double best = 1e300;
+        int best_nt = 128;
+        for (int t : cand) {
+            ctx->force_threads = t;
+            double ms_best = 1e300;
+            for (int rep = 0; rep < 3; rep++) {
+                cudaEvent_t e0, e1;
+                cudaEventCreate(&e0);
+                cudaEventCreate(&e1);
+                cudaEventRecord(e0, ctx->stream);
+                int rc = gpv_solve_batch(ctx, f, g, smp.data(), (int64_t)smp.size(), &p, out.data());
+                cudaEventRecord(e1, ctx->stream);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                if (rc) { ctx->force_threads = 0; return rc; }
+                if (rep > 0) ms_best = std::min(ms_best, (double)ms);
+            }
+            if (ms_best < best) { best = ms_best; best_nt = t; }
+        }
+        ctx->force_threads = 0;
+        ctx->tuned_threads[c] = best_nt;
+        if (threads_out) threads_out[c] = best_nt;
+        if (const char *path = getenv("GPV_TUNE_CACHE")) {
+            cudaDeviceProp prop;
+            if (cudaGetDeviceProperties(&prop, ctx->device) == cudaSuccess) {
+                if (FILE *fh = fopen(path, "a")) {
+                    fprintf(fh, "%s|%d|%d\n", prop.name, c, best_nt);
+                    fclose(fh);
+                }
+            }
+        }
+    }
+    return GPV_SUCCESS;
 }
 
 int gpv_probe_fp32_peak(gpv_context *ctx, double *tflops) {

@@ -809,6 +809,8 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
     A.h = (int)L.f->h; A.w = (int)L.f->w; A.border = L.f->border;
     A.desc = L.desc; A.order = L.order; A.n = (int)L.n;
     A.offs = static_cast<const short2 *>(ctx->offs.ptr);
+    A.slots = static_cast<const short2 *>(ctx->slots.ptr);
+    A.table_radius = ctx->table_radius;
     A.tab_off = static_cast<const int32_t *>(ctx->tab_off.ptr);
     A.tab_n = static_cast<const int32_t *>(ctx->tab_n.ptr);
     A.max_radius = L.max_radius;

@@ -23,7 +23,9 @@ struct KArgs {
     const int32_t *order;
     int n;
     const short2 *offs;
-    const int32_t *tab_off, *tab_n;
+    const short2 *slots;             // padded templates (rows padded to 32 lanes)
+    const int32_t *tab_off, *tab_n;  // [0, R]: compact templates, [R+1, 2R+1]: slot tables
+    int table_radius;
     int max_radius;
     const uint8_t *mask;
     int mh, mw;

@@ -34,14 +34,16 @@ struct TileSmem {
     double mom[3 * 15];
     double H[144];
     double Hinv[144];
-    double aug[288];
+    double aug[384];  // setup sums [0, 96), Gauss-Jordan workspace [96, 384)
     double A[12], S[12];
     double p[12], pprev[12], dp[12], grad[12];
     double red[kMaxTileWarps][16];
+    double red2[kMaxTileWarps][80];  // setup: one combined reduction
     double tot[16];
     double misc[8];
     int flag[4];
     int item;
+    int n_valid;
     int win_r0, win_c0, win_h, win_w, win_ok;
 };
 
@@ -50,6 +52,7 @@ struct TileArgs {
     const int32_t *seg;  // [start, count] of this order's segment in k.order
     int *queue;          // this kernel's work-queue counter
     int win_cap;         // floats of dynamic shared memory for the window
+    int padded;          // 1: template rows padded to 32 lanes (no straddling warps)
 };
 
 // Copy coefficient rows [r0, r0+wh) x cols [c0, c0+ww) (c0, ww multiples of 4)
@@ -59,6 +62,22 @@ __device__ __forceinline__ void stage(const float *__restrict__ C, int64_t pitch
                                       int ww, float *win) {
     const int nv = ww >> 2;
     for (int idx = threadIdx.x; idx < wh * nv; idx += NT) {
+        const int rr = idx / nv, cc = (idx - rr * nv) << 2;
+        int row = r0 + rr;
+        row = row < 0 ? 0 : (row > ch - 1 ? ch - 1 : row);
+        int col = c0 + cc;
+        col = col < 0 ? 0 : (col > (int)pitch - 4 ? (int)pitch - 4 : col);
+        const float4 v = __ldg(reinterpret_cast<const float4 *>(C + (int64_t)row * pitch + col));
+        *reinterpret_cast<float4 *>(win + rr * ww + cc) = v;
+    }
+}
+
+// Same with threads [t0, NT) only (the others are busy elsewhere).
+template <int NT>
+__device__ __forceinline__ void stage_part(const float *__restrict__ C, int64_t pitch, int ch, int r0, int c0, int wh,
+                                           int ww, float *win, int t0) {
+    const int nv = ww >> 2;
+    for (int idx = (int)threadIdx.x - t0; idx < wh * nv; idx += NT - t0) {
         const int rr = idx / nv, cc = (idx - rr * nv) << 2;
         int row = r0 + rr;
         row = row < 0 ? 0 : (row > ch - 1 ? ch - 1 : row);
@@ -164,8 +183,10 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
     constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int r = d.radius;
-    const int npx_t = A.tab_n[r];
-    const short2 *po = A.offs + A.tab_off[r];
+    // compact template, or rows padded to whole warps (empty slots: x = -32768)
+    const int tab = T.padded ? A.table_radius + 1 + r : r;
+    const int npx_t = A.tab_n[tab];
+    const short2 *po = (T.padded ? A.slots : A.offs) + A.tab_off[tab];
     const double cx = d.coord[0], cy = d.coord[1];
     const int cxi = (int)cx, cyi = (int)cy;
     const double fxd = floor(cx), fyd = floor(cy);
@@ -194,16 +215,37 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
     // (cx, cy) inside the image, so all share one fraction and one basis
     const bool interior = f_staged && bx - r >= 0 && bx + r <= A.w - 1 && by - r >= 0 && by + r <= A.h - 1;
 
-    // ---- setup pass 1: f, grad f, sum f, SSSIG --------------------------
-    double sum_f = 0.0, sssig = 0.0, cnt = 0.0;
+    // ---- setup --------------------------------------------------------------
+    // pass 1 samples f and its gradient (records) and accumulates, about a
+    // subset-uniform level s (a coefficient near the centre; it keeps the
+    // sums free of cancellation and a flat subset's sums exactly zero),
+    //   [count, sum (f-s), sum (f-s)^2, SSSIG, Bf_j = sum SDI_j (f-s) (M), S_j = sum SDI_j (M)];
+    // pass 2 (each thread re-reads its own records: no barrier) accumulates
+    // the 3*NMOM gradient moments of the Hessian.  FP32 partials per thread,
+    // combined across the block in FP64 by one reduction; then warp 0 forms
+    // A_j = Bf_j - (f_m - s) S_j, delta_f, H and H^-1 while the other warps stage
+    // g's window for the first iteration.
+    constexpr int NVA = 4 + 2 * M, NV = NVA + 3 * NMOM;
+    float acc[NVA];
+#pragma unroll
+    for (int q = 0; q < NVA; q++) acc[q] = 0.f;
+    // the shift level: the coefficient under the subset centre (uniform)
+    float shift = 0.f;
+    if (f_staged) {
+        const int wx = min(max(max(0, min(bx, A.w - 1)) + B - fc0, 0), fww - 1);
+        const int wy = min(max(max(0, min(by, A.h - 1)) + B - fr0, 0), fwh - 1);
+        shift = win[wy * fww + wx];
+    } else {
+        shift = A.f32[(int64_t)(max(0, min(by, A.h - 1)) + B) * A.pitch32 + max(0, min(bx, A.w - 1)) + B];
+    }
     {
         float a0[6], da0[6], b0[6], db0[6];
         basis(fy, a0); dbasis(fy, da0);
         basis(fx, b0); dbasis(fx, db0);
         for (int i = tid; i < npx_t; i += NT) {
             const short2 o = po[i];
-            if (!mask_ok(A, cxi, cyi, o.x, o.y)) {
-                S4[i] = pack_px(__int_as_float(0x7fc00000), 0.f, 0.f, o.x, o.y);
+            if (o.x == -32768 || !mask_ok(A, cxi, cyi, o.x, o.y)) {
+                S4[i] = pack_px(__int_as_float(0x7fc00000), 0.f, 0.f, 0, 0);
                 continue;
             }
             float gx, gy, f;
@@ -227,32 +269,33 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                 }
             }
             S4[i] = pack_px(f, gx, gy, o.x, o.y);
-            sum_f += (double)f;
-            sssig += 0.5 * ((double)gx * gx + (double)gy * gy);
-            cnt += 1.0;
+            const float dx = (float)o.x, dy = (float)o.y;
+            const float fs = f - shift;
+            acc[0] += 1.f;
+            acc[1] += fs;
+            acc[2] = fmaf(fs, fs, acc[2]);
+            acc[3] = fmaf(0.5f * gx, gx, fmaf(0.5f * gy, gy, acc[3]));
+            const float gxf = gx * fs, gyf = gy * fs;
+#pragma unroll
+            for (int mu = 0; mu < NMU; mu++) {
+                const float mv = mu_val<float>(mu, dx, dy);
+                acc[4 + 2 * mu] = fmaf(gxf, mv, acc[4 + 2 * mu]);
+                acc[5 + 2 * mu] = fmaf(gyf, mv, acc[5 + 2 * mu]);
+                acc[4 + M + 2 * mu] = fmaf(gx, mv, acc[4 + M + 2 * mu]);
+                acc[5 + M + 2 * mu] = fmaf(gy, mv, acc[5 + M + 2 * mu]);
+            }
         }
     }
-    {
-        const double v[3] = {sum_f, sssig, cnt};
-        block_reduce<NT, 3>(v, sm);
-    }
-    const double tot_f = sm.tot[0], tot_sssig = sm.tot[1];
-    const int n = (int)sm.tot[2];
-    if (n == 0) {
-        if (tid == 0) write_failed(A, idx, d, M, GPV_EMPTY_MASK, 0, 0.0, 0.0);
-        return;
-    }
-    const double dn = (double)n;
-    const double fm = tot_f / dn;
-    const float fmf = (float)fm;
-
-    // ---- setup pass 1b: gradient moments (Hessian) -------------------------
-    {
-        float mom[3][NMOM];
+    // warp partials of pass 1 straight into red2 (frees the accumulators)
 #pragma unroll
-        for (int p = 0; p < 3; p++)
+    for (int q = 0; q < NVA; q++) {
+        const double t = warp_sum((double)acc[q]);
+        if (lane == 0) sm.red2[wid][q] = t;
+    }
+    {
+        float mom[3 * NMOM];
 #pragma unroll
-            for (int q = 0; q < NMOM; q++) mom[p][q] = 0.f;
+        for (int q = 0; q < 3 * NMOM; q++) mom[q] = 0.f;
         for (int i = tid; i < npx_t; i += NT) {
             const float4 rec = S4[i];
             if (rec.x != rec.x) continue;
@@ -271,93 +314,89 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                     const float mono = pxp[dgr - bb] * pyp[bb];
 #pragma unroll
                     for (int p = 0; p < 3; p++)
-                        mom[p][mom_idx(dgr - bb, bb)] = fmaf(gg[p], mono, mom[p][mom_idx(dgr - bb, bb)]);
+                        mom[p * NMOM + mom_idx(dgr - bb, bb)] = fmaf(gg[p], mono, mom[p * NMOM + mom_idx(dgr - bb, bb)]);
                 }
         }
 #pragma unroll
-        for (int q0 = 0; q0 < 3 * NMOM; q0 += 15) {
-            double v[15];
-#pragma unroll
-            for (int j = 0; j < 15; j++) {
-                const int q = q0 + j;
-                v[j] = q < 3 * NMOM ? (double)mom[q / NMOM][q % NMOM] : 0.0;
-            }
-            block_reduce<NT, 15>(v, sm);
-            if (tid < 15 && q0 + tid < 3 * NMOM) sm.mom[q0 + tid] = sm.tot[tid];
+        for (int q = 0; q < 3 * NMOM; q++) {
+            const double t = warp_sum((double)mom[q]);
+            if (lane == 0) sm.red2[wid][NVA + q] = t;
         }
-    }
-
-    // ---- setup pass 2: delta_f, A_j, S_j --------------------------------
-    double sa, saa;
-    {
-        double acc[2 + 2 * M];
-#pragma unroll
-        for (int j = 0; j < 2 + 2 * M; j++) acc[j] = 0.0;
-        for (int i = tid; i < npx_t; i += NT) {
-            const float4 rec = S4[i];
-            if (rec.x != rec.x) continue;
-            float dxf, dyf;
-            unpack_off(rec.w, dxf, dyf);
-            const double a = (double)rec.x - fm;
-            const double gx = rec.y, gy = rec.z, dx = dxf, dy = dyf;
-            acc[0] += a;
-            acc[1] += a * a;
-#pragma unroll
-            for (int mu = 0; mu < NMU; mu++) {
-                const double mv = mu_val<double>(mu, dx, dy);
-                acc[2 + 2 * mu] += gx * mv * a;
-                acc[3 + 2 * mu] += gy * mv * a;
-                acc[2 + M + 2 * mu] += gx * mv;
-                acc[3 + M + 2 * mu] += gy * mv;
-            }
-        }
-        constexpr int K1 = (2 + 2 * M + 1) / 2, K2 = 2 + 2 * M - K1;
-        double v1[K1], v2[K2];
-#pragma unroll
-        for (int j = 0; j < K1; j++) v1[j] = acc[j];
-#pragma unroll
-        for (int j = 0; j < K2; j++) v2[j] = acc[K1 + j];
-        block_reduce<NT, K1>(v1, sm);
-        double *dst = sm.aug;  // scratch until the Hessian is inverted
-        if (tid < K1) dst[tid] = sm.tot[tid];
-        block_reduce<NT, K2>(v2, sm);
-        if (tid < K2) dst[K1 + tid] = sm.tot[tid];
-        __syncthreads();
-        sa = dst[0];
-        saa = dst[1];
-        if (tid < M) {
-            sm.A[tid] = dst[2 + tid];
-            sm.S[tid] = dst[2 + M + tid];
-        }
-        __syncthreads();
-    }
-    const double df = sqrt(saa);
-    if (!(sqrt(saa / dn) > 1e-6 * fmax(1.0, fabs(fm)))) {  // flat subset
-        if (tid == 0) write_failed(A, idx, d, M, GPV_FEATURELESS, n, fm, df);
-        return;
-    }
-    if (wid == 0) {
-        assemble_hessian<ORDER>(sm.mom, sm.H, lane);
-        const bool ok = spd_inverse_warp<M>(sm.H, sm.aug, sm.Hinv, lane);
-        if (lane == 0) sm.flag[0] = ok;
     }
     __syncthreads();
-    if (!sm.flag[0]) {
+    if (wid == 0) {
+        // sum the warp partials: aug[0..NV)
+        for (int q = lane; q < NV; q += 32) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < NT / 32; w++) t += sm.red2[w][q];
+            sm.aug[q] = t;
+        }
+        __syncwarp();
+        const int n = (int)(sm.aug[0] + 0.5);
+        const double dn = (double)n, ms = sm.aug[1] / (n > 0 ? dn : 1.0);  // mean of f - s
+        const double fm = (double)shift + ms;
+        const double saa = sm.aug[2] - ms * sm.aug[1];  // sum (f - f_m)^2
+        int st = GPV_OK;
+        if (n == 0) st = GPV_EMPTY_MASK;
+        else if (!(sqrt(fmax(saa, 0.0) / dn) > 1e-6 * fmax(1.0, fabs(fm)))) st = GPV_FEATURELESS;  // flat subset
+        if (st == GPV_OK) {
+            if (lane < M) {
+                sm.A[lane] = sm.aug[4 + lane] - ms * sm.aug[4 + M + lane];  // sum SDI (f - f_m)
+                sm.S[lane] = sm.aug[4 + M + lane];
+            }
+            if (lane < 3 * NMOM) sm.mom[lane] = sm.aug[NVA + lane];
+            if (lane + 32 < 3 * NMOM) sm.mom[lane + 32] = sm.aug[NVA + lane + 32];
+            __syncwarp();
+            assemble_hessian<ORDER>(sm.mom, sm.H, lane);
+            if (!spd_inverse_warp<M>(sm.H, sm.aug + 96, sm.Hinv, lane)) st = GPV_SINGULAR_H;
+        }
+        if (lane == 0) {
+            sm.flag[0] = st;
+            sm.misc[5] = fm;
+            sm.misc[6] = saa;
+            sm.misc[7] = sm.aug[3];
+            sm.n_valid = n;
+        }
+        if (lane < M) {
+            sm.p[lane] = d.p0[lane];
+            sm.pprev[lane] = d.p0[lane];
+        }
+    } else {
+        // meanwhile: stage g's window around the initial warp
+        int xlo, xhi, ylo, yhi, r0 = 0, c0 = 0, wh = 0, ww = 0;
+        double p0[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) p0[k] = d.p0[k % M];
+        warp_extent<ORDER>(p0, cx, cy, r, A.w, A.h, xlo, xhi, ylo, yhi);
+        const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, r0, c0, wh, ww);
+        if (ok) stage_part<NT>(A.g32, A.pitch32, ch, r0, c0, wh, ww, win, 32);
+        if (tid == 32) {
+            sm.win_ok = ok;
+            sm.win_r0 = r0; sm.win_c0 = c0; sm.win_h = wh; sm.win_w = ww;
+        }
+    }
+    __syncthreads();
+    const int st0 = sm.flag[0];
+    const int n = sm.n_valid;
+    const double dn = (double)n;
+    const double fm = sm.misc[5], saa = sm.misc[6], tot_sssig = sm.misc[7];
+    const float fmf = (float)fm;
+    const double sa = 0.0;  // sum (f - f_m) is zero by construction of f_m
+    const double df = sqrt(fmax(saa, 0.0));
+    if (st0 != GPV_OK) {
         if (tid == 0) {
-            write_failed(A, idx, d, M, GPV_SINGULAR_H, n, fm, df);
-            A.out[idx].sssig = tot_sssig;
-            A.out[idx].sigma = sqrt(saa / dn);
+            write_failed(A, idx, d, M, st0, n, n ? fm : 0.0, n ? df : 0.0);
+            if (st0 == GPV_SINGULAR_H) {
+                A.out[idx].sssig = tot_sssig;
+                A.out[idx].sigma = sqrt(saa / dn);
+            }
         }
         return;
     }
 
     // ---- ICGN iterations --------------------------------------------------
     const double size = sqrt(dn);
-    if (tid < M) {
-        sm.p[tid] = d.p0[tid];
-        sm.pprev[tid] = d.p0[tid];
-    }
-    __syncthreads();
     int iters = 0, status = GPV_OK;
     bool converged = false;
     double c_zncc = 0.0, c_znssd = 4.0, last_norm = 0.0, gm_last = 0.0, dg_last = 0.0;
@@ -396,13 +435,15 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         float pb[M];
 #pragma unroll
         for (int j = 0; j < M; j++) pb[j] = 0.f;
+        float4 rec_next = tid < npx_t ? S4[tid] : make_float4(0.f, 0.f, 0.f, 0.f);
         for (int base = 0; base < npx_t; base += NT * kChunk) {
             float p1 = 0.f, p2 = 0.f, pfg = 0.f;
 #pragma unroll 2
             for (int c = 0; c < kChunk; c++) {
                 const int i = base + c * NT + tid;
                 if (i < npx_t) {
-                    const float4 rec = S4[i];
+                    const float4 rec = rec_next;  // loaded one sample ahead
+                    if (i + NT < npx_t) rec_next = S4[i + NT];
                     const float fv = rec.x;
                     if (fv == fv) {
                         float dx, dy;
@@ -453,23 +494,38 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             s2 += (double)p2;
             sfg += (double)pfg;
         }
+        // block sums: warp partials to shared memory, one barrier, then warp 0
+        // adds them up and updates the warp; a second barrier publishes p
         {
             double v[3 + M];
             v[0] = s1; v[1] = s2; v[2] = sfg;
 #pragma unroll
             for (int j = 0; j < M; j++) v[3 + j] = (double)pb[j];
-            block_reduce<NT, 3 + M>(v, sm);
+#pragma unroll
+            for (int k = 0; k < 3 + M; k++) {
+                const double t = warp_sum(v[k]);
+                if (lane == 0) sm.red[wid][k] = t;
+            }
         }
-        // uniform FP64 update by warp 0
-        const double gmt = sm.tot[0] / dn;
-        const double dg2 = sm.tot[1] - sm.tot[0] * gmt;
-        const double dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
-        const double sab = sm.tot[2] - gmt * sa;
-        const double znssd = 2.0 - 2.0 * sab / (df * dg);
-        const double ratio = df / dg;
-        gm_last = fm + gmt;
-        dg_last = dg;
+        __syncthreads();
         if (wid == 0) {
+            if (lane < 3 + M) {
+                double t = 0.0;
+#pragma unroll
+                for (int w = 0; w < NT / 32; w++) t += sm.red[w][lane];
+                sm.tot[lane] = t;
+            }
+            __syncwarp();
+        }
+        // (all threads read tot only after the update barrier below)
+        double gmt = 0.0, dg = 0.0, znssd = 0.0;
+        if (wid == 0) {
+            gmt = sm.tot[0] / dn;
+            const double dg2 = sm.tot[1] - sm.tot[0] * gmt;
+            dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
+            const double sab = sm.tot[2] - gmt * sa;
+            znssd = 2.0 - 2.0 * sab / (df * dg);
+            const double ratio = df / dg;
             if (lane < M) sm.grad[lane] = sm.A[lane] - ratio * (sm.tot[3 + lane] - gmt * sm.S[lane]);
             __syncwarp();
             if (lane < M) {
@@ -502,9 +558,17 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                 }
                 sm.flag[1] = ok;
                 sm.misc[1] = conv_norm<M>(dpl, size);
+                sm.misc[2] = gmt;
+                sm.misc[3] = dg;
+                sm.misc[4] = znssd;
             }
         }
         __syncthreads();
+        gmt = sm.misc[2];
+        dg = sm.misc[3];
+        znssd = sm.misc[4];
+        gm_last = fm + gmt;
+        dg_last = dg;
         if (!sm.flag[1]) {
             status = GPV_SINGULAR_WDELTA;  // p keeps the last valid warp
             break;
@@ -700,6 +764,8 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
     T.k = K;
     T.k.order = order_out;
     T.win_cap = cap;
+    const char *lay = getenv("GPV_TILE_LAYOUT");
+    T.padded = lay && lay[0] == 'p';
     GPV_CUDA_TRY(cudaEventRecord(ctx->ev[0], s));
     cudaStream_t st[3] = {s, ctx->aux[0], ctx->aux[1]};
     int total_blocks = 0;
@@ -712,7 +778,7 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         total_blocks = std::max(total_blocks, per_sm * ctx->num_sms);
     }
     // scratch: one slot per resident block of each of the three kernels
-    const int64_t nmax = (int64_t)(ctx->h_tab_n[K.max_radius] + 31) / 32 * 32;
+    const int64_t nmax = (int64_t)(ctx->h_slot_n[K.max_radius] + 31) / 32 * 32;
     const int64_t stride = 5 * nmax;  // float4 record + eta sample per pixel
     if (int rc = ctx->scratch.ensure((size_t)3 * total_blocks * stride * sizeof(float))) return rc;
     for (int k = 0; k < 3; k++) {
@@ -734,6 +800,7 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
 }
 
 int tile_threads_for(gpv_context *ctx, int max_radius) {
+    if (ctx->force_threads) return ctx->force_threads;
     if (const char *v = getenv("GPV_TILE_THREADS")) return atoi(v) == 256 ? 256 : 128;
     const int cls = max_radius <= 20 ? 0 : (max_radius <= 40 ? 1 : 2);
     if (ctx->tuned_threads[cls]) return ctx->tuned_threads[cls];

@@ -47,10 +47,11 @@ struct gpv_context {
     std::mutex mu;
     // circular mask offset tables, radii 1..table_radius (short2 per pixel)
     int table_radius = 0;
-    gpv::DevBuf offs;     // short2
+    gpv::DevBuf offs;     // short2, compact circle templates
+    gpv::DevBuf slots;    // short2, templates with rows padded to 32 (x = -32768: empty)
     gpv::DevBuf tab_off;  // int32 [table_radius + 1]
     gpv::DevBuf tab_n;    // int32 [table_radius + 1]
-    std::vector<int32_t> h_tab_off, h_tab_n;
+    std::vector<int32_t> h_tab_off, h_tab_n, h_slot_n;
     // solve workspace
     gpv::DevBuf scratch;   // per-warp / per-block pixel arrays
     gpv::DevBuf queue;     // work-queue counters
@@ -64,6 +65,7 @@ struct gpv_context {
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     int mixed_blocks_per_sm = 0;
     int tuned_threads[3] = {0, 0, 0};  // autotuned threads per block by radius class
+    int force_threads = 0;             // set while the autotuner times a candidate
 };
 
 struct gpv_image {

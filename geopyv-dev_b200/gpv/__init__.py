@@ -17,7 +17,7 @@ from . import _lib
 from ._lib import (DESC_DTYPE, RESULT_DTYPE, PREC_FP64, PREC_MIXED, SOLVE_ETA, STATUS, GpvError, SolveParams,
                    check, lib, ptr)
 
-__all__ = ["Context", "Image", "Mask", "Subset", "solve_batch", "make_desc", "DESC_DTYPE", "RESULT_DTYPE",
+__all__ = ["Context", "Image", "Mask", "Subset", "solve_batch", "autotune", "make_desc", "DESC_DTYPE", "RESULT_DTYPE",
            "GpvError", "PREC_MIXED", "PREC_FP64", "STATUS", "version"]
 
 
@@ -220,6 +220,18 @@ def solve_batch(f_img: Image, g_img: Image, desc, max_norm=1e-5, max_iterations=
     check(lib().gpv_solve_batch(f_img.ctx.handle, f_img.handle, g_img.handle, ptr(desc), desc.size,
                                 ct.byref(prm), ptr(out)), "gpv_solve_batch")
     return (out, hist) if history else out
+
+
+def autotune(f_img: Image, g_img: Image, desc, max_norm=1e-5, max_iterations=50, tolerance=0.75,
+             sample_per_class=1024):
+    """Pick the fastest launch shape per radius class on a sample of `desc`
+    (gpv_autotune); returns threads per subset block for r <= 20, 21..40, > 40."""
+    desc = np.ascontiguousarray(desc, dtype=DESC_DTYPE)
+    prm = _params(max_norm, max_iterations, tolerance, False, PREC_MIXED, None, None)
+    out = (ct.c_int32 * 3)()
+    check(lib().gpv_autotune(f_img.ctx.handle, f_img.handle, g_img.handle, ptr(desc), desc.size, ct.byref(prm),
+                             sample_per_class, out), "gpv_autotune")
+    return list(out)
 
 
 class Subset:

@@ -162,6 +162,17 @@ int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image
                            const gpv_subset_desc *desc_dev, const int32_t *work_order_dev, int64_t n,
                            const gpv_solve_params *params, gpv_subset_result *out_dev, void *stream);
 
+/* ---- autotuning (no counterpart in the reference) ------------------------
+ * Times the candidate launch shapes of the mixed-precision kernel (threads
+ * per subset block) on a sample of up to sample_per_class subsets of each
+ * radius class (r <= 20, 21..40, > 40) present in desc, keeps the fastest per
+ * class in the context, and returns the choices in threads_out[3] (0 = class
+ * absent).  If the environment variable GPV_TUNE_CACHE names a file, the
+ * choices are appended to it keyed by device name, and gpv_context_create
+ * reads them back. */
+int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc, int64_t n,
+                 const gpv_solve_params *params, int32_t sample_per_class, int32_t *threads_out);
+
 /* ---- calibration (no counterpart in the reference) ----------------------
  * Measured FP32 FMA throughput of this device (TFLOP/s, 2 FLOP per FMA) from
  * a register-only FMA kernel: the denominator of the interpolation roofline. */

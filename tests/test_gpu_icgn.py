@@ -176,3 +176,29 @@ def test_subset_api(oracle, gpv_mod):
     with pytest.raises(RuntimeError):
         gpv_mod.Subset([40.0, 40.0], gpv_mod.Mask("local", shape="circle", size=10),
                        gpv_mod.Image(image_gs=np.full((80, 80), 9.0)), gpv_mod.Image(image_gs=np.full((80, 80), 9.0))).solve()
+
+
+def test_autotune_choices_do_not_change_results(oracle, gpv_mod):
+    """Every launch shape the autotuner can pick gives the same solution."""
+    from gpv import synth
+    W = synth.workload(3, scale_down=8)
+    F, G, Cf, Cg = _images(gpv_mod, oracle, W)
+    d = _desc(gpv_mod, W)
+    tuned = gpv_mod.autotune(F, G, d, sample_per_class=256)
+    present = {0: np.any(d["radius"] <= 20), 1: np.any((d["radius"] > 20) & (d["radius"] <= 40)), 2: np.any(d["radius"] > 40)}
+    for c in range(3):
+        assert tuned[c] in ((128, 256) if present[c] else (0,))
+    import os
+    res = {}
+    for nt in ("128", "256"):
+        os.environ["GPV_TILE_THREADS"] = nt
+        try:
+            ctx = gpv_mod.Context(0)  # a fresh context carries no tuned choice
+            F2 = gpv_mod.Image(image_gs=W["f"], border=BORDER, ctx=ctx)
+            G2 = gpv_mod.Image(image_gs=W["g"], border=BORDER, ctx=ctx)
+            res[nt] = gpv_mod.solve_batch(F2, G2, d, max_norm=1e-5, max_iterations=50)
+        finally:
+            del os.environ["GPV_TILE_THREADS"]
+    assert np.array_equal(res["128"]["iterations"], res["256"]["iterations"]) or \
+        (res["128"]["iterations"] != res["256"]["iterations"]).mean() < 0.02
+    assert np.abs(res["128"]["p"] - res["256"]["p"]).max() < 1e-4
