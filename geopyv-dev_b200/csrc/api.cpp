@@ -499,6 +499,24 @@ int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image
 }
 
 static int check_pair(const gpv_image *f, const gpv_image *g, const gpv_solve_params *prm);
+
+int gpv_solve_batch_noalloc(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
+                            int64_t n, int32_t max_radius, const gpv_solve_params *prm, gpv_subset_result *out_dev,
+                            void *stream) {
+    if (!ctx) { set_error("ctx is NULL"); return GPV_ERR_INVALID; }
+    if (int rc = check_pair(f, g, prm)) return rc;
+    if (prm->precision != GPV_PREC_MIXED) {
+        set_error("gpv_solve_batch_noalloc runs the mixed-precision solve only");
+        return GPV_ERR_INVALID;
+    }
+    if (n < 0 || (n > 0 && (!desc_dev || !out_dev)) || n > INT32_MAX) { set_error("invalid batch arrays"); return GPV_ERR_INVALID; }
+    if (n == 0) return GPV_SUCCESS;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    return solve_noalloc_launch(ctx, f, g, desc_dev, n, max_radius, prm, out_dev, s);
+}
+
 static int radius_class(int r) { return r <= 20 ? 0 : (r <= 40 ? 1 : 2); }
 
 static void tune_cache_load(gpv_context *ctx) {

@@ -162,6 +162,23 @@ int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image
                            const gpv_subset_desc *desc_dev, const int32_t *work_order_dev, int64_t n,
                            const gpv_solve_params *params, gpv_subset_result *out_dev, void *stream);
 
+/* ---- batched subset solve without device allocation ---------------------
+ * No counterpart in the reference: an extra entry point for callers that may
+ * not allocate device memory on the solve path (their device memory belongs
+ * to another framework's pool, or an allocation's implicit device-wide
+ * synchronisation is not acceptable in their loop).  Same arguments and
+ * results as gpv_solve_batch_device (mixed precision, device arrays, async
+ * on `stream`), but all working memory comes from one static device array of
+ * 64 MiB that every GPU loading this library holds until exit: subsets up to
+ * radius 32 only (max_radius > 32 is rejected with GPV_ERR_INVALID; subsets
+ * above max_radius get GPV_INVALID_SUBSET), no work-order array.  The first
+ * call on a device performs a one-time set-up that synchronises `stream`, so
+ * make it before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU race, so serialise them.  Allocates nothing. */
+int gpv_solve_batch_noalloc(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
+                            int64_t n, int32_t max_radius, const gpv_solve_params *params,
+                            gpv_subset_result *out_dev, void *stream);
+
 /* ---- autotuning (no counterpart in the reference) ------------------------
  * Times the candidate launch shapes of the mixed-precision kernel (threads
  * per subset block) on a sample of up to sample_per_class subsets of each
