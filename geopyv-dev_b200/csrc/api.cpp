@@ -517,6 +517,46 @@ int gpv_solve_batch_noalloc(gpv_context *ctx, const gpv_image *f, const gpv_imag
     return solve_noalloc_launch(ctx, f, g, desc_dev, n, max_radius, prm, out_dev, s);
 }
 
+// ---- mesh driver ----------------------------------------------------------
+
+struct GpuMeshSolver {
+    gpv_context *ctx;
+    const gpv_image *f, *g;
+    gpv_solve_params prm;
+};
+
+static int gpu_mesh_solver(void *user, const gpv_subset_desc *desc, int64_t n, double tolerance,
+                           gpv_subset_result *out) {
+    auto *S = static_cast<GpuMeshSolver *>(user);
+    gpv_solve_params q = S->prm;
+    q.tolerance = tolerance;
+    return gpv_solve_batch(S->ctx, S->f, S->g, desc, n, &q, out);
+}
+
+int gpv_mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements, int64_t n_elements,
+                   int32_t nodes_per_element, const gpv_mesh_params *params, gpv_batch_solver_fn solver,
+                   void *solver_user, gpv_subset_result *out, int32_t *rounds, gpv_mesh_stats *stats) {
+    return gpv::mesh_drive(nodes, n_nodes, elements, n_elements, nodes_per_element, params, solver, solver_user, out,
+                           rounds, stats);
+}
+
+int gpv_mesh_solve(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const double *nodes, int64_t n_nodes,
+                   const int64_t *elements, int64_t n_elements, int32_t nodes_per_element,
+                   const gpv_mesh_params *params, gpv_subset_result *out, int32_t *rounds, gpv_mesh_stats *stats) {
+    if (!ctx || !params) { set_error("ctx or params is NULL"); return GPV_ERR_INVALID; }
+    GpuMeshSolver S;
+    S.ctx = ctx; S.f = f; S.g = g;
+    std::memset(&S.prm, 0, sizeof(S.prm));
+    S.prm.max_norm = params->max_norm;
+    S.prm.tolerance = params->tolerance;
+    S.prm.max_iterations = params->max_iterations;
+    S.prm.precision = params->precision;
+    S.prm.mask = params->mask;
+    if (int rc = check_pair(f, g, &S.prm)) return rc;
+    return gpv::mesh_drive(nodes, n_nodes, elements, n_elements, nodes_per_element, params, gpu_mesh_solver, &S, out,
+                           rounds, stats);
+}
+
 static int radius_class(int r) { return r <= 20 ? 0 : (r <= 40 ? 1 : 2); }
 
 static void tune_cache_load(gpv_context *ctx) {

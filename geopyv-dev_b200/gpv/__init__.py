@@ -17,7 +17,7 @@ from . import _lib
 from ._lib import (DESC_DTYPE, RESULT_DTYPE, PREC_FP64, PREC_MIXED, SOLVE_ETA, STATUS, GpvError, SolveParams,
                    check, lib, ptr)
 
-__all__ = ["Context", "Image", "Mask", "Subset", "solve_batch", "autotune", "make_desc", "DESC_DTYPE", "RESULT_DTYPE",
+__all__ = ["Context", "Image", "Mask", "Subset", "Mesh", "mesh_drive", "solve_batch", "autotune", "make_desc", "DESC_DTYPE", "RESULT_DTYPE",
            "GpvError", "PREC_MIXED", "PREC_FP64", "STATUS", "version"]
 
 
@@ -308,3 +308,6 @@ class Subset:
     def eta_omitted(self):
         r = self._result
         return (float(r["eta_u"]), float(r["eta_v"])) if r is not None and r["has_eta"] else None
+
+
+from .mesh import Cancelled, Mesh, mesh_drive  # noqa: E402  (uses the classes above only through arguments)

@@ -31,6 +31,27 @@ class SolveParams(ct.Structure):
                 ("mask", ct.c_void_p), ("history", ct.c_void_p)]
 
 
+# gpv_progress_fn / gpv_batch_solver_fn
+PROGRESS_FN = ct.CFUNCTYPE(ct.c_int, ct.c_void_p, ct.c_int64, ct.c_int64)
+BATCH_SOLVER_FN = ct.CFUNCTYPE(ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_double, ct.c_void_p)
+
+
+class MeshParams(ct.Structure):
+    _fields_ = [("seed_coord", ct.c_double * 2), ("seed_warp", ct.c_double * 12), ("seed_tolerance", ct.c_double),
+                ("max_norm", ct.c_double), ("tolerance", ct.c_double), ("root_rel_eps", ct.c_double),
+                ("max_iterations", ct.c_int32), ("subset_order", ct.c_int32), ("radius", ct.c_int32),
+                ("precision", ct.c_int32), ("layer_rg", ct.c_int32), ("batch_factor", ct.c_int32),
+                ("max_workers", ct.c_int32), ("reserved", ct.c_int32), ("mask", ct.c_void_p),
+                ("progress", PROGRESS_FN), ("progress_user", ct.c_void_p)]
+
+
+class MeshStats(ct.Structure):
+    _fields_ = [("n_bad", ct.c_int64), ("n_unreached", ct.c_int64), ("batches", ct.c_int64), ("solves", ct.c_int64),
+                ("retries", ct.c_int64), ("rounds", ct.c_int64), ("seed_node", ct.c_int64)]
+
+
+assert ct.sizeof(MeshParams) == 200 and ct.sizeof(MeshStats) == 56
+
 # enums
 GPV_U8, GPV_U16, GPV_F32, GPV_F64 = 1, 2, 3, 4
 PREC_MIXED, PREC_FP64 = 0, 1
@@ -67,6 +88,8 @@ SIGNATURES = {
     "gpv_probe_fp32_peak": (ct.c_int, [P, P]),
     "gpv_autotune": (ct.c_int, [P, P, P, P, I64, P, I32, P]),
     "gpv_solve_batch_noalloc": (ct.c_int, [P, P, P, P, I64, I32, P, P, P]),
+    "gpv_mesh_solve": (ct.c_int, [P, P, P, P, I64, P, I64, I32, P, P, P, P]),
+    "gpv_mesh_drive": (ct.c_int, [P, I64, P, I64, I32, P, BATCH_SOLVER_FN, P, P, P, P]),
 }
 
 _lib = None

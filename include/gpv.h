@@ -179,6 +179,78 @@ int gpv_solve_batch_noalloc(gpv_context *ctx, const gpv_image *f, const gpv_imag
                             int64_t n, int32_t max_radius, const gpv_solve_params *params,
                             gpv_subset_result *out_dev, void *stream);
 
+/* ---- mesh driver: reliability-guided propagation -------------------------
+ * Replaces the propagation stage of Mesh::solve_impl (src/mesh.rs:628-764):
+ * the seed node (find_seed_node :1682-1690, the forced seed warp and the seed
+ * tolerance, :667-677), then either the serial RG cascade
+ * (Preconditioning::Rg, :683-705, solve_neighbours_from :1112-1154) or the
+ * epsilon-band layer-RG rounds (Preconditioning::LayerRg, :706-764) whose
+ * graph colours (expand_parallel :1169-1252, greedy_graph_colour :1884-1903)
+ * are solved as one batch each.  Per node: the two attempts of solve_node
+ * (:1068-1106) -- the preconditioned warp of precondition_warp
+ * (:2130-2233), then the zero warp for the nodes that missed quality_ok --
+ * folded in ascending node order by store_result (:2385-2402).  The
+ * corrections stage (:766-790), element strains and the quality gate's
+ * error (:792-799) stay with the caller; gpv_mesh_stats.n_bad is the count
+ * that gate tests.  Every node's result (or, for a node the propagation
+ * never reaches, a zeroed result with status GPV_INVALID_SUBSET and round
+ * -1) is written to out[i]; rounds[i] (optional) is the batch round that
+ * solved node i: nodes of one round never share an element. */
+
+/* Progress observer (src/progress.rs:17-38): called after every stored
+ * node; a nonzero return cancels the solve with GPV_ERR_CANCELLED. */
+typedef int (*gpv_progress_fn)(void *user, int64_t done, int64_t total);
+
+/* Batch solver used by gpv_mesh_drive: solve n subsets at `tolerance`
+ * (the seed node uses the seed tolerance); returns a gpv_err. */
+typedef int (*gpv_batch_solver_fn)(void *user, const gpv_subset_desc *desc, int64_t n, double tolerance,
+                                   gpv_subset_result *out);
+
+/* SolveConfig + SeedConfig + LayerRgConfig (src/mesh.rs:222-262, :339-356;
+ * python/src/py_mesh.rs:215-225 defaults in brackets).  200 bytes. */
+typedef struct {
+    double seed_coord[2];
+    double seed_warp[12];     /* first 6 * subset_order used          [0]    */
+    double seed_tolerance;    /*                                      [0.9]  */
+    double max_norm;          /*                                      [1e-5] */
+    double tolerance;         /*                                      [0.75] */
+    double root_rel_eps;      /* layer-RG epsilon band                [0.02] */
+    int32_t max_iterations;   /*                                      [50]   */
+    int32_t subset_order;     /* 1 or 2 (mesh p_len = 6 * order, :636)       */
+    int32_t radius;           /* circular local mask radius                  */
+    int32_t precision;        /* gpv_precision (gpv_mesh_solve only)          */
+    int32_t layer_rg;         /* 0 = "RG", 1 = "layer-RG"             [0]    */
+    int32_t batch_factor;     /* layer-RG roots per round / worker    [4]    */
+    int32_t max_workers;      /* the worker count rounds are sized by (the
+                                 reference's rayon pool size), >= 1          */
+    int32_t reserved;
+    const gpv_mask *mask;     /* global mask or NULL (gpv_mesh_solve only)   */
+    gpv_progress_fn progress; /* or NULL */
+    void *progress_user;
+} gpv_mesh_params;
+
+typedef struct {
+    int64_t n_bad;       /* nodes without quality_ok (unreached included)   */
+    int64_t n_unreached; /* nodes the propagation never reached              */
+    int64_t batches;     /* solver calls                                     */
+    int64_t solves;      /* subset solves, zero-warp retries included        */
+    int64_t retries;     /* zero-warp second attempts                        */
+    int64_t rounds;      /* fold rounds                                      */
+    int64_t seed_node;
+} gpv_mesh_stats;
+
+/* The mesh driver on this library's GPU batch solve (gpv_solve_batch on
+ * ctx with params->precision / mask / max_norm / max_iterations).
+ * nodes: n_nodes x 2 (x, y); elements: n_elements x nodes_per_element
+ * (3 or 6) node indices.  Synchronous; host arrays. */
+int gpv_mesh_solve(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const double *nodes, int64_t n_nodes,
+                   const int64_t *elements, int64_t n_elements, int32_t nodes_per_element,
+                   const gpv_mesh_params *params, gpv_subset_result *out, int32_t *rounds, gpv_mesh_stats *stats);
+/* The same driver over any batch solver (no device work of its own). */
+int gpv_mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements, int64_t n_elements,
+                   int32_t nodes_per_element, const gpv_mesh_params *params, gpv_batch_solver_fn solver,
+                   void *solver_user, gpv_subset_result *out, int32_t *rounds, gpv_mesh_stats *stats);
+
 /* ---- autotuning (no counterpart in the reference) ------------------------
  * Times the candidate launch shapes of the mixed-precision kernel (threads
  * per subset block) on a sample of up to sample_per_class subsets of each

@@ -111,6 +111,43 @@ KATS = [
          value=42.0, points=[[0.0, 0.0], [1.5, 2.25], [3.0, 3.0]], rtol=1e-8, literal="(0.0, 0.0), (1.5, 2.25), (3.0, 3.0)"),
     dict(name="far_out_of_range_clamp", src="src/subset.rs:1845-1868", fn="clamp", shape=[8, 9], border=5, atol=1e-3,
          literal="bspline_eval(1_000_000.0, 0.0, &img)"),
+    # mesh propagation helpers (src/mesh.rs) -- checked against oracle/mesh_oracle.py
+    dict(name="connectivity_order1_corner", src="src/mesh.rs:2657-2661", fn="mesh_connectivity",
+         elements=[[0, 1, 2], [1, 3, 2]], order=1, idx=0, full=False, expected=[1, 2],
+         literal="assert_eq!(result, vec![1, 2]);"),
+    dict(name="connectivity_order1_shared_node", src="src/mesh.rs:2664-2668", fn="mesh_connectivity",
+         elements=[[0, 1, 2], [1, 3, 2]], order=1, idx=1, full=False, expected=[0, 2, 3],
+         literal="assert_eq!(result, vec![0, 2, 3]);"),
+    dict(name="connectivity_order2_corner_gets_midpoints", src="src/mesh.rs:2671-2676", fn="mesh_connectivity",
+         elements=[[0, 1, 2, 4, 5, 6], [1, 3, 2, 7, 8, 5]], order=2, idx=0, full=False, expected=[4, 6],
+         literal="assert_eq!(result, vec![4, 6]);"),
+    dict(name="connectivity_order2_midpoint_gets_corners", src="src/mesh.rs:2679-2684", fn="mesh_connectivity",
+         elements=[[0, 1, 2, 4, 5, 6], [1, 3, 2, 7, 8, 5]], order=2, idx=4, full=False, expected=[0, 1],
+         literal="assert_eq!(result, vec![0, 1]);"),
+    dict(name="connectivity_indexed_matches", src="src/mesh.rs:2693-2720", fn="mesh_adjacency",
+         cases=[[[[0, 1, 2], [1, 3, 2]], 1, 4], [[[0, 1, 2, 4, 5, 6], [1, 3, 2, 7, 8, 5]], 2, 9]],
+         literal="let elements2 = array![[0usize, 1, 2, 4, 5, 6], [1, 3, 2, 7, 8, 5]];"),
+    dict(name="find_seed_node_exact", src="src/mesh.rs:2724-2727", fn="mesh_seed",
+         nodes=[[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]], coord=[1.0, 0.0], expected=1,
+         literal="assert_eq!(find_seed_node(&nodes, [1.0, 0.0]), 1);"),
+    dict(name="find_seed_node_nearest", src="src/mesh.rs:2730-2734", fn="mesh_seed",
+         nodes=[[0.0, 0.0], [1.0, 0.0], [0.0, 1.0], [1.0, 1.0]], coord=[0.4, 0.4], expected=0,
+         literal="assert_eq!(find_seed_node(&nodes, [0.4, 0.4]), 0);"),
+    dict(name="project_warp_second_order_terms", src="src/mesh.rs:2804-2813", fn="mesh_project",
+         p={"4": 1.0, "8": 1.0}, dx=2.0, dy=3.0, slot=4, expected=3.0, atol=1e-12,
+         literal="let p_proj = project_warp(&p, 2.0, 3.0);"),
+    dict(name="project_warp_every_slot", src="src/mesh.rs:3237-3246", fn="mesh_project_quad",
+         q=[0.1, -0.2, 0.02, 0.07, 0.03, -0.01, 0.004, 0.008, 0.005, 0.009, 0.006, -0.003], c=[2.0, -1.0],
+         d=[3.0, 5.0], atol=1e-12, literal="let (cx, cy, dx, dy) = (2.0, -1.0, 3.0, 5.0);"),
+    dict(name="affine_field_fit_recovers_exact_linear_field", src="src/mesh.rs:2819-2848", fn="mesh_affine_fit",
+         nodes=[[0.0, 0.0], [10.0, 0.0], [0.0, 10.0], [10.0, 10.0], [5.0, 2.0]], u=[0.1, -0.05, 2.0],
+         v=[-0.02, 0.08, -1.0], target=[3.0, 7.0], atol=1e-9, literal="v = -0.02*x + 0.08*y - 1.0"),
+    dict(name="affine_field_fit_none_when_collinear", src="src/mesh.rs:2851-2857", fn="mesh_affine_collinear",
+         nodes=[[0.0, 0.0], [1.0, 0.0], [2.0, 0.0]], target=[1.0, 5.0],
+         literal="assert!(affine_field_fit(&nodes, [1.0, 5.0], &trusted, &p, 6).is_none());"),
+    dict(name="precondition_warp_thresholds", src="src/mesh.rs:2861-2878", fn="mesh_precondition",
+         nodes=[[0.0, 0.0], [1.0, 0.0]], c_zncc=[0.9, 0.95], p=[[1.0, 2.0, 0, 0, 0, 0], [3.0, 4.0, 0, 0, 0, 0]],
+         target=[5.0, 5.0], atol=1e-12, literal="let one = precondition_warp(&nodes, [5.0, 5.0], &[1], &c_zncc, &p, 6);"),
 ]
 
 

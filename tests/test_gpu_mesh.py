@@ -1,0 +1,115 @@
+"""gpv_mesh_solve (the mesh driver over the GPU batch solve) against the
+oracle's restatement of the reference propagation over the FP64 oracle.
+
+FP64 solves: same seed, same batch rounds, same flags and iterations, warps
+within 1e-7.  Mixed precision: same flags, displacement within 1e-3 px and
+gradient terms within 1e-5 (the batch-solve parity bar).
+"""
+import numpy as np
+import pytest
+
+import mesh_cases as MC
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_run(oracle, f, g, border, nodes, el, **kw):
+    import mesh_oracle as M
+    solver = MC.oracle_solver(oracle, f, g, border)
+    kw = dict(kw)
+    kw["batch_factor"] = kw.pop("layer_rg_batch_factor", 4)
+    kw["root_rel_eps"] = kw.pop("layer_rg_root_rel_eps", 0.02)
+    kw["max_workers"] = kw.pop("layer_rg_max_workers", 1)
+    r = M.solve_mesh(nodes, el, solver, desc_dtype=oracle.DESC_DTYPE, **kw)
+    r["results"] = np.array(r["results"], dtype=oracle.RESULT_DTYPE)
+    return r
+
+
+def _gpu_run(gpv, f, g, border, nodes, el, precision, **kw):
+    F = gpv.Image(image_gs=f, border=border, keep_f64=(precision == gpv.PREC_FP64))
+    G = gpv.Image(image_gs=g, border=border, keep_f64=(precision == gpv.PREC_FP64))
+    radius = kw.pop("radius")
+    m = gpv.Mesh(nodes, el, F, G)
+    m.solve(radius, precision=precision, override_active=True, **kw)
+    return m
+
+
+def _compare(m, ref, precision):
+    r, q = m.results, ref["results"]
+    assert m.seed_node == ref["seed_node"]
+    assert np.array_equal(r["status"], q["status"])
+    assert np.array_equal(r["quality_ok"], q["quality_ok"])
+    ok = r["status"] == 0
+    if precision == 1:
+        assert np.array_equal(m.rounds, ref["rounds"])
+        assert np.array_equal(r["iterations"], q["iterations"])
+        assert np.abs(r["p"][ok] - q["p"][ok]).max() < 1e-7
+    else:
+        assert np.abs(r["p"][ok, :2] - q["p"][ok, :2]).max() <= 1e-3
+        assert np.abs(r["p"][ok, 2:6] - q["p"][ok, 2:6]).max() <= 1e-5
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
+@pytest.mark.parametrize("prec", ["RG", "layer-RG"])
+def test_band_mesh_matches_oracle(gpv_mod, oracle, precision, prec):
+    f = MC.texture(100)
+    g = MC.shift_band(f, 50, 1.5, -1.5)
+    nodes, el = MC.grid_mesh()
+    kw = dict(radius=6, seed_coord=(50.0, 30.0), seed_tolerance=0.5, tolerance=0.5, subset_order=1,
+              preconditioning=prec, layer_rg_max_workers=2)
+    ref = _oracle_run(oracle, f, g, 15, nodes, el, **kw)
+    m = _gpu_run(gpv_mod, f, g, 15, nodes, el, precision, **kw)
+    _compare(m, ref, precision)
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["mixed", "fp64"])
+@pytest.mark.parametrize("subset_order", [1, 2])
+def test_order2_mesh_matches_oracle(gpv_mod, oracle, precision, subset_order):
+    f = MC.texture(100)
+    g = MC.shift_uniform(f, 1.5)
+    nodes, el = MC.to_order2(*MC.grid_mesh(n_side=6, step=12.0))
+    kw = dict(radius=8, seed_coord=(50.0, 50.0), seed_tolerance=0.5, tolerance=0.5, subset_order=subset_order,
+              preconditioning="layer-RG", layer_rg_max_workers=2, seed_warp=[1.4, 0.0])
+    ref = _oracle_run(oracle, f, g, 15, nodes, el, **kw)
+    m = _gpu_run(gpv_mod, f, g, 15, nodes, el, precision, **kw)
+    _compare(m, ref, precision)
+
+
+def test_large_mesh_layer_rg(gpv_mod, oracle):
+    """A 1024 x 1024 speckle pair with a smooth field, 1,600-node mesh,
+    layer-RG rounds sized for 64 workers: one GPU batch per colour."""
+    from gpv import synth
+    W = synth.workload(1, scale_down=1)
+    f, g = W["f"].astype(np.float64), W["g"].astype(np.float64)
+    nodes, el = MC.grid_mesh(n_side=40, start=60.0, step=23.0)
+    kw = dict(radius=20, seed_coord=(512.0, 512.0), seed_tolerance=0.9, tolerance=0.75, subset_order=1,
+              preconditioning="layer-RG", layer_rg_max_workers=64)
+    ref = _oracle_run(oracle, f, g, 20, nodes, el, **kw)
+    m = _gpu_run(gpv_mod, f, g, 20, nodes, el, 0, **kw)
+    _compare(m, ref, 0)
+    assert m.quality_ok.all()
+    st = m.stats
+    assert st["batches"] < len(nodes) / 10, st  # batched, not node by node
+    # layer-RG is run-to-run deterministic on the GPU too
+    again = _gpu_run(gpv_mod, f, g, 20, nodes, el, 0, **kw)
+    assert again.results.tobytes() == m.results.tobytes()
+
+
+def test_mesh_api_and_gate(gpv_mod):
+    f = MC.texture(100)
+    g = MC.shift_uniform(f, 1.5)
+    nodes, el = MC.grid_mesh()
+    F = gpv_mod.Image(image_gs=f, border=15)
+    G = gpv_mod.Image(image_gs=g, border=15)
+    m = gpv_mod.Mesh(nodes, el, F, G)
+    assert not m.solved
+    m.solve(gpv_mod.Mask("local", shape="circle", size=8), seed_coord=(50.0, 50.0), seed_tolerance=0.5,
+            tolerance=0.5, override_active=False)
+    assert m.solved and m.quality_ok.all()
+    assert np.abs(m.displacements[:, 0] - 1.5).max() < 0.05
+    assert m.p.shape == (len(nodes), 6) and m.iterations.min() >= 1
+    # a tolerance no subset reaches fails the quality gate unless overridden
+    with pytest.raises(gpv_mod.GpvError, match="mesh unsolvable"):
+        m.solve(8, seed_coord=(50.0, 50.0), seed_tolerance=0.5, tolerance=1.01)
+    m.solve(8, seed_coord=(50.0, 50.0), seed_tolerance=0.5, tolerance=1.01, override_active=True)
+    assert not m.quality_ok.any()

@@ -160,6 +160,56 @@ def test_reference_kat(oracle, k):
         assert np.isfinite(far) and abs(far) < 200.0 and abs(far - edge) < k["atol"]
         _, g = O.evaluate(C, img.shape, k["border"], [[1_000_000.0, -1_000_000.0]], grad=True)
         assert np.all(np.isfinite(g)) and np.all(np.abs(g) < 200.0)
+    elif fn.startswith("mesh_"):
+        _mesh_kat(k)
+    else:
+        raise AssertionError(f"unknown KAT kind {fn}")
+
+
+def _mesh_kat(k):
+    import mesh_oracle as M
+    fn = k["fn"]
+    if fn == "mesh_connectivity":
+        assert M.connectivity(k["elements"], k["order"], k["idx"], k["full"]) == k["expected"]
+    elif fn == "mesh_adjacency":  # the per-node table equals the brute-force scan, both relations
+        for elements, order, n in k["cases"]:
+            full, edge = M.adjacency(elements, order, n)
+            for i in range(n):
+                assert full[i] == M.connectivity(elements, order, i, True)
+                assert edge[i] == M.connectivity(elements, order, i, False)
+    elif fn == "mesh_seed":
+        assert M.find_seed_node(k["nodes"], k["coord"]) == k["expected"]
+    elif fn == "mesh_project":
+        p = [0.0] * 12
+        for slot, v in k["p"].items():
+            p[int(slot)] = v
+        assert abs(M.project_warp(p, k["dx"], k["dy"])[k["slot"]] - k["expected"]) < k["atol"]
+    elif fn == "mesh_project_quad":
+        q = k["q"]
+
+        def full(x, y):  # quad_warp (src/particle.rs:2624-2635), every slot
+            u, v = _quad_warp(q, x, y)
+            return [u, v, q[2] + q[6] * x + q[8] * y, q[3] + q[7] * x + q[9] * y, q[4] + q[8] * x + q[10] * y,
+                    q[5] + q[9] * x + q[11] * y] + list(q[6:])
+        (cx, cy), (dx, dy) = k["c"], k["d"]
+        w = M.project_warp(full(cx, cy), dx, dy)
+        assert np.abs(np.array(w) - full(cx + dx, cy + dy)).max() < k["atol"]
+    elif fn == "mesh_affine_fit":
+        (ux, uy, u0), (vx, vy, v0) = k["u"], k["v"]
+        nodes = k["nodes"]
+        p = [[ux * x + uy * y + u0, vx * x + vy * y + v0, 0, 0, 0, 0] for x, y in nodes]
+        t = k["target"]
+        fit = M.affine_field_fit(nodes, t, list(range(len(nodes))), p, 6)
+        want = [ux * t[0] + uy * t[1] + u0, vx * t[0] + vy * t[1] + v0, ux, vx, uy, vy]
+        assert np.abs(np.array(fit) - want).max() < k["atol"]
+    elif fn == "mesh_affine_collinear":
+        nodes = k["nodes"]
+        assert M.affine_field_fit(nodes, k["target"], [0, 1, 2], [[0.0] * 6] * 3, 6) is None
+    elif fn == "mesh_precondition":
+        nodes, c, p, t = k["nodes"], k["c_zncc"], k["p"], k["target"]
+        assert all(v == 0.0 for v in M.precondition_warp(nodes, t, [], c, p, 6))
+        one = M.precondition_warp(nodes, t, [1], c, p, 6)
+        assert abs(one[0] - 3.0) < k["atol"] and abs(one[1] - 4.0) < k["atol"]
     else:
         raise AssertionError(f"unknown KAT kind {fn}")
 
