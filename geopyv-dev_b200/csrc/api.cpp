@@ -164,8 +164,8 @@ int gpv_context_create(int device, gpv_context **out) {
     return GPV_SUCCESS;
 }
 
-int gpv_context_destroy(gpv_context *ctx) {
-    if (!ctx) return GPV_SUCCESS;
+static void context_release(gpv_context *ctx) {
+    if (ctx->refs.fetch_sub(1) != 1) return;
     DeviceGuard dg(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->offs, &ctx->slots, &ctx->tab_off, &ctx->tab_n, &ctx->scratch, &ctx->queue, &ctx->desc_dev, &ctx->out_dev,
@@ -177,6 +177,11 @@ int gpv_context_destroy(gpv_context *ctx) {
         if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
+}
+
+int gpv_context_destroy(gpv_context *ctx) {
+    if (!ctx) return GPV_SUCCESS;
+    context_release(ctx);
     return GPV_SUCCESS;
 }
 
@@ -191,6 +196,7 @@ static int image_alloc(gpv_context *ctx, int64_t h, int64_t w, int32_t border, u
     if (!dtype_size(dtype)) { set_error("unknown pixel dtype"); return GPV_ERR_INVALID; }
     auto *img = new gpv_image();
     img->ctx = ctx;
+    ctx->refs.fetch_add(1);
     img->h = h;
     img->w = w;
     img->border = border;
@@ -208,6 +214,7 @@ static int image_alloc(gpv_context *ctx, int64_t h, int64_t w, int32_t border, u
         cudaFree(img->c64);
         cudaFree(img->rowpass);
         delete img;
+        context_release(ctx);
         return GPV_ERR_NOMEM;
     }
     *out = img;
@@ -284,7 +291,9 @@ int gpv_image_destroy(gpv_image *img) {
     cudaFree(img->c64);
     cudaFree(img->rowpass);
     cudaFree(img->px_dev);
+    gpv_context *ctx = img->ctx;
     delete img;
+    context_release(ctx);
     return GPV_SUCCESS;
 }
 
@@ -344,6 +353,7 @@ int gpv_mask_create(gpv_context *ctx, const uint8_t *mask, int64_t h, int64_t w,
     DeviceGuard dg(ctx->device);
     auto *m = new gpv_mask();
     m->ctx = ctx;
+    ctx->refs.fetch_add(1);
     m->h = h;
     m->w = w;
     cudaError_t e = cudaMalloc(&m->dev, (size_t)h * w);
@@ -352,6 +362,7 @@ int gpv_mask_create(gpv_context *ctx, const uint8_t *mask, int64_t h, int64_t w,
         set_error(std::string("mask upload: ") + cudaGetErrorString(e));
         cudaFree(m->dev);
         delete m;
+        context_release(ctx);
         return GPV_ERR_CUDA;
     }
     *out = m;
@@ -360,9 +371,13 @@ int gpv_mask_create(gpv_context *ctx, const uint8_t *mask, int64_t h, int64_t w,
 
 int gpv_mask_destroy(gpv_mask *m) {
     if (!m) return GPV_SUCCESS;
-    DeviceGuard dg(m->ctx->device);
-    cudaFree(m->dev);
+    gpv_context *ctx = m->ctx;
+    {
+        DeviceGuard dg(ctx->device);
+        cudaFree(m->dev);
+    }
     delete m;
+    context_release(ctx);
     return GPV_SUCCESS;
 }
 

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -66,6 +67,10 @@ struct gpv_context {
     int mixed_blocks_per_sm = 0;
     int tuned_threads[3] = {0, 0, 0};  // autotuned threads per block by radius class
     int force_threads = 0;             // set while the autotuner times a candidate
+    // owner reference + one per image / mask created on it: the context is
+    // freed when gpv_context_destroy and every dependant's destroy have run,
+    // in whatever order they come
+    std::atomic<int> refs{1};
 };
 
 struct gpv_image {

@@ -108,6 +108,8 @@ size_t gpv_last_error(char *buf, size_t len);
 
 /* ---- context: one device, one stream, reusable workspace ---------------- */
 int gpv_context_create(int device, gpv_context **out);
+/* The context's resources are freed once gpv_context_destroy and the destroy
+ * of every image and mask created on it have all run, in any order. */
 int gpv_context_destroy(gpv_context *ctx);
 /* The context's CUDA stream, as a cudaStream_t cast to void*. */
 void *gpv_context_stream(gpv_context *ctx);

@@ -78,6 +78,17 @@ def to_order2(nodes, elements):
     return np.array(nodes), np.array(out, dtype=np.int64)
 
 
+def speckle_quadratic(size=256, seed=5):
+    """A seeded speckle pair under a smooth field (translation + affine +
+    quadratic terms about the centre) and that field."""
+    from gpv import synth
+    c = size / 2.0
+    field = synth.make_field(xc=c, yc=c, t=(1.3, -0.7), a=(0.01, 0.004, -0.006, 0.008),
+                             q=(2e-5, -1e-5, 1e-5, -2e-5, 1e-5, 3e-5))
+    f, g = synth.pair(size, size, field, seed)
+    return f.astype(np.float64), g.astype(np.float64), field
+
+
 def oracle_solver(oracle, f, g, border, max_norm=1e-5, max_iterations=50, mask=None):
     """solver(desc, tolerance) over the FP64 oracle for images f, g."""
     Cf = oracle.get_c(np.asarray(f, dtype=np.float64), border)
