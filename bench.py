@@ -38,6 +38,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "geopyv-dev_b200"))
 
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of the icgn_tile<2,128>
+# launch of one full-size second-order step (690.36 + 323.75 MB)
+ICGN_C2_DRAM_BYTES = 1014.11e6
+
 METRIC = "ICGN subsets/s at <=1e-3 px vs FP64 oracle; p50/p99 served solve latency"
 
 
@@ -52,6 +56,7 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mesh", action="store_true", help="skip the mesh-propagation leg")
     return ap.parse_args()
 
 
@@ -88,8 +93,12 @@ def max_over_ranks(x, world):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons during the timed region."""
+    """SM clock and clock-event reasons during the timed region, read through
+    NVML every 10 ms (nvidia-smi every 200 ms when NVML is unavailable).
+    Reads only; changes no setting."""
 
+    NAMES = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap",
+             0x80: "hw_power_brake_slowdown"}
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -97,9 +106,44 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm_mhz, reason bits)
+        self.smax = None
+        self.stop_ev = threading.Event()
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        idx = self.device
+        if vis:
+            ids = [v.strip() for v in vis.split(",") if v.strip()]
+            if self.device < len(ids) and ids[self.device].isdigit():
+                idx = int(ids[self.device])
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
 
     def start(self):
+        try:
+            nv, h = self._handle()
+            self.nvml = (nv, h)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+
+            def poll():
+                while not self.stop_ev.is_set():
+                    try:
+                        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                             int(get_reasons(h))))
+                    except Exception:
+                        pass
+                    self.stop_ev.wait(0.01)
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -114,8 +158,18 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_ev.set()
+            self.t.join(timeout=2)
+            sm = [c for c, _ in self.samples]
+            bits = 0
+            for _, b in self.samples:
+                bits |= b
+            reasons = sorted(n for k, n in self.NAMES.items() if bits & k)
+            return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.smax, "reasons": reasons,
+                    "samples": len(sm), "source": "NVML, 10 ms"}
         if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -136,7 +190,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # ---------------------------------------------------------------------------
@@ -146,6 +200,15 @@ def load_workload(args):
     W = synth.workload(args.config, scale_down=args.scale_down)
     W["gen_s"] = time.time() - t
     return W
+
+
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool (MEASURED_PEAKS.json), else
+    the pool's earlier measurement."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        return 6650.0
 
 
 def algorithmic_flop(res):
@@ -186,6 +249,82 @@ def cpu_baseline(W, args, nthreads=None, seconds=None, rng_seed=7):
     t_step = 2 * t_pref1 + per * n  # prefilter both images + every subset
     return dict(value=n / t_step, cores=int(nthreads), per_subset_s=per, prefilter_s=t_pref1,
                 sample_idx=sample, sample_res=ref, n=n, solve_s=t_solve)
+
+
+# ---------------------------------------------------------------------------
+def grid_mesh(coords):
+    """Two triangles per cell of a structured node grid (row-major coords)."""
+    xs = np.unique(coords[:, 0])
+    ys = np.unique(coords[:, 1])
+    nx = len(xs)
+    el = []
+    for r in range(len(ys) - 1):
+        for c in range(nx - 1):
+            a, b, d, e = r * nx + c, r * nx + c + 1, (r + 1) * nx + c, (r + 1) * nx + c + 1
+            el.append((a, b, d))
+            el.append((b, e, d))
+    return np.array(el, dtype=np.int64)
+
+
+def mesh_leg(W, F, G, args, cpu=True):
+    """Mesh propagation (gpv_mesh_solve, layer-RG) over the workload's image
+    pair: a 20 px structured triangular mesh, second-order subsets of the
+    workload's radius, rounds sized for 64 workers.  CPU rate: the oracle's
+    restatement of the propagation over the FP64 oracle, on a sub-mesh."""
+    import gpv
+    from gpv import synth
+    h, w = W["f"].shape
+    r = int(W["radius"].max())
+    margin = r + 3 + 0.012 * h
+    nodes = synth.grid(h, w, 20, margin)
+    el = grid_mesh(nodes)
+    c = nodes[np.argmin(np.sum((nodes - [(w - 1) / 2.0, (h - 1) / 2.0]) ** 2, axis=1))]
+    seed_warp = np.zeros(12)
+    seed_warp[:2] = synth.displacement(W["field"], [c])[0]
+    kw = dict(seed_coord=tuple(c), seed_warp=list(seed_warp), subset_order=2, preconditioning="layer-RG",
+              layer_rg_max_workers=64, max_norm=1e-5, max_iterations=50)
+    m = gpv.Mesh(nodes, el, F, G)
+    m.solve(r, override_active=True, **kw)  # warm-up (tables, workspace)
+    t0 = time.perf_counter()
+    m.solve(r, override_active=True, **kw)
+    t = time.perf_counter() - t0
+    truth = synth.displacement(W["field"], nodes)
+    out = {"nodes": int(len(nodes)), "elements": int(len(el)), "radius": r, "order": 2,
+           "preconditioning": "layer-RG, batch_factor 4, root_rel_eps 0.02, max_workers 64",
+           "ms": 1e3 * t, "nodes_per_s": len(nodes) / t, "batches": m.stats["batches"],
+           "subset_solves": m.stats["solves"], "quality_ok_frac": float(m.quality_ok.mean()),
+           "max_err_vs_field_px_quality_ok": float(np.abs(m.displacements - truth)[m.quality_ok].max()),
+           "not_quality_ok": int((~m.quality_ok).sum()),
+           "timing": "host wall clock around the synchronous C-ABI call (host driver + every batch)"}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import mesh_oracle as MO
+        import oracle as O
+        half = 30 * 20  # a 61 x 61-node sub-mesh around the seed
+        sub = np.all(np.abs(nodes - c) <= half + 1e-9, axis=1)
+        idx = np.nonzero(sub)[0]
+        remap = -np.ones(len(nodes), np.int64)
+        remap[idx] = np.arange(len(idx))
+        sel = np.all(sub[el], axis=1)
+        sel_el = remap[el[sel]]
+        Cf = O.get_c(W["f"].astype(np.float64), 20)
+        Cg = O.get_c(W["g"].astype(np.float64), 20)
+
+        def solver(d, tol):
+            return O.solve_batch(Cf, Cg, W["f"].shape, 20, d, max_norm=1e-5, max_iterations=50, tolerance=tol)
+        t0 = time.perf_counter()
+        ref = MO.solve_mesh(nodes[idx], sel_el, solver, desc_dtype=O.DESC_DTYPE, radius=r, seed_coord=tuple(c),
+                            seed_warp=list(seed_warp), subset_order=2, preconditioning="layer-RG", max_workers=64)
+        tc = time.perf_counter() - t0
+        ms = gpv.Mesh(nodes[idx], sel_el, F, G)
+        ms.solve(r, override_active=True, **kw)
+        rp = np.array([x["p"][:2] for x in ref["results"]])
+        out["cpu_oracle"] = {"nodes": int(len(idx)), "s": tc, "nodes_per_s": len(idx) / tc,
+                             "cores": int(O.lib().gpvo_max_threads()),
+                             "max_disp_diff_vs_gpu_px": float(np.abs(ms.displacements - rp).max()),
+                             "same_rounds": bool(np.array_equal(ms.rounds, ref["rounds"])),
+                             "what": "oracle/mesh_oracle.py over the FP64 C oracle (one OpenMP batch per colour)"}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -251,7 +390,9 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.Stream()  # a real stream: the C ABI maps NULL to the context stream
     torch.cuda.set_stream(stream)
     sptr = ct.c_void_p(stream.cuda_stream)
-    launches_per_step = 5  # 2 images x (row pass + column pass) + 1 solve
+    # 2 images x (row pass + column pass), then the solve: the mixed form is
+    # count_orders + scatter_orders + one tile kernel per order; FP64 one kernel
+    launches_per_step = 4 + (5 if prec == gpv.PREC_MIXED else 1)
     # the prefilter runs on the library's context stream, the solve on torch's
     # current stream; events order the two
     ctx_stream = torch.cuda.ExternalStream(ctx.stream)
@@ -353,19 +494,24 @@ def run_ours(args, world, rank, local):
                "flag_agreement": float(np.mean((res["converged"][idx] == ref["converged"]) &
                                                (res["quality_ok"][idx] == ref["quality_ok"]))),
                "iteration_agreement": float(np.mean(res["iterations"][idx] == ref["iterations"]))}
+    mesh = None
+    if not args.no_mesh and args.config == 2:
+        mesh = mesh_leg(W, F, G, args, cpu=not args.no_cpu_baseline)
     flop = algorithmic_flop(res)
     solve_avg_ms = float(np.mean(solve_ms))
     achieved = flop / (solve_avg_ms * 1e-3) / 1e12
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "icgn_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            tj = json.load(open(tpath))
-            traffic = float(tj["bytes_per_subset_iteration"]) * float(np.sum(res["iterations"])) + \
-                float(tj.get("bytes_per_subset_setup", 0.0)) * n
-        except Exception:
-            traffic = None
+    # DRAM bytes (read + write) of one solve launch, from ncu at full size
+    # (profiles/icgn_tile_c2.md): known for the second-order workload only
+    traffic = ICGN_C2_DRAM_BYTES if (args.config == 2 and args.scale_down == 1 and prec == gpv.PREC_MIXED) else None
     samples = float(np.sum(res["n_px"].astype(np.float64) * (res["iterations"] + 1)))
+    # roofline time = the slower of the tap FMAs at the FP32 peak and the
+    # coefficient-window bytes at the measured HBM bandwidth
+    coef_bytes = float(np.sum((res["iterations"].astype(np.float64) + 1.0) *
+                              (2.0 * desc["radius"].astype(np.float64) + 6.0) ** 2 * 4.0))
+    hbm_gbs = measured_hbm_gbs()
+    t_fma = flop / (fp32_peak * 1e12) if fp32_peak else 0.0
+    t_bytes = coef_bytes / (hbm_gbs * 1e9)
+    l2_bytes = 2 * 4 * (h + 40) * (w + 40) + 2 * 8 * h * (w + 40)
     line = {
         "metric": METRIC, "value": value, "unit": "subsets/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -374,7 +520,9 @@ def run_ours(args, world, rank, local):
                    "radius": max_r, "order": 2 if args.config == 2 else "mixed", "max_norm": 1e-5,
                    "max_iterations": 50, "precision": args.precision,
                    "step": "prefilter(f)+prefilter(g)+batched ICGN solve",
-                   "l2": "inputs larger than L2: 2 x 4136^2 FP32 coefficients + FP64 row pass (~410 MB) rewritten each step",
+                   "l2": (("inputs larger than L2" if l2_bytes > 126e6 else "inputs SMALLER than L2 (profiling case)") +
+                          f": 2 x {h + 40}x{w + 40} FP32 coefficients + FP64 row passes ({l2_bytes / 1e6:.0f} MB)"
+                          " rewritten each step"),
                    "parallelism": f"replicas x{world}",
                    "tuned_threads_per_subset": {"r<=20": tuned[0], "r21-40": tuned[1], "r>40": tuned[2]}},
         "solve_ms": solve_avg_ms, "prefilter_ms": t_max / args.steps - solve_avg_ms,
@@ -382,16 +530,24 @@ def run_ours(args, world, rank, local):
         "iterations_mean": float(np.mean(res["iterations"])),
         "converged_frac": float(np.mean(res["converged"])),
         "accuracy": acc,
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
-                     "kernel": "icgn_mixed" if prec == gpv.PREC_MIXED else "icgn_fp64",
+        "roofline": {"bound": "fp32" if t_fma >= t_bytes else "hbm", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
+                     "kernel": "icgn_tile<2,128>" if prec == gpv.PREC_MIXED else "icgn_fp64",
                      "peak_source": "measured live: register-only FP32 FMA kernel (gpv_probe_fp32_peak)",
-                     "work": "2 x (42 FMA per target sample x iterations + 90 FMA per reference sample)"},
+                     "work": "2 x (42 FMA per target sample x iterations + 90 FMA per reference sample)",
+                     "t_fma_ms": 1e3 * t_fma, "t_bytes_ms": 1e3 * t_bytes,
+                     "roofline_frac": max(t_fma, t_bytes) / (solve_avg_ms * 1e-3),
+                     "hbm": {"algorithmic_bytes": coef_bytes, "achieved_gbs": coef_bytes / (solve_avg_ms * 1e-3) / 1e9,
+                             "peak_gbs": hbm_gbs, "frac": coef_bytes / (solve_avg_ms * 1e-3) / 1e9 / hbm_gbs,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                             "bytes": "(2r+6)^2 x 4 B coefficient window per subset per iteration and per setup"}},
         "e2e": {"value": e2e_value, "unit": "subsets/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)), "p99": 1e3 * float(np.percentile(lat, 99))}},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": cl,
     }
+    if mesh is not None:
+        line["mesh"] = mesh
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": "subsets/s", "cores": cpu["cores"], "kind": "port",
                                 "sample": f"{len(cpu['sample_idx'])} random subsets of the same batch solved by the FP64 C "

@@ -39,6 +39,20 @@ struct DevBuf {
     void release();
 };
 
+// Makes `dev` current for a scope and restores the caller's device.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace gpv
 
 struct gpv_context {

@@ -89,6 +89,11 @@ SIGNATURES = {
     "gpv_autotune": (ct.c_int, [P, P, P, P, I64, P, I32, P]),
     "gpv_solve_batch_noalloc": (ct.c_int, [P, P, P, P, I64, I32, P, P, P]),
     "gpv_mesh_solve": (ct.c_int, [P, P, P, P, I64, P, I64, I32, P, P, P, P]),
+    "gpv_sequence_create": (ct.c_int, [P, P, P, P, I64, P, I32, U32, P]),
+    "gpv_sequence_frame": (ct.c_int, [P, P, I32, P]),
+    "gpv_sequence_results_device": (P, [P]),
+    "gpv_sequence_frames": (I64, [P]),
+    "gpv_sequence_destroy": (ct.c_int, [P]),
     "gpv_mesh_drive": (ct.c_int, [P, I64, P, I64, I32, P, BATCH_SOLVER_FN, P, P, P, P]),
 }
 

@@ -67,6 +67,7 @@ typedef struct gpv_context gpv_context;
 typedef struct gpv_image gpv_image;
 typedef struct gpv_mask gpv_mask;
 typedef struct gpv_server gpv_server;
+typedef struct gpv_sequence gpv_sequence;
 
 /* One subset to solve (src/subset.rs:836-843 Subset::new arguments +
  * src/subset.rs:992-999 p_0).  Layout fixed: 120 bytes. */
@@ -180,6 +181,29 @@ int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image
 int gpv_solve_batch_noalloc(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
                             int64_t n, int32_t max_radius, const gpv_solve_params *params,
                             gpv_subset_result *out_dev, void *stream);
+
+/* ---- sequence: frame-to-frame tracking with device-resident seeds -------
+ * The per-frame work of Sequence::solve (src/sequence.rs:624-968) for a
+ * fixed set of subsets: each frame's target is re-prefiltered in place
+ * (a1 again, :693-694, :914) and every subset is solved against the fixed
+ * reference f with its initial warp taken from its own last converged
+ * solution (desc p0 on the first frame).  Seeds and results stay on the
+ * device; from the second frame on, the frame's device work (prefilter,
+ * seeding, solve) is one CUDA graph replayed per frame, unless
+ * GPV_SEQUENCE_NO_GRAPH is given or the image is narrower than 89 px.
+ * f and g must outlive the sequence; g's coefficients are overwritten by
+ * every frame. */
+#define GPV_SEQUENCE_NO_GRAPH 1u
+int gpv_sequence_create(gpv_context *ctx, const gpv_image *f, gpv_image *g, const gpv_subset_desc *desc, int64_t n,
+                        const gpv_solve_params *params, int32_t dtype, uint32_t flags, gpv_sequence **out);
+/* One frame: px (h x w of the sequence's dtype) on the host, or on the
+ * device when px_on_device != 0.  out (host, n results) may be NULL: the
+ * frame then stays asynchronous on the context stream and its results are
+ * at gpv_sequence_results_device() until the next frame. */
+int gpv_sequence_frame(gpv_sequence *s, const void *px, int32_t px_on_device, gpv_subset_result *out);
+gpv_subset_result *gpv_sequence_results_device(gpv_sequence *s);
+int64_t gpv_sequence_frames(const gpv_sequence *s);
+int gpv_sequence_destroy(gpv_sequence *s);
 
 /* ---- mesh driver: reliability-guided propagation -------------------------
  * Replaces the propagation stage of Mesh::solve_impl (src/mesh.rs:628-764):
