@@ -17,7 +17,7 @@ from . import _lib
 from ._lib import (DESC_DTYPE, RESULT_DTYPE, PREC_FP64, PREC_MIXED, SOLVE_ETA, STATUS, GpvError, SolveParams,
                    check, lib, ptr)
 
-__all__ = ["Context", "Image", "Mask", "Subset", "Mesh", "mesh_drive", "solve_batch", "autotune", "make_desc", "DESC_DTYPE", "RESULT_DTYPE",
+__all__ = ["Context", "Image", "Mask", "Subset", "Mesh", "mesh_drive", "SubsetSequence", "solve_batch", "autotune", "make_desc", "DESC_DTYPE", "RESULT_DTYPE",
            "GpvError", "PREC_MIXED", "PREC_FP64", "STATUS", "version"]
 
 
@@ -104,6 +104,16 @@ class Image:
     @property
     def handle(self):
         return self._h
+
+    def update(self, image_gs) -> None:
+        """Re-prefilter new pixels of the same shape into this image in place
+        (gpv_image_update; a sequence's next frame, src/sequence.rs:914)."""
+        arr = np.ascontiguousarray(image_gs)
+        if arr.shape != tuple(self.shape):
+            raise ValueError(f"shape {arr.shape} != {tuple(self.shape)}")
+        if arr.dtype not in _lib.DTYPES:
+            arr = np.ascontiguousarray(arr, dtype=np.float64)
+        check(lib().gpv_image_update(self._h, ptr(arr), _lib.DTYPES[arr.dtype]), "gpv_image_update")
 
     def coef(self, f64: bool = False) -> np.ndarray:
         """Coefficient array C, shape (h + 2 border, w + 2 border) (src/image.rs:48-51)."""
@@ -311,3 +321,62 @@ class Subset:
 
 
 from .mesh import Cancelled, Mesh, mesh_drive  # noqa: E402  (uses the classes above only through arguments)
+
+
+class SubsetSequence:
+    """Frame-to-frame tracking of a fixed set of subsets (gpv_sequence_*):
+    the per-frame work of Sequence.solve (src/sequence.rs:624-968) with the
+    reference image fixed, every frame's target re-prefiltered in place and
+    each subset seeded from its own last converged solution on the device.
+    From the second frame on, the frame's device work is one CUDA graph
+    (``graph=False`` launches it eagerly instead)."""
+
+    def __init__(self, f_img: Image, g_img: Image, desc, dtype, max_norm=1e-5, max_iterations=50, tolerance=0.75,
+                 precision=PREC_MIXED, global_mask: Mask | None = None, graph: bool = True):
+        desc = np.ascontiguousarray(desc, dtype=DESC_DTYPE)
+        self.n = desc.size
+        self.dtype = np.dtype(dtype)
+        if self.dtype not in _lib.DTYPES:
+            raise TypeError(f"unsupported pixel dtype {self.dtype}")
+        self.shape = f_img.shape
+        self._imgs = (f_img, g_img, global_mask)  # kept alive while the sequence exists
+        prm = _params(max_norm, max_iterations, tolerance, False, precision, global_mask, None)
+        h = ct.c_void_p()
+        check(lib().gpv_sequence_create(f_img.ctx.handle, f_img.handle, g_img.handle, ptr(desc), self.n,
+                                        ct.byref(prm), _lib.DTYPES[self.dtype], 0 if graph else 1, ct.byref(h)),
+              "gpv_sequence_create")
+        self._h = h
+
+    def frame(self, px=None, device_ptr: int | None = None, download: bool = True):
+        """Solve one frame from host pixels `px` (h x w of the sequence's
+        dtype) or from device pixels at `device_ptr`; returns the results
+        (RESULT_DTYPE) when `download`, else None (results stay on the device)."""
+        out = np.zeros(self.n, RESULT_DTYPE) if download else None
+        if device_ptr is not None:
+            rc = lib().gpv_sequence_frame(self._h, ct.c_void_p(device_ptr), 1, ptr(out))
+        else:
+            a = np.ascontiguousarray(px, dtype=self.dtype)
+            if a.shape != tuple(self.shape):
+                raise ValueError(f"frame shape {a.shape} != {tuple(self.shape)}")
+            rc = lib().gpv_sequence_frame(self._h, ptr(a), 0, ptr(out))
+        check(rc, "gpv_sequence_frame")
+        return out
+
+    def results_device(self) -> int:
+        """Device address of the last frame's results (valid until the next frame)."""
+        return int(lib().gpv_sequence_results_device(self._h) or 0)
+
+    @property
+    def frames(self) -> int:
+        return int(lib().gpv_sequence_frames(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gpv_sequence_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
