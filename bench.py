@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mesh", action="store_true", help="skip the mesh-propagation leg")
+    ap.add_argument("--no-sequence", action="store_true", help="skip the frame-tracking leg")
     return ap.parse_args()
 
 
@@ -328,6 +329,66 @@ def mesh_leg(W, F, G, args, cpu=True):
 
 
 # ---------------------------------------------------------------------------
+def sequence_leg(ctx, n_frames=20, frame_step=10):
+    """Frame-to-frame tracking (gpv_sequence_*) on the incremental-sequence
+    workload: 2048^2 u8 frames under simple shear rising by 0.25% per frame,
+    20,000 subsets of radius 25, reference fixed at frame 0.  Per frame:
+    pinned host pixels -> device, in-place prefilter, seeding from the last
+    converged warps, batched solve; results stay on the device.  Timed with
+    CUDA events on the library stream over frames 1..n-1, once as CUDA-graph
+    replay and once as eager launches."""
+    import torch
+
+    import gpv
+    from gpv import synth
+    Ws = [synth.workload(4, 1, seed_frame=frame_step * k) for k in range(n_frames)]
+    W0 = Ws[0]
+    pins = [torch.from_numpy(W["g"].copy()).pin_memory() for W in Ws]
+    desc = gpv.make_desc(W0["coords"], W0["radius"], W0["order"], W0["p0"])
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = {"workload": W0["name"].replace("frame 0 ", "") + f", {n_frames} frames, shear +{0.05 * frame_step / 200:.4f}/frame",
+           "subsets": int(len(desc)), "frames_timed": n_frames - 1}
+    for graph in (True, False):
+        F = gpv.Image(image_gs=W0["f"], border=20, ctx=ctx)
+        G = gpv.Image(image_gs=W0["f"], border=20, ctx=ctx)
+        seq = gpv.SubsetSequence(F, G, desc, np.uint8, graph=graph)
+        seq.frame(pins[0].numpy(), download=False)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(1, n_frames):
+            _lib_frame(seq, pins[k])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / (n_frames - 1)
+        key = "graph" if graph else "eager"
+        out[f"ms_per_frame_{key}"] = ms
+        out[f"subsets_per_s_{key}"] = len(desc) / (ms * 1e-3)
+        if graph:
+            from gpv import _lib
+            res = np.zeros(len(desc), _lib.RESULT_DTYPE)
+            torch.cuda.synchronize()
+            import ctypes as ct
+            _lib.check(_lib.lib().gpv_sequence_frame(seq._h, ct.c_void_p(pins[-1].data_ptr()), 0,
+                                                     res.ctypes.data_as(ct.c_void_p)), "frame")
+            truth = synth.displacement(Ws[-1]["field"], W0["coords"])
+            good = res["converged"] == 1
+            out["converged_frac_last_frame"] = float(good.mean())
+            out["max_err_vs_field_px_last_frame"] = float(np.abs(res["p"][good, :2] - truth[good]).max())
+        seq.close()
+    out["timing"] = "CUDA events on the library stream; per frame: H2D of pinned pixels + prefilter + seeding + solve"
+    return out
+
+
+def _lib_frame(seq, pinned):
+    import ctypes as ct
+
+    from gpv import _lib
+    _lib.check(_lib.lib().gpv_sequence_frame(seq._h, ct.c_void_p(pinned.data_ptr()), 0, None), "gpv_sequence_frame")
+
+
+# ---------------------------------------------------------------------------
 def run_reference(args, world, rank):
     """--impl reference: the oracle restatement of the reference's CPU solver."""
     if rank != 0:
@@ -497,6 +558,9 @@ def run_ours(args, world, rank, local):
     mesh = None
     if not args.no_mesh and args.config == 2:
         mesh = mesh_leg(W, F, G, args, cpu=not args.no_cpu_baseline)
+    seq = None
+    if not args.no_sequence and args.config == 2 and args.scale_down == 1:
+        seq = sequence_leg(ctx)
     flop = algorithmic_flop(res)
     solve_avg_ms = float(np.mean(solve_ms))
     achieved = flop / (solve_avg_ms * 1e-3) / 1e12
@@ -548,6 +612,8 @@ def run_ours(args, world, rank, local):
     }
     if mesh is not None:
         line["mesh"] = mesh
+    if seq is not None:
+        line["sequence"] = seq
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": "subsets/s", "cores": cpu["cores"], "kind": "port",
                                 "sample": f"{len(cpu['sample_idx'])} random subsets of the same batch solved by the FP64 C "

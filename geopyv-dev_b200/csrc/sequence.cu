@@ -76,7 +76,7 @@ int frame_work(gpv_sequence *s, bool seed) {
     L.mw = s->prm.mask ? s->prm.mask->w : 0;
     L.out = s->out_dev;
     L.history = nullptr;
-    L.max_radius = ctx->table_radius;
+    L.max_radius = s->max_radius;  // within the context's tables (reserved at creation)
     return solve_launch(ctx, L, st);
 }
 

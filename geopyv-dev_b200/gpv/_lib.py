@@ -52,6 +52,30 @@ class MeshStats(ct.Structure):
 
 assert ct.sizeof(MeshParams) == 200 and ct.sizeof(MeshStats) == 56
 
+EXECUTOR_FN = ct.CFUNCTYPE(ct.c_int, ct.c_void_p, ct.c_int32, ct.c_void_p, ct.c_void_p, ct.c_void_p)
+
+
+class Request(ct.Structure):
+    _fields_ = [("f_px", ct.c_void_p), ("g_px", ct.c_void_p), ("dtype", ct.c_int32), ("border", ct.c_int32),
+                ("h", ct.c_int64), ("w", ct.c_int64), ("desc", ct.c_void_p), ("n", ct.c_int64),
+                ("params", SolveParams), ("session", ct.c_uint64), ("flags", ct.c_uint32), ("reserved", ct.c_uint32),
+                ("out", ct.c_void_p)]
+
+
+class ServerConfig(ct.Structure):
+    _fields_ = [("hbm_budget", ct.c_size_t), ("workers", ct.c_int32), ("device", ct.c_int32),
+                ("executor", EXECUTOR_FN), ("executor_user", ct.c_void_p)]
+
+
+class ServerStats(ct.Structure):
+    _fields_ = [("submitted", ct.c_int64), ("completed", ct.c_int64), ("failed", ct.c_int64), ("queued", ct.c_int64),
+                ("in_flight", ct.c_int64), ("subsets", ct.c_int64), ("p50_ms", ct.c_double), ("p99_ms", ct.c_double),
+                ("mean_ms", ct.c_double), ("max_ms", ct.c_double), ("subsets_per_s", ct.c_double),
+                ("bytes_in_flight", ct.c_size_t), ("peak_bytes", ct.c_size_t), ("hbm_budget", ct.c_size_t)]
+
+
+REQUEST_REUSE_REFERENCE, REQUEST_SEED_FROM_PREVIOUS = 1, 2
+
 # enums
 GPV_U8, GPV_U16, GPV_F32, GPV_F64 = 1, 2, 3, 4
 PREC_MIXED, PREC_FP64 = 0, 1
@@ -90,6 +114,12 @@ SIGNATURES = {
     "gpv_solve_batch_noalloc": (ct.c_int, [P, P, P, P, I64, I32, P, P, P]),
     "gpv_mesh_solve": (ct.c_int, [P, P, P, P, I64, P, I64, I32, P, P, P, P]),
     "gpv_sequence_create": (ct.c_int, [P, P, P, P, I64, P, I32, U32, P]),
+    "gpv_server_create": (ct.c_int, [P, P]),
+    "gpv_server_submit": (ct.c_int, [P, P, P]),
+    "gpv_server_wait": (ct.c_int, [P, ct.c_uint64, I32, P, P]),
+    "gpv_server_get_stats": (ct.c_int, [P, P]),
+    "gpv_server_reset_stats": (ct.c_int, [P]),
+    "gpv_server_destroy": (ct.c_int, [P]),
     "gpv_sequence_frame": (ct.c_int, [P, P, I32, P]),
     "gpv_sequence_results_device": (P, [P]),
     "gpv_sequence_frames": (I64, [P]),

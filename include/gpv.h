@@ -277,6 +277,72 @@ int gpv_mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements
                    int32_t nodes_per_element, const gpv_mesh_params *params, gpv_batch_solver_fn solver,
                    void *solver_user, gpv_subset_result *out, int32_t *rounds, gpv_mesh_stats *stats);
 
+/* ---- serving: a request loop (no single counterpart in the reference) ----
+ * Requests -- an image pair, subsets, solver settings -- are submitted from
+ * any host thread and served by `workers` worker threads, each with its own
+ * context (CUDA stream and solve workspace) on `device`, so several requests
+ * are on the GPU at once.  Admission is by device-memory footprint against
+ * `hbm_budget` bytes (0 = 80% of the memory free at creation): requests start
+ * in arrival order when they fit; a request that does not fit is overtaken
+ * by later ones that do (at most 8 times); one larger than the whole budget
+ * runs alone.  A session (nonzero `session`) is served by one worker, in
+ * order, and keeps its reference coefficients and its last results on that
+ * worker: GPV_REQUEST_REUSE_REFERENCE skips the reference upload and
+ * prefilter (f_px may then be NULL), GPV_REQUEST_SEED_FROM_PREVIOUS starts
+ * every subset from its last converged warp (same subset count), as a
+ * sequence's frame loop does (src/sequence.rs:624-968).  Host buffers
+ * (pixels, desc, out) must stay valid until gpv_server_wait returns; desc is
+ * copied at submit. */
+#define GPV_REQUEST_REUSE_REFERENCE 1u
+#define GPV_REQUEST_SEED_FROM_PREVIOUS 2u
+
+typedef struct {
+    const void *f_px;   /* reference pixels, host, h x w of dtype (or NULL, see above) */
+    const void *g_px;   /* target pixels, host                                     */
+    int32_t dtype;      /* gpv_dtype                                               */
+    int32_t border;     /* >= 3 (20 as Image::from_array's default)                */
+    int64_t h, w;
+    const gpv_subset_desc *desc;
+    int64_t n;
+    gpv_solve_params params;  /* mixed precision; no mask, no history           */
+    uint64_t session;         /* 0 = none                                        */
+    uint32_t flags;           /* GPV_REQUEST_*                                   */
+    uint32_t reserved;
+    gpv_subset_result *out;   /* host, n results, written before completion     */
+} gpv_request;
+
+/* Executes one request on worker `worker` (desc is the server's copy,
+ * already seeded); returns a gpv_err.  NULL = the GPU solve of this library
+ * (a stand-in lets the request loop itself be exercised without a GPU). */
+typedef int (*gpv_request_executor_fn)(void *user, int32_t worker, const gpv_request *req, gpv_subset_desc *desc,
+                                       gpv_subset_result *out);
+
+typedef struct {
+    size_t hbm_budget;   /* bytes; 0 = 80% of free device memory */
+    int32_t workers;     /* 1..64 */
+    int32_t device;
+    gpv_request_executor_fn executor;  /* NULL = GPU */
+    void *executor_user;
+} gpv_server_config;
+
+typedef struct {
+    int64_t submitted, completed, failed, queued, in_flight, subsets;
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> results in host memory */
+    double subsets_per_s;                    /* completed subsets / (last done - first submit) */
+    size_t bytes_in_flight, peak_bytes, hbm_budget;
+} gpv_server_stats;
+
+int gpv_server_create(const gpv_server_config *cfg, gpv_server **out);
+int gpv_server_submit(gpv_server *s, const gpv_request *req, uint64_t *id);
+/* Waits up to timeout_ms for request `id`: GPV_ERR_TIMEOUT if unfinished,
+ * GPV_ERR_NOT_FOUND for an unknown or already collected id; otherwise
+ * GPV_SUCCESS with the request's own gpv_err in *req_status. */
+int gpv_server_wait(gpv_server *s, uint64_t id, int32_t timeout_ms, int32_t *req_status, double *latency_ms);
+int gpv_server_get_stats(gpv_server *s, gpv_server_stats *out);
+int gpv_server_reset_stats(gpv_server *s);
+/* Serves what is queued, then stops the workers and frees every resource. */
+int gpv_server_destroy(gpv_server *s);
+
 /* ---- autotuning (no counterpart in the reference) ------------------------
  * Times the candidate launch shapes of the mixed-precision kernel (threads
  * per subset block) on a sample of up to sample_per_class subsets of each
