@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mesh", action="store_true", help="skip the mesh-propagation leg")
     ap.add_argument("--no-sequence", action="store_true", help="skip the frame-tracking leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--serving-seconds", type=float, default=10.0)
     return ap.parse_args()
 
 
@@ -389,6 +391,80 @@ def _lib_frame(seq, pinned):
 
 
 # ---------------------------------------------------------------------------
+def serving_leg(seconds=10.0, rate=200.0, workers=6, seed=55):
+    """The serving stream: Poisson arrivals at `rate` req/s for `seconds`,
+    each request a seeded speckle pair of side 512..4096 (u8 or u16) under a
+    random affine field (|strain| <= 2%, |rotation| <= 1 deg, |t| <= 5 px),
+    100..100k subsets (log-uniform) of radius 15..50 and mixed order, initial
+    warps from the field +-0.3 px (a coarse upstream estimate).  Pixels and
+    subsets come from a pre-generated pool (one pair per size and pixel type,
+    pinned host memory); latency is submit -> results in host memory."""
+    import math
+
+    import torch
+
+    import gpv
+    from gpv import synth
+    rng = np.random.default_rng(seed)
+    pool = []
+    for size in (512, 1024, 2048, 4096):
+        for dt in (np.uint8, np.uint16):
+            c = (size - 1) / 2.0
+            th = math.radians(rng.uniform(-1, 1))
+            e = rng.uniform(-0.02, 0.02, 2)
+            a = ((1 + e[0]) * math.cos(th) - 1.0, -math.sin(th), math.sin(th), (1 + e[1]) * math.cos(th) - 1.0)
+            fld = synth.make_field(xc=c, yc=c, t=tuple(rng.uniform(-5, 5, 2)), a=a)
+            f, g = synth.pair(size, size, fld, 7000 + size + (1 if dt == np.uint16 else 0), dtype=dt,
+                              scale=16.0 if dt == np.uint16 else 1.0)
+            fp = torch.from_numpy(f.view(np.uint8 if dt == np.uint8 else np.int16).copy()).pin_memory()
+            gp = torch.from_numpy(g.view(np.uint8 if dt == np.uint8 else np.int16).copy()).pin_memory()
+            margin = 60 + 0.027 * size  # radius 50 + the largest |u| of the field + 5 px
+            m = 100000
+            xy = rng.uniform(margin, size - margin, (m, 2))
+            radius = rng.integers(15, 51, m).astype(np.int32)
+            order = rng.integers(1, 3, m).astype(np.int32)
+            desc = gpv.make_desc(xy, radius, order, synth.seeded_p0(fld, xy, rng))
+            pool.append((fp.numpy().view(dt), gp.numpy().view(dt), desc, (fp, gp)))
+    srv = gpv.Server(workers=workers)
+    # warm-up: every pool entry once (image caches, tables, workspace)
+    for f, g, d, _ in pool:
+        srv.wait(srv.submit(f, g, d[:2000]), 120000)
+    srv.reset_stats()
+    t0 = time.perf_counter()
+    tickets = []
+    t_next = 0.0
+    while t_next < seconds:
+        while time.perf_counter() - t0 < t_next:
+            time.sleep(0.0002)
+        f, g, d, _ = pool[rng.integers(len(pool))]
+        n = int(math.exp(rng.uniform(math.log(100), math.log(100000))))
+        start = int(rng.integers(0, len(d) - n + 1))
+        tickets.append((n, srv.submit(f, g, d[start:start + n])))
+        t_next += rng.exponential(1.0 / rate)
+    lat = []
+    conv = []
+    for n, t in tickets:
+        out = srv.wait(t, 600000)
+        lat.append((n, t.latency_ms))
+        conv.append(float(np.mean(out["converged"])))
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    ln = np.array([x[1] for x in lat])
+    ns = np.array([x[0] for x in lat])
+    mid = (ns >= 5000) & (ns <= 20000)
+    return {"requests": len(tickets), "arrival_rate_per_s": rate, "seconds_of_arrivals": seconds, "workers": workers,
+            "p50_ms": float(np.percentile(ln, 50)), "p99_ms": float(np.percentile(ln, 99)),
+            "p99_ms_5k_20k_subsets": float(np.percentile(ln[mid], 99)) if mid.any() else None,
+            "p50_ms_5k_20k_subsets": float(np.percentile(ln[mid], 50)) if mid.any() else None,
+            "requests_5k_20k_subsets": int(mid.sum()),
+            "subsets_per_s": float(ns.sum() / wall), "subsets": int(ns.sum()), "wall_s": wall,
+            "mean_converged_frac": float(np.mean(conv)), "peak_admitted_bytes": int(st["peak_bytes"]),
+            "hbm_budget_bytes": int(st["hbm_budget"]),
+            "latency": "submit -> results in host memory; pinned host pixels; per request: H2D, prefilter x2, solve, D2H"}
+
+
+# ---------------------------------------------------------------------------
 def run_reference(args, world, rank):
     """--impl reference: the oracle restatement of the reference's CPU solver."""
     if rank != 0:
@@ -561,6 +637,9 @@ def run_ours(args, world, rank, local):
     seq = None
     if not args.no_sequence and args.config == 2 and args.scale_down == 1:
         seq = sequence_leg(ctx)
+    serving = None
+    if not args.no_serving and args.config == 2 and args.scale_down == 1:
+        serving = serving_leg(seconds=args.serving_seconds)
     flop = algorithmic_flop(res)
     solve_avg_ms = float(np.mean(solve_ms))
     achieved = flop / (solve_avg_ms * 1e-3) / 1e12
@@ -614,6 +693,10 @@ def run_ours(args, world, rank, local):
         line["mesh"] = mesh
     if seq is not None:
         line["sequence"] = seq
+    if serving is not None:
+        line["serving"] = serving
+        line["p50_ms"] = serving["p50_ms"]
+        line["p99_ms"] = serving["p99_ms"]
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": "subsets/s", "cores": cpu["cores"], "kind": "port",
                                 "sample": f"{len(cpu['sample_idx'])} random subsets of the same batch solved by the FP64 C "

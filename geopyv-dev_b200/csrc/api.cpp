@@ -507,8 +507,8 @@ int gpv_solve_batch_noalloc(gpv_context *ctx, const gpv_image *f, const gpv_imag
                             void *stream) {
     if (!ctx) { set_error("ctx is NULL"); return GPV_ERR_INVALID; }
     if (int rc = check_pair(f, g, prm)) return rc;
-    if (prm->precision != GPV_PREC_MIXED) {
-        set_error("gpv_solve_batch_noalloc runs the mixed-precision solve only");
+    if (prm->precision != GPV_PREC_MIXED || (prm->flags & GPV_SOLVE_FAGN)) {
+        set_error("gpv_solve_batch_noalloc runs the mixed-precision ICGN solve only");
         return GPV_ERR_INVALID;
     }
     if (n < 0 || (n > 0 && (!desc_dev || !out_dev)) || n > INT32_MAX) { set_error("invalid batch arrays"); return GPV_ERR_INVALID; }
@@ -554,6 +554,7 @@ int gpv_mesh_solve(gpv_context *ctx, const gpv_image *f, const gpv_image *g, con
     S.prm.max_iterations = params->max_iterations;
     S.prm.precision = params->precision;
     S.prm.mask = params->mask;
+    S.prm.flags = params->method == 1 ? GPV_SOLVE_FAGN : 0;
     if (int rc = check_pair(f, g, &S.prm)) return rc;
     return gpv::mesh_drive(nodes, n_nodes, elements, n_elements, nodes_per_element, params, gpu_mesh_solver, &S, out,
                            rounds, stats);
@@ -592,7 +593,7 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
     gpv_solve_params p = *prm;
     p.precision = GPV_PREC_MIXED;
     p.history = nullptr;
-    p.flags &= ~GPV_SOLVE_ETA;
+    p.flags &= ~(GPV_SOLVE_ETA | GPV_SOLVE_FAGN);  // the tuned kernel is the mixed ICGN one
     static const int cand[2] = {128, 256};
     for (int c = 0; c < 3; c++) {
         if (threads_out) threads_out[c] = 0;

@@ -376,6 +376,273 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
     }
 }
 
+// =====================================================================
+// Forward additive Gauss-Newton (solve_fagn_result, src/subset.rs:1228-1334)
+// =====================================================================
+// One block per subset, FP64 arithmetic on FP64 coefficients when the images
+// keep them, else on the FP32 coefficients.  Per iteration (:1258-1307): the
+// target value and gradient at the warped positions, g_m and delta_g (two
+// sweeps), the steepest-descent images from the target gradient about the
+// warped centre g_center = coord + (u, v) (steepest_descent at :1281), the
+// Hessian from FP64 gradient moments of those offsets, the residual
+// gradient of delta_p_fagn (:452-473), p += H^-1 grad, then the norm and
+// ZNSSD.  Scratch per pixel: f, df/dx, df/dy, g, dg/dx, dg/dy.
+template <int ORDER, typename C>
+__device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, double *S, int64_t nmax, BlockSmem &sm,
+                            const C *Fc, const C *Gc, int64_t pitch) {
+    using O = Ord<ORDER>;
+    constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int r = d.radius;
+    const int npx_t = A.tab_n[r];
+    const short2 *po = A.offs + A.tab_off[r];
+    double *Sf = S, *Sgx = S + nmax, *Sgy = S + 2 * nmax, *Sg = S + 3 * nmax, *Shx = S + 4 * nmax,
+           *Shy = S + 5 * nmax;
+    const double cx = d.coord[0], cy = d.coord[1];
+    const int cxi = (int)cx, cyi = (int)cy;
+    const double fxd = floor(cx), fyd = floor(cy);
+    const int bx = (int)fxd, by = (int)fyd;
+    const double fx = cx - fxd, fy = cy - fyd;
+    const C *F = Fc + (int64_t)(A.border - 2) * pitch + (A.border - 2);
+    const C *G = Gc + (int64_t)(A.border - 2) * pitch + (A.border - 2);
+
+    // Subset::new (:836-919)
+    double loc[4] = {0, 0, 0, 0};
+    for (int i = tid; i < npx_t; i += nthr) {
+        const short2 o = po[i];
+        if (!mask_ok(A, cxi, cyi, o.x, o.y)) { Sf[i] = __longlong_as_double(0x7ff8000000000000ll); continue; }
+        int ix, iy;
+        double tx, ty;
+        split_clamped(bx, fx + (double)o.x, A.w, ix, tx);
+        split_clamped(by, fy + (double)o.y, A.h, iy, ty);
+        double a[6], da[6], b[6], db[6];
+        basis(ty, a); dbasis(ty, da);
+        basis(tx, b); dbasis(tx, db);
+        double gx, gy;
+        const double f = contract_grad<double>(F + (int64_t)iy * pitch + ix, pitch, a, da, b, db, gx, gy);
+        Sf[i] = f; Sgx[i] = gx; Sgy[i] = gy;
+        loc[0] += f;
+        loc[1] += 1.0;
+        loc[2] += 0.5 * (gx * gx + gy * gy);
+    }
+    block_sum<4>(loc, sm);
+    const int n = (int)loc[1];
+    const double sssig = loc[2];
+    if (n == 0) {
+        if (tid == 0) write_failed(A, idx, d, M, GPV_EMPTY_MASK, 0, 0.0, 0.0);
+        return;
+    }
+    const double dn = (double)n, fm = loc[0] / dn;
+    double ss = 0.0;
+    for (int i = tid; i < npx_t; i += nthr) {
+        const double f = Sf[i];
+        if (f != f) continue;
+        ss += (f - fm) * (f - fm);
+    }
+    ss = block_sum1(ss, sm);
+    const double df = sqrt(ss);
+    if (!(sqrt(ss / dn) > 1e-6 * fmax(1.0, fabs(fm)))) {
+        if (tid == 0) write_failed(A, idx, d, M, GPV_FEATURELESS, n, fm, df);
+        return;
+    }
+    const double size = sqrt(dn);
+    double p[M];
+#pragma unroll
+    for (int k = 0; k < M; k++) p[k] = d.p0[k];
+    int iters = 0, status = GPV_OK;
+    bool converged = false;
+    double c_zncc = 0.0, c_znssd = 4.0, last_norm = 0.0, gm_last = 0.0, dg_last = 0.0;
+    for (int it = 1; it <= A.max_iter; it++) {
+        // target value + gradient at the warped positions (:1265-1279)
+        double sg = 0.0;
+        for (int i = tid; i < npx_t; i += nthr) {
+            if (Sf[i] != Sf[i]) continue;
+            const short2 o = po[i];
+            const double dx = o.x, dy = o.y;
+            double xw = cx + dx + p[0], yw = cy + dy + p[1];
+            if (ORDER >= 1) {
+                xw = (cx + dx) + p[0] + p[2 % M] * dx + p[4 % M] * dy;
+                yw = (cy + dy) + p[1] + p[3 % M] * dx + p[5 % M] * dy;
+            }
+            if (ORDER == 2) {
+                xw += 0.5 * p[6 % M] * dx * dx + p[8 % M] * dx * dy + 0.5 * p[10 % M] * dy * dy;
+                yw += 0.5 * p[7 % M] * dx * dx + p[9 % M] * dx * dy + 0.5 * p[11 % M] * dy * dy;
+            }
+            const double xfl = floor(xw), yfl = floor(yw);
+            int ix, iy;
+            double tx, ty;
+            split_clamped((int)xfl, xw - xfl, A.w, ix, tx);
+            split_clamped((int)yfl, yw - yfl, A.h, iy, ty);
+            double a[6], da[6], b[6], db[6];
+            basis(ty, a); dbasis(ty, da);
+            basis(tx, b); dbasis(tx, db);
+            double hx, hy;
+            const double g = contract_grad<double>(G + (int64_t)iy * pitch + ix, pitch, a, da, b, db, hx, hy);
+            Sg[i] = g; Shx[i] = hx; Shy[i] = hy;
+            sg += g;
+        }
+        sg = block_sum1(sg, sm);
+        const double gm = sg / dn;
+        double sgg = 0.0;
+        for (int i = tid; i < npx_t; i += nthr) {
+            if (Sf[i] != Sf[i]) continue;
+            sgg += (Sg[i] - gm) * (Sg[i] - gm);
+        }
+        sgg = block_sum1(sgg, sm);
+        const double dg = sqrt(sgg);
+        // Hessian moments, residual gradient and ZNSSD in one sweep
+        const double gcx = cx + p[0], gcy = cy + p[1];
+        const double ratio = dg / df;
+        double mom[3 * NMOM], acc[M + 1];
+#pragma unroll
+        for (int q = 0; q < 3 * NMOM; q++) mom[q] = 0.0;
+#pragma unroll
+        for (int k = 0; k <= M; k++) acc[k] = 0.0;
+        for (int i = tid; i < npx_t; i += nthr) {
+            const double f = Sf[i];
+            if (f != f) continue;
+            const short2 o = po[i];
+            const double ox = o.x, oy = o.y;
+            double xw = cx + ox + p[0], yw = cy + oy + p[1];
+            if (ORDER >= 1) {
+                xw = (cx + ox) + p[0] + p[2 % M] * ox + p[4 % M] * oy;
+                yw = (cy + oy) + p[1] + p[3 % M] * ox + p[5 % M] * oy;
+            }
+            if (ORDER == 2) {
+                xw += 0.5 * p[6 % M] * ox * ox + p[8 % M] * ox * oy + 0.5 * p[10 % M] * oy * oy;
+                yw += 0.5 * p[7 % M] * ox * ox + p[9 % M] * ox * oy + 0.5 * p[11 % M] * oy * oy;
+            }
+            const double dx = xw - gcx, dy = yw - gcy;
+            const double hx = Shx[i], hy = Shy[i], g = Sg[i];
+            double pxp[5], pyp[5];
+            pxp[0] = pyp[0] = 1.0;
+#pragma unroll
+            for (int e = 1; e <= 2 * O::DEG; e++) { pxp[e] = pxp[e - 1] * dx; pyp[e] = pyp[e - 1] * dy; }
+            const double hh[3] = {hx * hx, hx * hy, hy * hy};
+#pragma unroll
+            for (int dgr = 0; dgr <= 2 * O::DEG; dgr++)
+#pragma unroll
+                for (int bb = 0; bb <= dgr; bb++) {
+                    const double mono = pxp[dgr - bb] * pyp[bb];
+#pragma unroll
+                    for (int q = 0; q < 3; q++) mom[q * NMOM + mom_idx(dgr - bb, bb)] += hh[q] * mono;
+                }
+            const double a = f - fm, bq = g - gm;
+            const double z = a / df - bq / dg;
+            acc[M] += z * z;
+            const double res = a * ratio - bq;
+#pragma unroll
+            for (int mu = 0; mu < NMU; mu++) {
+                const double mv = mu_val<double>(mu, dx, dy);
+                acc[2 * mu] += hx * mv * res;
+                acc[2 * mu + 1] += hy * mv * res;
+            }
+        }
+        block_sum<M + 1>(acc, sm);
+#pragma unroll
+        for (int q = 0; q < 3 * NMOM; q++) {
+            const double v = block_sum1(mom[q], sm);
+            if (tid == 0) sm.mom[q] = v;
+        }
+        __syncthreads();
+        if (tid < 32) assemble_hessian<ORDER>(sm.mom, sm.H, tid);
+        __syncthreads();
+        if (tid == 0) sm.flag[0] = gj_inverse_serial<M>(sm.H, sm.Hinv);
+        __syncthreads();
+        gm_last = gm;
+        dg_last = dg;
+        if (!sm.flag[0]) {  // the reference panics ("FAGN Hessian singular")
+            status = GPV_SINGULAR_H;
+            break;
+        }
+        double dp[M];
+#pragma unroll
+        for (int j = 0; j < M; j++) {
+            double s2 = 0.0;
+#pragma unroll
+            for (int k = 0; k < M; k++) s2 += sm.Hinv[j * M + k] * acc[k];
+            dp[j] = s2;
+        }
+#pragma unroll
+        for (int k = 0; k < M; k++) p[k] += dp[k];  // additive update (:1293-1296)
+        const double nrm = conv_norm<M>(dp, size);
+        c_znssd = acc[M];
+        c_zncc = 1.0 - acc[M] / 2.0;
+        iters = it;
+        last_norm = nrm;
+        if (tid == 0) write_history(A, idx, it, nrm, c_zncc, c_znssd);
+        if (!isfinite(nrm)) { status = GPV_NONFINITE; break; }
+        if (nrm < A.max_norm) { converged = true; break; }
+    }
+    double eu = 0.0, ev = 0.0;
+    const bool want_eta = (A.flags & GPV_SOLVE_ETA) && iters > 0 && status == GPV_OK;
+    if (want_eta) {  // with the last sampled target and the reference gradients (:1313-1323)
+        auto load = [&](int i, double &f, double &gx, double &gy, double &g, double &dx, double &dy) -> bool {
+            f = Sf[i];
+            if (f != f) return false;
+            const short2 o = po[i];
+            gx = Sgx[i]; gy = Sgy[i]; g = Sg[i]; dx = o.x; dy = o.y;
+            return true;
+        };
+        auto red = [&](double v) { return block_sum1(v, sm); };
+        eta_sums<ORDER>(npx_t, tid, nthr, dn, fm, df, gm_last, dg_last, load, red, eu, ev);
+    }
+    if (tid == 0) {
+        gpv_subset_result *o = A.out + idx;
+#pragma unroll
+        for (int k = 0; k < 12; k++) o->p[k] = k < M ? p[k % M] : 0.0;
+        o->c_zncc = c_zncc;
+        o->c_znssd = c_znssd;
+        o->norm = last_norm;
+        o->eta_u = eu;
+        o->eta_v = ev;
+        o->f_m = fm;
+        o->delta_f = df;
+        o->sssig = sssig;
+        o->sigma = sqrt(ss / dn);
+        o->iterations = iters;
+        o->converged = converged;
+        o->quality_ok = converged && c_zncc >= A.tolerance;
+        o->status = status;
+        o->n_px = n;
+        o->has_eta = want_eta;
+    }
+}
+
+__global__ void __launch_bounds__(kFp64Threads) fagn_kernel(KArgs A) {
+    __shared__ BlockSmem sm;
+    __shared__ int item_s;
+    double *S = reinterpret_cast<double *>(A.scratch) + (int64_t)blockIdx.x * A.scratch_stride;
+    const int64_t nmax = A.scratch_stride / 6;
+    const bool c64 = A.f64 != nullptr && A.g64 != nullptr;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) item_s = atomicAdd(A.queue, 1);
+        __syncthreads();
+        const int item = item_s;
+        if (item >= A.n) break;
+        const int idx = A.order ? A.order[item] : item;
+        const gpv_subset_desc d = A.desc[idx];
+        if (d.radius < 1 || d.radius > A.max_radius || d.order < 0 || d.order > 2) {
+            if (threadIdx.x == 0) write_failed(A, idx, d, 12, GPV_INVALID_SUBSET, 0, 0.0, 0.0);
+            continue;
+        }
+        if (c64) {
+            switch (d.order) {
+                case 0: fagn_subset<0, double>(A, idx, d, S, nmax, sm, A.f64, A.g64, A.pitch64); break;
+                case 1: fagn_subset<1, double>(A, idx, d, S, nmax, sm, A.f64, A.g64, A.pitch64); break;
+                default: fagn_subset<2, double>(A, idx, d, S, nmax, sm, A.f64, A.g64, A.pitch64); break;
+            }
+        } else {
+            switch (d.order) {
+                case 0: fagn_subset<0, float>(A, idx, d, S, nmax, sm, A.f32, A.g32, A.pitch32); break;
+                case 1: fagn_subset<1, float>(A, idx, d, S, nmax, sm, A.f32, A.g32, A.pitch32); break;
+                default: fagn_subset<2, float>(A, idx, d, S, nmax, sm, A.f32, A.g32, A.pitch32); break;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kFp64Threads) icgn_fp64(KArgs A) {
     __shared__ BlockSmem sm;
     __shared__ int item_s;
@@ -473,6 +740,29 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
     A.max_iter = prm->max_iterations; A.flags = prm->flags;
     A.out = L.out; A.history = L.history;
     const int64_t npx_max = ctx->h_tab_n[L.max_radius];
+    if (prm->flags & GPV_SOLVE_FAGN) {  // FP64 arithmetic in either precision mode
+        if (fp64) {
+            A.f64 = L.f->c64;
+            A.g64 = L.g->c64;
+        } else {
+            A.f64 = nullptr;
+            A.g64 = nullptr;
+        }
+        int per_sm = 0;
+        GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fagn_kernel, kFp64Threads, 0));
+        if (per_sm < 1) per_sm = 1;
+        const int workers = ctx->num_sms * per_sm;
+        const int64_t stride = 6 * ((npx_max + 31) / 32 * 32);
+        if (int rc = ctx->scratch.ensure((size_t)workers * stride * sizeof(double))) return rc;
+        if (int rc = ctx->queue.ensure(64)) return rc;
+        A.scratch = ctx->scratch.ptr;
+        A.scratch_stride = stride;
+        A.queue = static_cast<int *>(ctx->queue.ptr);
+        GPV_CUDA_TRY(cudaMemsetAsync(A.queue, 0, sizeof(int), s));
+        fagn_kernel<<<workers, kFp64Threads, 0, s>>>(A);
+        GPV_CUDA_TRY(cudaGetLastError());
+        return GPV_SUCCESS;
+    }
     if (!fp64 && !use_warp_kernel()) {
         if (int rc = ctx->tile_ws.ensure(sizeof(int32_t) * (32 + (size_t)L.n))) return rc;
         return tile_launch(ctx, A, L.n, s);

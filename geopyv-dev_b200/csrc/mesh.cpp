@@ -372,6 +372,10 @@ int mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements, in
         set_error("mesh solves use subset_order 1 or 2 and radius >= 1");
         return GPV_ERR_INVALID;
     }
+    if (mp->method != 0 && mp->method != 1) {
+        set_error("method must be 0 (ICGN) or 1 (FAGN)");
+        return GPV_ERR_INVALID;
+    }
     if (mp->layer_rg && (mp->batch_factor < 1 || mp->max_workers < 1)) {
         set_error("layer-RG needs batch_factor >= 1 and max_workers >= 1");
         return GPV_ERR_INVALID;

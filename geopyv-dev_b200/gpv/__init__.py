@@ -212,21 +212,24 @@ def make_desc(coords, radius, order, p0=None) -> np.ndarray:
     return d
 
 
-def _params(max_norm, max_iterations, tolerance, eta, precision, mask, history_buf):
+def _params(max_norm, max_iterations, tolerance, eta, precision, mask, history_buf, method="icgn"):
+    if method not in ("icgn", "fagn"):
+        raise ValueError(f"method must be 'icgn' or 'fagn', got {method!r}")
+    flags = (SOLVE_ETA if eta else 0) | (_lib.SOLVE_FAGN if method == "fagn" else 0)
     return SolveParams(max_norm=max_norm, tolerance=tolerance, max_iterations=max_iterations,
-                       flags=(SOLVE_ETA if eta else 0), precision=precision, reserved=0,
+                       flags=flags, precision=precision, reserved=0,
                        mask=(mask.handle if mask is not None else None),
                        history=(history_buf.ctypes.data if history_buf is not None else None))
 
 
 def solve_batch(f_img: Image, g_img: Image, desc, max_norm=1e-5, max_iterations=50, tolerance=0.75, eta=False,
-                precision=PREC_MIXED, global_mask: Mask | None = None, history=False):
+                precision=PREC_MIXED, global_mask: Mask | None = None, history=False, method="icgn"):
     """Batched Subset::new + solve_icgn_result on the GPU; returns a RESULT_DTYPE array
     (and the (n, max_iterations, 3) history of (norm, zncc, znssd) when asked)."""
     desc = np.ascontiguousarray(desc, dtype=DESC_DTYPE)
     out = np.zeros(desc.size, RESULT_DTYPE)
     hist = np.zeros((desc.size, max(max_iterations, 1), 3)) if history else None
-    prm = _params(max_norm, max_iterations, tolerance, eta, precision, global_mask, hist)
+    prm = _params(max_norm, max_iterations, tolerance, eta, precision, global_mask, hist, method)
     check(lib().gpv_solve_batch(f_img.ctx.handle, f_img.handle, g_img.handle, ptr(desc), desc.size,
                                 ct.byref(prm), ptr(out)), "gpv_solve_batch")
     return (out, hist) if history else out
@@ -264,13 +267,22 @@ class Subset:
         self._history = None
         self.solved = False
 
-    def solve(self, p_0=None, solver=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED):
-        if solver not in (None, "icgn"):
-            raise NotImplementedError("only solver='icgn' runs on the GPU")
-        self.solve_icgn(p_0=p_0, max_norm=max_norm, max_iterations=max_iterations, tolerance=tolerance,
-                        precision=precision)
+    def solve(self, p_0=None, solver=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED,
+              algorithm=None):
+        """Subset.solve: ``algorithm`` (or ``solver``) "icgn" (default) or "fagn"."""
+        method = algorithm or solver or "icgn"
+        if method not in ("icgn", "fagn"):
+            raise ValueError(f"algorithm must be 'icgn' or 'fagn', got {method!r}")
+        self._solve(method, p_0, max_norm, max_iterations, tolerance, precision)
 
     def solve_icgn(self, p_0=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED):
+        self._solve("icgn", p_0, max_norm, max_iterations, tolerance, precision)
+
+    def solve_fagn(self, p_0=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED):
+        """Forward additive Gauss-Newton (Subset::solve_fagn, src/subset.rs:1011-1020, 1228-1334)."""
+        self._solve("fagn", p_0, max_norm, max_iterations, tolerance, precision)
+
+    def _solve(self, method, p_0, max_norm, max_iterations, tolerance, precision):
         m = {0: 2, 1: 6, 2: 12}[self.subset_order]
         p0 = np.zeros(m)
         if p_0 is not None:  # resized to the order's length (src/subset.rs:1134-1136)
@@ -279,18 +291,20 @@ class Subset:
         d = make_desc([self.coord], self.local_mask.size, self.subset_order, p0[None, :])
         out, hist = solve_batch(self.f_img, self.g_img, d, max_norm=max_norm, max_iterations=max_iterations,
                                 tolerance=tolerance, eta=True, precision=precision, global_mask=self.global_mask,
-                                history=True)
+                                history=True, method=method)
         r = out[0]
         st = int(r["status"])
         if st in (1, 2):  # Subset::new errors (src/subset.rs:853-892) -> RuntimeError (python/src/lib.rs:18-38)
             raise RuntimeError("invalid input: " + ("effective mask coords is empty" if st == 1
                                                     else "reference subset is featureless (delta_f = 0)"))
-        if st in (3, 4):  # the reference panics (src/subset.rs:520,595,1143)
-            raise RuntimeError("ICGN Hessian singular" if st == 3 else "W_delta singular")
+        if st in (3, 4):  # the reference panics (src/subset.rs:471,520,595,1143)
+            what = "FAGN Hessian singular" if method == "fagn" else "ICGN Hessian singular"
+            raise RuntimeError(what if st == 3 else "W_delta singular")
         self._result = r
         k = int(r["iterations"])
         self._history = [(i + 1, *hist[0, i]) for i in range(k)]
         self.solved = True
+        self.method = method
 
     def _get(self, key):
         if self._result is None:

@@ -41,7 +41,7 @@ class MeshParams(ct.Structure):
                 ("max_norm", ct.c_double), ("tolerance", ct.c_double), ("root_rel_eps", ct.c_double),
                 ("max_iterations", ct.c_int32), ("subset_order", ct.c_int32), ("radius", ct.c_int32),
                 ("precision", ct.c_int32), ("layer_rg", ct.c_int32), ("batch_factor", ct.c_int32),
-                ("max_workers", ct.c_int32), ("reserved", ct.c_int32), ("mask", ct.c_void_p),
+                ("max_workers", ct.c_int32), ("method", ct.c_int32), ("mask", ct.c_void_p),
                 ("progress", PROGRESS_FN), ("progress_user", ct.c_void_p)]
 
 
@@ -79,7 +79,7 @@ REQUEST_REUSE_REFERENCE, REQUEST_SEED_FROM_PREVIOUS = 1, 2
 # enums
 GPV_U8, GPV_U16, GPV_F32, GPV_F64 = 1, 2, 3, 4
 PREC_MIXED, PREC_FP64 = 0, 1
-SOLVE_ETA, SOLVE_HISTORY = 1, 2
+SOLVE_ETA, SOLVE_HISTORY, SOLVE_FAGN = 1, 2, 4
 IMAGE_KEEP_F64 = 1
 STATUS = {0: "OK", 1: "EMPTY_MASK", 2: "FEATURELESS", 3: "SINGULAR_H", 4: "SINGULAR_WDELTA", 5: "NONFINITE",
           6: "TIMEOUT", 7: "CANCELLED", 8: "INVALID_SUBSET"}

@@ -59,6 +59,10 @@ typedef enum {
 /* gpv_solve_params.flags */
 #define GPV_SOLVE_ETA 1u     /* omitted-mode diagnostic (src/subset.rs:748-820) */
 #define GPV_SOLVE_HISTORY 2u /* per-iteration (norm, zncc, znssd) history       */
+#define GPV_SOLVE_FAGN 4u    /* forward additive Gauss-Newton instead of ICGN
+                                (solve_fagn_result, src/subset.rs:1228-1334);
+                                FP64 arithmetic in either precision mode, on the
+                                FP64 coefficients when precision is FP64     */
 
 /* gpv_image_create flags */
 #define GPV_IMAGE_KEEP_F64 1u /* also keep FP64 coefficients (needed by GPV_PREC_FP64) */
@@ -249,7 +253,7 @@ typedef struct {
     int32_t batch_factor;     /* layer-RG roots per round / worker    [4]    */
     int32_t max_workers;      /* the worker count rounds are sized by (the
                                  reference's rayon pool size), >= 1          */
-    int32_t reserved;
+    int32_t method;           /* 0 = ICGN, 1 = FAGN (SolveMethod, :284-288)  */
     const gpv_mask *mask;     /* global mask or NULL (gpv_mesh_solve only)   */
     gpv_progress_fn progress; /* or NULL */
     void *progress_user;

@@ -58,7 +58,7 @@ typedef struct {
     double max_norm;
     double tolerance;
     int32_t max_iterations;
-    int32_t flags; /* bit 0: eta diagnostic */
+    int32_t flags; /* bit 0: eta diagnostic; bit 2: FAGN instead of ICGN */
 } gpvo_params;
 
 enum {
@@ -731,6 +731,92 @@ static void solve_one(const spline *F, const spline *G, const gpvo_desc *d, cons
     free(g); free(sdi); subset_free(&s);
 }
 
+/* Subset::solve_fagn_result (src/subset.rs:1228-1334): per iteration the
+ * target value and gradient at the warped positions, g_m and delta_g, the
+ * steepest-descent images from the target gradient about the warped centre
+ * coord + (u, v), H = SDI^T SDI, delta_p_fagn (:452-473), p += dp. */
+static void solve_one_fagn(const spline *F, const spline *G, const gpvo_desc *d, const gpvo_params *prm,
+                           const uint8_t *mask, int64_t mh, int64_t mw, gpvo_result *r, double *hist) {
+    int order = d->order;
+    if (order < 0 || order > 2 || d->radius <= 0) { fill_failed(r, d, 12, ST_INVALID); return; }
+    int m = p_len(order);
+    subset_ref s;
+    int st = subset_new(F, d->coord, d->radius, mask, mh, mw, &s);
+    if (st != ST_OK) {
+        fill_failed(r, d, m, st);
+        r->n_px = (int32_t)s.n;
+        r->f_m = s.f_m; r->delta_f = s.delta_f;
+        subset_free(&s);
+        return;
+    }
+    int64_t n = s.n;
+    double size = sqrt((double)n);
+    double *sdi = (double *)malloc(sizeof(double) * n * m);
+    double *g = (double *)calloc(n, sizeof(double));
+    double *gc = (double *)malloc(sizeof(double) * 2 * n);
+    double *gg = (double *)malloc(sizeof(double) * 2 * n);
+    memset(r, 0, sizeof(*r));
+    r->n_px = (int32_t)n; r->f_m = s.f_m; r->delta_f = s.delta_f; r->sssig = s.sssig; r->sigma = s.sigma;
+    double p[12] = {0}, dp[12], grad_z[12], H[144], Hi[144];
+    for (int k = 0; k < m; k++) p[k] = d->p0[k];
+    int converged = 0, iters = 0, status = ST_OK;
+    double last_norm = 0.0, c_zncc = 0.0, c_znssd = 4.0;
+    for (int it = 1; it <= prm->max_iterations; it++) {
+        double g_center[2] = {d->coord[0] + p[0], d->coord[1] + p[1]};
+        for (int64_t i = 0; i < n; i++) {
+            warp_point(d->coord, p, m, s.fc[2 * i], s.fc[2 * i + 1], &gc[2 * i], &gc[2 * i + 1]);
+            g[i] = sp_eval_grad(G, gc[2 * i], gc[2 * i + 1], &gg[2 * i], &gg[2 * i + 1]);
+        }
+        double gs = 0.0;
+        for (int64_t i = 0; i < n; i++) gs += g[i];
+        double g_m = gs / (double)n, gss = 0.0;
+        for (int64_t i = 0; i < n; i++) gss += (g[i] - g_m) * (g[i] - g_m);
+        double delta_g = sqrt(gss);
+        for (int64_t i = 0; i < n; i++)
+            sdi_row(gc[2 * i] - g_center[0], gc[2 * i + 1] - g_center[1], gg[2 * i], gg[2 * i + 1], m, sdi + i * m);
+        for (int a = 0; a < m; a++)
+            for (int b = a; b < m; b++) {
+                double dot = 0.0;
+                for (int64_t k = 0; k < n; k++) dot += sdi[k * m + a] * sdi[k * m + b];
+                H[a * m + b] = dot; H[b * m + a] = dot;
+            }
+        for (int k = 0; k < m; k++) grad_z[k] = 0.0;
+        for (int k = 0; k < m; k++)
+            for (int64_t i = 0; i < n; i++)
+                grad_z[k] += sdi[i * m + k] * ((s.f[i] - s.f_m) * (delta_g / s.delta_f) - (g[i] - g_m));
+        if (!invert(H, m, Hi)) { status = ST_SINGULAR_H; break; }  /* the reference panics */
+        for (int k = 0; k < m; k++) {
+            double acc = 0.0;
+            for (int j = 0; j < m; j++) acc += Hi[k * m + j] * grad_z[j];
+            dp[k] = acc;
+        }
+        for (int k = 0; k < m; k++) p[k] += dp[k];
+        double nrm = gpvo_norm(dp, m, size);
+        double z = gpvo_znssd(s.f, g, n, s.f_m, g_m, s.delta_f, delta_g);
+        c_znssd = z;
+        c_zncc = 1.0 - z / 2.0;
+        iters = it;
+        last_norm = nrm;
+        if (hist) { hist[3 * (it - 1)] = nrm; hist[3 * (it - 1) + 1] = c_zncc; hist[3 * (it - 1) + 2] = z; }
+        if (!isfinite(nrm)) { status = ST_NONFINITE; break; }
+        if (nrm < prm->max_norm) { converged = 1; break; }
+    }
+    for (int k = 0; k < m; k++) r->p[k] = p[k];
+    r->c_zncc = c_zncc; r->c_znssd = c_znssd; r->norm = last_norm;
+    r->iterations = iters; r->converged = converged;
+    r->quality_ok = converged && c_zncc >= prm->tolerance;
+    r->status = status;
+    if ((prm->flags & 1) && iters > 0 && status == ST_OK) {
+        double gs = 0.0;
+        for (int64_t i = 0; i < n; i++) gs += g[i];
+        double g_m = gs / (double)n, gss = 0.0;
+        for (int64_t i = 0; i < n; i++) gss += (g[i] - g_m) * (g[i] - g_m);
+        gpvo_eta(d->coord, order, s.fc, s.grad, s.f, s.f_m, s.delta_f, g, g_m, sqrt(gss), n, &r->eta_u, &r->eta_v);
+        r->has_eta = 1;
+    }
+    free(sdi); free(g); free(gc); free(gg); subset_free(&s);
+}
+
 /* Batch entry: nthreads OpenMP workers, one subset per task (dynamic). */
 void gpvo_solve_batch(const double *cf, const double *cg, int64_t h, int64_t w, int64_t border,
                       const gpvo_desc *desc, int64_t n, const gpvo_params *prm, const uint8_t *mask,
@@ -738,9 +824,13 @@ void gpvo_solve_batch(const double *cf, const double *cg, int64_t h, int64_t w, 
     spline F = {cf, h, w, border, w + 2 * border};
     spline G = {cg, h, w, border, w + 2 * border};
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
-    for (int64_t i = 0; i < n; i++)
-        solve_one(&F, &G, &desc[i], prm, mask, h, w, &out[i],
-                  history ? history + i * (int64_t)prm->max_iterations * 3 : NULL);
+    for (int64_t i = 0; i < n; i++) {
+        double *hi = history ? history + i * (int64_t)prm->max_iterations * 3 : NULL;
+        if (prm->flags & 4)
+            solve_one_fagn(&F, &G, &desc[i], prm, mask, h, w, &out[i], hi);
+        else
+            solve_one(&F, &G, &desc[i], prm, mask, h, w, &out[i], hi);
+    }
 }
 
 /* Reference-subset quantities only (Subset::new), for the setup parity tests. */

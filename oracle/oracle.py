@@ -213,11 +213,13 @@ def subset_setup(coef, shape, border, coord, radius, mask=None):
 
 
 def solve_batch(coef_f, coef_g, shape, border, desc, max_norm=1e-5, max_iterations=50, tolerance=0.75,
-                eta=False, mask=None, history=False, nthreads=0):
-    """Batched Subset::new + solve_icgn_result (src/subset.rs:836-919, 1117-1219)."""
+                eta=False, mask=None, history=False, nthreads=0, method="icgn"):
+    """Batched Subset::new + solve_icgn_result (src/subset.rs:836-919, 1117-1219),
+    or solve_fagn_result (:1228-1334) with method="fagn"."""
     desc = np.ascontiguousarray(desc, dtype=DESC_DTYPE)
     prm = np.zeros(1, PARAMS_DTYPE)
-    prm["max_norm"], prm["tolerance"], prm["max_iterations"], prm["flags"] = max_norm, tolerance, max_iterations, int(eta)
+    flags = int(eta) | (4 if method == "fagn" else 0)
+    prm["max_norm"], prm["tolerance"], prm["max_iterations"], prm["flags"] = max_norm, tolerance, max_iterations, flags
     out = np.zeros(desc.size, RESULT_DTYPE)
     hist = np.zeros((desc.size, max_iterations, 3)) if history else None
     m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
