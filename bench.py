@@ -425,7 +425,7 @@ def serving_leg(seconds=10.0, rate=200.0, workers=6, seed=55):
             order = rng.integers(1, 3, m).astype(np.int32)
             desc = gpv.make_desc(xy, radius, order, synth.seeded_p0(fld, xy, rng))
             pool.append((fp.numpy().view(dt), gp.numpy().view(dt), desc, (fp, gp)))
-    srv = gpv.Server(workers=workers)
+    srv = gpv.Server(workers=workers, reserve_subsets=100000, reserve_radius=50)
     # warm-up: every pool entry once (image caches, tables, workspace)
     for f, g, d, _ in pool:
         srv.wait(srv.submit(f, g, d[:2000]), 120000)
@@ -460,6 +460,7 @@ def serving_leg(seconds=10.0, rate=200.0, workers=6, seed=55):
             "requests_5k_20k_subsets": int(mid.sum()),
             "subsets_per_s": float(ns.sum() / wall), "subsets": int(ns.sum()), "wall_s": wall,
             "mean_converged_frac": float(np.mean(conv)), "peak_admitted_bytes": int(st["peak_bytes"]),
+            "mean_queue_ms": st["mean_queue_ms"], "mean_service_ms": st["mean_service_ms"],
             "hbm_budget_bytes": int(st["hbm_budget"]),
             "latency": "submit -> results in host memory; pinned host pixels; per request: H2D, prefilter x2, solve, D2H"}
 

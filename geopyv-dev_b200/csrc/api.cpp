@@ -382,7 +382,7 @@ int gpv_context_reserve(gpv_context *ctx, int64_t n_subsets, int32_t max_radius,
     if (int rc = ctx->desc_dev.ensure(sizeof(gpv_subset_desc) * (size_t)n_subsets)) return rc;
     if (int rc = ctx->out_dev.ensure(sizeof(gpv_subset_result) * (size_t)n_subsets)) return rc;
     if (int rc = ctx->order_dev.ensure(sizeof(int32_t) * (size_t)n_subsets)) return rc;
-    if (int rc = ctx->tile_ws.ensure(sizeof(int32_t) * (32 + (size_t)n_subsets))) return rc;
+    if (int rc = ctx->tile_ws.ensure(sizeof(int32_t) * (96 + (size_t)n_subsets))) return rc;
     (void)max_iterations;
     return GPV_SUCCESS;
 }
@@ -460,7 +460,10 @@ int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, co
     L.out = static_cast<gpv_subset_result *>(ctx->out_dev.ptr);
     L.history = hist_dev;
     L.max_radius = max_r;
-    if (int rc = solve_launch(ctx, L, ctx->stream)) return rc;
+    ctx->seg_mask = tile_segment_mask(desc, n, max_r);  // launch only the segments this batch holds
+    const int rc_launch = solve_launch(ctx, L, ctx->stream);
+    ctx->seg_mask = 0xFFFFFFFFu;
+    if (rc_launch) return rc_launch;
     GPV_CUDA_TRY(cudaMemcpyAsync(out, ctx->out_dev.ptr, sizeof(gpv_subset_result) * n, cudaMemcpyDeviceToHost, ctx->stream));
     if (prm->history) {
         GPV_CUDA_TRY(cudaMemcpyAsync(prm->history, hist_dev, hist_bytes, cudaMemcpyDeviceToHost, ctx->stream));

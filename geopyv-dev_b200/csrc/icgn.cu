@@ -764,7 +764,7 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
         return GPV_SUCCESS;
     }
     if (!fp64 && !use_warp_kernel()) {
-        if (int rc = ctx->tile_ws.ensure(sizeof(int32_t) * (32 + (size_t)L.n))) return rc;
+        if (int rc = ctx->tile_ws.ensure(sizeof(int32_t) * (96 + (size_t)L.n))) return rc;
         return tile_launch(ctx, A, L.n, s);
     }
     int workers, threads;

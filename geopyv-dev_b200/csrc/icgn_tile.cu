@@ -21,6 +21,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <mutex>
+#include <set>
+#include <utility>
 
 #include "icgn_common.cuh"
 
@@ -678,47 +681,69 @@ __global__ void __launch_bounds__(NT, 512 / NT) icgn_tile(TileArgs T) {
     }
 }
 
-// Split the work list by warp order: seg[2k], seg[2k+1] = start, count of
-// order 2 - k (order 2 first); order_out holds the segments back to back.
-// Subsets with an order outside {0, 1, 2} are failed here.
-__global__ void count_orders(const gpv_subset_desc *desc, const int32_t *order_in, int n, int32_t *cnt) {
+// Split the work list into segments by (order, radius class): segment
+// q = (2 - order) * kRClasses + class, the class being the first upper bound
+// in kRBound that the radius does not exceed.  seg[2q], seg[2q+1] = start,
+// count; order_out holds the segments back to back.  Each segment is solved
+// by its own launch, with a shared-memory window and thread count sized for
+// its largest radius, so small subsets in a batch with large ones keep the
+// occupancy of their own size.  Subsets with an order outside {0, 1, 2} or a
+// radius outside 1..max_radius are failed here.
+constexpr int kRClasses = 4;
+constexpr int kSegs = 3 * kRClasses;
+__constant__ int kRBound[kRClasses] = {20, 32, 48, 1 << 20};
+constexpr int kRBoundHost[kRClasses] = {20, 32, 48, 1 << 20};
+
+__device__ __forceinline__ int segment_of(const gpv_subset_desc &d, int max_radius) {
+    if (d.order < 0 || d.order > 2 || d.radius < 1 || d.radius > max_radius) return -1;
+    int c = 0;
+    while (c < kRClasses - 1 && d.radius > kRBound[c]) c++;
+    return (2 - d.order) * kRClasses + c;
+}
+
+__global__ void count_orders(const gpv_subset_desc *desc, const int32_t *order_in, int n, int max_radius,
+                             int32_t *cnt) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int o = -1;
-    if (i < n) o = desc[order_in ? order_in[i] : i].order;
+    int q = -1;
+    if (i < n) q = segment_of(desc[order_in ? order_in[i] : i], max_radius);
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-        const unsigned m = __ballot_sync(0xffffffffu, o == 2 - k);
+    for (int k = 0; k < kSegs; k++) {
+        const unsigned m = __ballot_sync(0xffffffffu, q == k);
         if ((threadIdx.x & 31) == 0 && m) atomicAdd(cnt + k, __popc(m));
     }
 }
 
-__global__ void scatter_orders(const gpv_subset_desc *desc, const int32_t *order_in, int n, const int32_t *cnt,
-                               int32_t *fill, int32_t *order_out, int32_t *seg, gpv_subset_result *out) {
+__global__ void scatter_orders(const gpv_subset_desc *desc, const int32_t *order_in, int n, int max_radius,
+                               const int32_t *cnt, int32_t *fill, int32_t *order_out, int32_t *seg,
+                               gpv_subset_result *out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    int idx = -1, o = -1;
+    int idx = -1, q = -1;
     if (i < n) {
         idx = order_in ? order_in[i] : i;
-        o = desc[idx].order;
+        q = segment_of(desc[idx], max_radius);
     }
-    const int start[3] = {0, cnt[0], cnt[0] + cnt[1]};
+    int start[kSegs];
+    start[0] = 0;
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-        const unsigned m = __ballot_sync(0xffffffffu, o == 2 - k);
+    for (int k = 1; k < kSegs; k++) start[k] = start[k - 1] + cnt[k - 1];
+#pragma unroll
+    for (int k = 0; k < kSegs; k++) {
+        const unsigned m = __ballot_sync(0xffffffffu, q == k);
         if (!m) continue;
         int base = 0;
         const int leader = __ffs(m) - 1;
         if (lane == leader) base = atomicAdd(fill + k, __popc(m));
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (o == 2 - k) order_out[start[k] + base + __popc(m & ((1u << lane) - 1))] = idx;
+        if (q == k) order_out[start[k] + base + __popc(m & ((1u << lane) - 1))] = idx;
     }
-    if (i < n && (o < 0 || o > 2)) {
+    if (i < n && q < 0) {
         const gpv_subset_desc d = desc[idx];
         write_failed_any(out, idx, d, GPV_INVALID_SUBSET);
     }
     if (i == 0) {
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
+        for (int k = 0; k < kSegs; k++) {
             seg[2 * k] = start[k];
             seg[2 * k + 1] = cnt[k];
         }
@@ -745,54 +770,119 @@ void tile_launch_one(int order, int blocks, size_t smem, cudaStream_t s, const T
 // size rule (GPV_TILE_THREADS overrides).
 int tile_threads_for(gpv_context *ctx, int max_radius);
 
-// Launch the three per-order kernels.
+// Raise a kernel's dynamic shared-memory limit to everything the device
+// allows beside its static shared memory, once per (device, kernel).  The
+// limit is a per-function attribute shared by every thread of the process:
+// setting it to each launch's own size would let concurrent launches of the
+// same kernel with different windows (two contexts, two host threads) undo
+// each other's setting between the set and the launch.
+static int allow_max_dynamic_smem(const void *fn) {
+    static std::mutex mu;
+    static std::set<std::pair<int, const void *>> done;
+    int dev = 0;
+    GPV_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({dev, fn})) return GPV_SUCCESS;
+    int optin = 0;
+    GPV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa;
+    GPV_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
+    GPV_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+    done.insert({dev, fn});
+    return GPV_SUCCESS;
+}
+
+// Window capacity (floats) for subsets up to radius r: a radius-r subset
+// stretched by 6%, plus margins.
+static int window_cap(int r) {
+    const int rw = (int)std::ceil(1.06 * r) + 2;
+    const int side = 2 * rw + 6 + 2 * kMargin + 4;
+    return side * side;
+}
+
+uint32_t tile_segment_mask(const gpv_subset_desc *desc, int64_t n, int max_radius) {
+    uint32_t mask = 0;
+    for (int64_t i = 0; i < n; i++) {
+        const gpv_subset_desc &d = desc[i];
+        if (d.order < 0 || d.order > 2 || d.radius < 1 || d.radius > max_radius) continue;
+        int c = 0;
+        while (c < kRClasses - 1 && d.radius > kRBoundHost[c]) c++;
+        mask |= 1u << ((2 - d.order) * kRClasses + c);
+    }
+    return mask;
+}
+
+// Launch one kernel per (order, radius class) segment that can hold
+// subsets, spread over the context stream and its two auxiliary streams;
+// kernels sharing a stream run one after the other and share its scratch.
 int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
     int32_t *ws = static_cast<int32_t *>(ctx->tile_ws.ptr);
-    int32_t *cnt = ws, *fill = ws + 4, *seg = ws + 8, *queues = ws + 16, *order_out = ws + 32;
-    GPV_CUDA_TRY(cudaMemsetAsync(ws, 0, 32 * sizeof(int32_t), s));
+    int32_t *cnt = ws, *fill = ws + 16, *seg = ws + 32, *queues = ws + 64, *order_out = ws + 96;
+    GPV_CUDA_TRY(cudaMemsetAsync(ws, 0, 96 * sizeof(int32_t), s));
     const unsigned blocks = (unsigned)((n + 255) / 256);
-    count_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, cnt);
-    scatter_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, cnt, fill, order_out, seg, K.out);
+    count_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, K.max_radius, cnt);
+    scatter_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, K.max_radius, cnt, fill, order_out, seg, K.out);
     GPV_CUDA_TRY(cudaGetLastError());
-    const int nt = tile_threads_for(ctx, K.max_radius);
-    // window capacity: a radius-max_radius subset stretched by 6%, plus margins
-    const int rw = (int)std::ceil(1.06 * K.max_radius) + 2;
-    const int side = 2 * rw + 6 + 2 * kMargin + 4;
-    const int cap = side * side;
-    const size_t smem = sizeof(float) * cap;
-    TileArgs T;
-    T.k = K;
-    T.k.order = order_out;
-    T.win_cap = cap;
     const char *lay = getenv("GPV_TILE_LAYOUT");
-    T.padded = lay && lay[0] == 'p';
+    const bool padded = lay && lay[0] == 'p';
+    struct Plan {
+        int rmax = 0, nt = 0, cap = 0, blocks = 0;
+        int64_t stride = 0;
+        bool live = false;
+    };
+    Plan plan[kSegs];
+    int64_t region = 0;  // scratch floats per stream: its largest launch
+    for (int q = 0; q < kSegs; q++) {
+        const int order = 2 - q / kRClasses, c = q % kRClasses;
+        const int lo = c == 0 ? 0 : kRBoundHost[c - 1];
+        Plan &P = plan[q];
+        P.live = lo < K.max_radius && ((ctx->seg_mask >> q) & 1u);
+        if (!P.live) continue;
+        P.rmax = std::min(kRBoundHost[c], K.max_radius);
+        P.nt = tile_threads_for(ctx, P.rmax);
+        P.cap = window_cap(P.rmax);
+        const size_t smem = sizeof(float) * P.cap;
+        const void *fn = P.nt == 256 ? tile_kernel<256>(order) : tile_kernel<128>(order);
+        if (int rc = allow_max_dynamic_smem(fn)) return rc;
+        int per_sm = 0;
+        GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, P.nt, smem));
+        if (per_sm < 1) { set_error("subset window does not fit in shared memory"); return GPV_ERR_INVALID; }
+        P.blocks = per_sm * ctx->num_sms;
+        const int64_t nmax = (int64_t)(ctx->h_slot_n[P.rmax] + 31) / 32 * 32;
+        P.stride = 5 * nmax;  // float4 record + eta sample per pixel
+        region = std::max(region, (int64_t)P.blocks * P.stride);
+    }
+    if (int rc = ctx->scratch.ensure((size_t)3 * region * sizeof(float))) return rc;
     GPV_CUDA_TRY(cudaEventRecord(ctx->ev[0], s));
     cudaStream_t st[3] = {s, ctx->aux[0], ctx->aux[1]};
-    int total_blocks = 0;
-    for (int k = 0; k < 3; k++) {
-        int per_sm = 0;
-        const void *fn = nt == 256 ? tile_kernel<256>(2 - k) : tile_kernel<128>(2 - k);
-        GPV_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nt, smem));
-        if (per_sm < 1) { set_error("subset window does not fit in shared memory"); return GPV_ERR_INVALID; }
-        total_blocks = std::max(total_blocks, per_sm * ctx->num_sms);
-    }
-    // scratch: one slot per resident block of each of the three kernels
-    const int64_t nmax = (int64_t)(ctx->h_slot_n[K.max_radius] + 31) / 32 * 32;
-    const int64_t stride = 5 * nmax;  // float4 record + eta sample per pixel
-    if (int rc = ctx->scratch.ensure((size_t)3 * total_blocks * stride * sizeof(float))) return rc;
-    for (int k = 0; k < 3; k++) {
-        if (k > 0) GPV_CUDA_TRY(cudaStreamWaitEvent(st[k], ctx->ev[0], 0));
-        TileArgs Tk = T;
-        Tk.seg = seg + 2 * k;
-        Tk.queue = queues + k;
-        Tk.k.scratch = static_cast<float *>(ctx->scratch.ptr) + (int64_t)k * total_blocks * stride;
-        Tk.k.scratch_stride = stride;
-        if (nt == 256) tile_launch_one<256>(2 - k, total_blocks, smem, st[k], Tk);
-        else tile_launch_one<128>(2 - k, total_blocks, smem, st[k], Tk);
+    bool used[3] = {true, false, false};
+    int next = 0;
+    for (int q = 0; q < kSegs; q++) {
+        const Plan &P = plan[q];
+        if (!P.live) continue;
+        const int k = next;
+        next = (next + 1) % 3;
+        if (!used[k]) {
+            GPV_CUDA_TRY(cudaStreamWaitEvent(st[k], ctx->ev[0], 0));
+            used[k] = true;
+        }
+        TileArgs T;
+        T.k = K;
+        T.k.order = order_out;
+        T.k.max_radius = P.rmax;
+        T.win_cap = P.cap;
+        T.padded = padded;
+        T.seg = seg + 2 * q;
+        T.queue = queues + q;
+        T.k.scratch = static_cast<float *>(ctx->scratch.ptr) + (int64_t)k * region;
+        T.k.scratch_stride = P.stride;
+        const size_t smem = sizeof(float) * P.cap;
+        if (P.nt == 256) tile_launch_one<256>(2 - q / kRClasses, P.blocks, smem, st[k], T);
+        else tile_launch_one<128>(2 - q / kRClasses, P.blocks, smem, st[k], T);
         GPV_CUDA_TRY(cudaGetLastError());
     }
     for (int k = 1; k < 3; k++) {
+        if (!used[k]) continue;
         GPV_CUDA_TRY(cudaEventRecord(ctx->ev[k], st[k]));
         GPV_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev[k], 0));
     }

@@ -81,6 +81,7 @@ struct gpv_context {
     int mixed_blocks_per_sm = 0;
     int tuned_threads[3] = {0, 0, 0};  // autotuned threads per block by radius class
     int force_threads = 0;             // set while the autotuner times a candidate
+    uint32_t seg_mask = 0xFFFFFFFFu;   // tiled-solve segments a host batch holds (all when unknown)
     // owner reference + one per image / mask created on it: the context is
     // freed when gpv_context_destroy and every dependant's destroy have run,
     // in whatever order they come
@@ -130,6 +131,9 @@ int probe_fp32_peak(gpv_context *ctx, double *tflops);
 int mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements, int64_t n_elements,
                int32_t nodes_per_element, const gpv_mesh_params *mp, gpv_batch_solver_fn solver, void *solver_user,
                gpv_subset_result *out, int32_t *rounds, gpv_mesh_stats *stats);
+// The (order, radius class) segments of the tiled solve that a host batch
+// holds (bit q = segment q); lets the launcher skip empty segments.
+uint32_t tile_segment_mask(const gpv_subset_desc *desc, int64_t n, int max_radius);
 int solve_noalloc_launch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
                          int64_t n, int max_radius, const gpv_solve_params *prm, gpv_subset_result *out_dev,
                          cudaStream_t s);

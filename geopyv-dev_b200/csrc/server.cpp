@@ -92,6 +92,7 @@ struct gpv_server {
     size_t bytes_in_flight = 0, peak_bytes = 0;
     int64_t submitted = 0, completed = 0, failed = 0, in_flight = 0, subsets_done = 0;
     std::vector<double> latencies_ms;
+    double queue_ms_sum = 0.0, service_ms_sum = 0.0;
     Clock::time_point t_first, t_last;
     bool any_done = false;
 };
@@ -218,6 +219,8 @@ void worker_loop(gpv_server *S, Worker *W) {
                 S->completed++;
                 S->subsets_done += q->r.n;
                 S->latencies_ms.push_back(std::chrono::duration<double, std::milli>(q->t_done - q->t_submit).count());
+                S->queue_ms_sum += std::chrono::duration<double, std::milli>(q->t_start - q->t_submit).count();
+                S->service_ms_sum += std::chrono::duration<double, std::milli>(q->t_done - q->t_start).count();
                 if (!S->any_done) S->t_first = q->t_submit;
                 S->any_done = true;
                 S->t_last = q->t_done;
@@ -264,7 +267,12 @@ int gpv_server_create(const gpv_server_config *cfg, gpv_server **out) {
         auto W = std::make_unique<Worker>();
         W->index = k;
         if (!cfg->executor) {
-            if (int rc = gpv_context_create(cfg->device, &W->ctx)) {
+            int rc = gpv_context_create(cfg->device, &W->ctx);
+            // sized once here, the workspace never grows (nor frees) while serving
+            if (!rc && cfg->reserve_subsets > 0 && cfg->reserve_radius > 0)
+                rc = gpv_context_reserve(W->ctx, cfg->reserve_subsets, cfg->reserve_radius, 50);
+            if (rc) {
+                S->workers.push_back(std::move(W));
                 for (auto &w : S->workers) release_worker(*w);
                 delete S;
                 return rc;
@@ -363,6 +371,8 @@ int gpv_server_get_stats(gpv_server *S, gpv_server_stats *st) {
         double s = 0.0;
         for (double x : v) s += x;
         st->mean_ms = s / (double)v.size();
+        st->mean_queue_ms = S->queue_ms_sum / (double)v.size();
+        st->mean_service_ms = S->service_ms_sum / (double)v.size();
         const double span = std::chrono::duration<double>(S->t_last - S->t_first).count();
         st->subsets_per_s = span > 0 ? (double)S->subsets_done / span : 0.0;
     }
@@ -373,6 +383,7 @@ int gpv_server_reset_stats(gpv_server *S) {
     if (!S) { set_error("NULL argument"); return GPV_ERR_INVALID; }
     std::lock_guard<std::mutex> lk(S->mu);
     S->latencies_ms.clear();
+    S->queue_ms_sum = S->service_ms_sum = 0.0;
     S->completed = S->failed = S->subsets_done = 0;
     S->submitted = (int64_t)S->queue.size() + S->in_flight;
     S->peak_bytes = S->bytes_in_flight;

@@ -64,13 +64,15 @@ class Request(ct.Structure):
 
 class ServerConfig(ct.Structure):
     _fields_ = [("hbm_budget", ct.c_size_t), ("workers", ct.c_int32), ("device", ct.c_int32),
-                ("executor", EXECUTOR_FN), ("executor_user", ct.c_void_p)]
+                ("executor", EXECUTOR_FN), ("executor_user", ct.c_void_p), ("reserve_subsets", ct.c_int64),
+                ("reserve_radius", ct.c_int32), ("reserved", ct.c_int32)]
 
 
 class ServerStats(ct.Structure):
     _fields_ = [("submitted", ct.c_int64), ("completed", ct.c_int64), ("failed", ct.c_int64), ("queued", ct.c_int64),
                 ("in_flight", ct.c_int64), ("subsets", ct.c_int64), ("p50_ms", ct.c_double), ("p99_ms", ct.c_double),
-                ("mean_ms", ct.c_double), ("max_ms", ct.c_double), ("subsets_per_s", ct.c_double),
+                ("mean_ms", ct.c_double), ("max_ms", ct.c_double), ("mean_queue_ms", ct.c_double),
+                ("mean_service_ms", ct.c_double), ("subsets_per_s", ct.c_double),
                 ("bytes_in_flight", ct.c_size_t), ("peak_bytes", ct.c_size_t), ("hbm_budget", ct.c_size_t)]
 
 

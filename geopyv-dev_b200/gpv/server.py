@@ -27,11 +27,14 @@ class Ticket:
 
 
 class Server:
-    def __init__(self, workers: int = 4, hbm_budget: int = 0, device: int = 0, executor=None):
+    def __init__(self, workers: int = 4, hbm_budget: int = 0, device: int = 0, executor=None,
+                 reserve_subsets: int = 0, reserve_radius: int = 0):
         """executor(worker, request_dict, desc, out) -> int replaces the GPU solve
-        (a stand-in for exercising the request loop without a GPU)."""
+        (a stand-in for exercising the request loop without a GPU).
+        reserve_subsets / reserve_radius size every worker's workspace up front."""
         cfg = _lib.ServerConfig()
         cfg.hbm_budget, cfg.workers, cfg.device = hbm_budget, workers, device
+        cfg.reserve_subsets, cfg.reserve_radius = reserve_subsets, reserve_radius
         self._cb = None
         if executor is not None:
             def _exec(user, worker, req_p, desc_p, out_p):

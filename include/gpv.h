@@ -327,11 +327,15 @@ typedef struct {
     int32_t device;
     gpv_request_executor_fn executor;  /* NULL = GPU */
     void *executor_user;
+    int64_t reserve_subsets;  /* size each worker's workspace for this many subsets */
+    int32_t reserve_radius;   /* of up to this radius (0, 0 = grow on demand)       */
+    int32_t reserved;
 } gpv_server_config;
 
 typedef struct {
     int64_t submitted, completed, failed, queued, in_flight, subsets;
     double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> results in host memory */
+    double mean_queue_ms, mean_service_ms;   /* submit -> start, start -> done */
     double subsets_per_s;                    /* completed subsets / (last done - first submit) */
     size_t bytes_in_flight, peak_bytes, hbm_budget;
 } gpv_server_stats;

@@ -64,8 +64,9 @@ def test_session_frames_match_the_frame_tracker(gpv_mod):
                        seed_from_previous=k > 0)
         served.append(srv.wait(t, 60000).copy())
     srv.close()
-    F = gpv_mod.Image(image_gs=W0["f"])
-    G = gpv_mod.Image(image_gs=W0["f"])
+    ctx = gpv_mod.Context(0)  # untuned, like the server's worker contexts
+    F = gpv_mod.Image(image_gs=W0["f"], ctx=ctx)
+    G = gpv_mod.Image(image_gs=W0["f"], ctx=ctx)
     seq = gpv_mod.SubsetSequence(F, G, desc, np.uint8)
     for W, got in zip(Ws, served):
         assert seq.frame(W["g"]).tobytes() == got.tobytes()
