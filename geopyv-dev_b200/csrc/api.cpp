@@ -54,9 +54,9 @@ int ensure_tables(gpv_context *ctx, int max_radius) {
         set_error("radius above 4000 is not supported");
         return GPV_ERR_INVALID;
     }
+    const int R1 = max_radius + 1;
     std::vector<short2_h> offs, slots;
-    std::vector<int32_t> toff(max_radius + 1, 0), tn(max_radius + 1, 0), soff(max_radius + 1, 0),
-        sn(max_radius + 1, 0);
+    std::vector<int32_t> toff(R1, 0), tn(R1, 0), soff(R1, 0), sn(R1, 0), qoff(R1, 0), qn(R1, 0), nmax(R1, 0);
     for (int r = 1; r <= max_radius; r++) {
         toff[r] = (int32_t)offs.size();
         soff[r] = (int32_t)slots.size();
@@ -77,21 +77,44 @@ int ensure_tables(gpv_context *ctx, int max_radius) {
         tn[r] = (int32_t)offs.size() - toff[r];
         sn[r] = (int32_t)slots.size() - soff[r];
     }
+    // tiles: the disk covered by 8-wide x 4-high tiles, one per warp, slots in
+    // tile order (4 rows of 8); with a window pitch of 8 mod 32 the 32 lanes
+    // of a tile read 32 different shared-memory banks
+    for (int r = 1; r <= max_radius; r++) {
+        qoff[r] = (int32_t)slots.size();
+        for (int y0 = -r; y0 <= r; y0 += 4) {
+            int xmin = r + 1, xmax = -r - 1;
+            for (int y = y0; y < y0 + 4 && y <= r; y++)
+                for (int x = -r; x <= r; x++)
+                    if (x * x + y * y <= r * r) { xmin = std::min(xmin, x); xmax = std::max(xmax, x); }
+            for (int x0 = xmin; x0 <= xmax; x0 += 8)
+                for (int ty = 0; ty < 4; ty++)
+                    for (int tx = 0; tx < 8; tx++) {
+                        const int x = x0 + tx, y = y0 + ty;
+                        const bool in = y <= r && x * x + y * y <= r * r;
+                        slots.push_back({in ? (int16_t)x : kSlotEmpty, (int16_t)y});
+                    }
+        }
+        qn[r] = (int32_t)slots.size() - qoff[r];
+        nmax[r] = std::max(std::max(tn[r], sn[r]), qn[r]);
+    }
     if (int rc = ctx->offs.ensure(offs.size() * sizeof(short2_h))) return rc;
     if (int rc = ctx->slots.ensure(slots.size() * sizeof(short2_h))) return rc;
-    if (int rc = ctx->tab_off.ensure(2 * toff.size() * sizeof(int32_t))) return rc;
-    if (int rc = ctx->tab_n.ensure(2 * tn.size() * sizeof(int32_t))) return rc;
+    if (int rc = ctx->tab_off.ensure(3 * toff.size() * sizeof(int32_t))) return rc;
+    if (int rc = ctx->tab_n.ensure(3 * tn.size() * sizeof(int32_t))) return rc;
     GPV_CUDA_TRY(cudaMemcpy(ctx->offs.ptr, offs.data(), offs.size() * sizeof(short2_h), cudaMemcpyHostToDevice));
     GPV_CUDA_TRY(cudaMemcpy(ctx->slots.ptr, slots.data(), slots.size() * sizeof(short2_h), cudaMemcpyHostToDevice));
-    // tab_off / tab_n: compact template tables, then the padded slot tables
+    // tab_off / tab_n: compact template tables, padded-row slot tables, tile slot tables
     std::vector<int32_t> to2(toff), tn2(tn);
     to2.insert(to2.end(), soff.begin(), soff.end());
     tn2.insert(tn2.end(), sn.begin(), sn.end());
+    to2.insert(to2.end(), qoff.begin(), qoff.end());
+    tn2.insert(tn2.end(), qn.begin(), qn.end());
     GPV_CUDA_TRY(cudaMemcpy(ctx->tab_off.ptr, to2.data(), to2.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     GPV_CUDA_TRY(cudaMemcpy(ctx->tab_n.ptr, tn2.data(), tn2.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     ctx->h_tab_off = toff;
     ctx->h_tab_n = tn;
-    ctx->h_slot_n = sn;
+    ctx->h_slot_n = nmax;  // the most slots any layout uses (per-block scratch)
     ctx->table_radius = max_radius;
     return GPV_SUCCESS;
 }

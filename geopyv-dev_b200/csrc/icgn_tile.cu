@@ -55,8 +55,18 @@ struct TileArgs {
     const int32_t *seg;  // [start, count] of this order's segment in k.order
     int *queue;          // this kernel's work-queue counter
     int win_cap;         // floats of dynamic shared memory for the window
-    int padded;          // 1: template rows padded to 32 lanes (no straddling warps)
+    int layout;          // template slots: kLayoutCompact, kLayoutRows or kLayoutTiles
 };
+
+// Template slot layouts: the compact scan order; rows padded to whole warps
+// (a warp never straddles two rows); 8 x 4 tiles, one per warp, read from a
+// window whose pitch is 8 mod 32 so a tile's 32 lanes hit 32 different banks.
+constexpr int kLayoutCompact = 0, kLayoutRows = 1, kLayoutTiles = 2;
+
+// Row pitch (floats) of a window `ww` columns wide in a layout.
+__host__ __device__ __forceinline__ int window_pitch(int ww, int layout) {
+    return layout == kLayoutTiles ? ww + ((8 - ww) % 32 + 32) % 32 : ww;
+}
 
 // Copy coefficient rows [r0, r0+wh) x cols [c0, c0+ww) (c0, ww multiples of 4)
 // into win (row pitch ww).  Out-of-range rows / columns are clamped.
@@ -93,12 +103,12 @@ __device__ __forceinline__ void stage_part(const float *__restrict__ C, int64_t 
 
 // Plan a window covering pixel indices [xlo, xhi] x [ylo, yhi] (already
 // clamped to the image) plus kMargin; returns false if it does not fit.
-__device__ __forceinline__ bool plan_window(int xlo, int xhi, int ylo, int yhi, int border, int cap, int &r0, int &c0,
-                                            int &wh, int &ww) {
+__device__ __forceinline__ bool plan_window(int xlo, int xhi, int ylo, int yhi, int border, int cap, int layout,
+                                            int &r0, int &c0, int &wh, int &ww) {
     for (int m = kMargin; m >= 0; m -= kMargin) {
         const int clo = xlo + border - 2 - m, chi = xhi + border + 3 + m;
         c0 = clo >= 0 ? (clo & ~3) : -(((-clo) + 3) & ~3);
-        ww = ((chi + 1 - c0) + 3) & ~3;
+        ww = window_pitch(((chi + 1 - c0) + 3) & ~3, layout);
         r0 = ylo + border - 2 - m;
         wh = yhi + border + 3 + m + 1 - r0;
         if (ww * wh <= cap) return true;
@@ -186,10 +196,10 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
     constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int r = d.radius;
-    // compact template, or rows padded to whole warps (empty slots: x = -32768)
-    const int tab = T.padded ? A.table_radius + 1 + r : r;
+    // compact template, rows padded to whole warps, or 8 x 4 tiles (empty slots: x = -32768)
+    const int tab = T.layout * (A.table_radius + 1) + r;
     const int npx_t = A.tab_n[tab];
-    const short2 *po = (T.padded ? A.slots : A.offs) + A.tab_off[tab];
+    const short2 *po = (T.layout != kLayoutCompact ? A.slots : A.offs) + A.tab_off[tab];
     const double cx = d.coord[0], cy = d.coord[1];
     const int cxi = (int)cx, cyi = (int)cy;
     const double fxd = floor(cx), fyd = floor(cy);
@@ -203,7 +213,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         const int xlo = max(0, min(bx - r - 1, A.w - 1)), xhi = max(0, min(bx + r + 1, A.w - 1));
         const int ylo = max(0, min(by - r - 1, A.h - 1)), yhi = max(0, min(by + r + 1, A.h - 1));
         int r0, c0, wh, ww;
-        const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, r0, c0, wh, ww);
+        const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, T.layout, r0, c0, wh, ww);
         if (ok) stage<NT>(A.f32, A.pitch32, ch, r0, c0, wh, ww, win);
         if (tid == 0) {
             sm.win_ok = 0;  // g must be staged before the iterations
@@ -372,7 +382,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
 #pragma unroll
         for (int k = 0; k < 12; k++) p0[k] = d.p0[k % M];
         warp_extent<ORDER>(p0, cx, cy, r, A.w, A.h, xlo, xhi, ylo, yhi);
-        const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, r0, c0, wh, ww);
+        const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, T.layout, r0, c0, wh, ww);
         if (ok) stage_part<NT>(A.g32, A.pitch32, ch, r0, c0, wh, ww, win, 32);
         if (tid == 32) {
             sm.win_ok = ok;
@@ -410,7 +420,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             warp_extent<ORDER>(sm.p, cx, cy, r, A.w, A.h, xlo, xhi, ylo, yhi);
             if (!window_covers(sm, xlo, xhi, ylo, yhi, B)) {
                 int r0, c0, wh, ww;
-                const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, r0, c0, wh, ww);
+                const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, T.layout, r0, c0, wh, ww);
                 __syncthreads();  // nobody still reads the old window
                 if (ok) stage<NT>(A.g32, A.pitch32, ch, r0, c0, wh, ww, win);
                 if (tid == 0) {
@@ -794,10 +804,10 @@ static int allow_max_dynamic_smem(const void *fn) {
 
 // Window capacity (floats) for subsets up to radius r: a radius-r subset
 // stretched by 6%, plus margins.
-static int window_cap(int r) {
+static int window_cap(int r, int layout) {
     const int rw = (int)std::ceil(1.06 * r) + 2;
     const int side = 2 * rw + 6 + 2 * kMargin + 4;
-    return side * side;
+    return side * window_pitch(side, layout);
 }
 
 uint32_t tile_segment_mask(const gpv_subset_desc *desc, int64_t n, int max_radius) {
@@ -823,8 +833,11 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
     count_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, K.max_radius, cnt);
     scatter_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, K.max_radius, cnt, fill, order_out, seg, K.out);
     GPV_CUDA_TRY(cudaGetLastError());
+    // GPV_TILE_LAYOUT = compact (default) | rows | tiles; the compact layout
+    // measured fastest: the other two remove most bank conflicts but add
+    // empty slots, and the kernel is latency- rather than bank-bound
     const char *lay = getenv("GPV_TILE_LAYOUT");
-    const bool padded = lay && lay[0] == 'p';
+    const int layout = !lay ? kLayoutCompact : (lay[0] == 'r' ? kLayoutRows : (lay[0] == 't' ? kLayoutTiles : kLayoutCompact));
     struct Plan {
         int rmax = 0, nt = 0, cap = 0, blocks = 0;
         int64_t stride = 0;
@@ -840,7 +853,7 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         if (!P.live) continue;
         P.rmax = std::min(kRBoundHost[c], K.max_radius);
         P.nt = tile_threads_for(ctx, P.rmax);
-        P.cap = window_cap(P.rmax);
+        P.cap = window_cap(P.rmax, layout);
         const size_t smem = sizeof(float) * P.cap;
         const void *fn = P.nt == 256 ? tile_kernel<256>(order) : tile_kernel<128>(order);
         if (int rc = allow_max_dynamic_smem(fn)) return rc;
@@ -871,7 +884,7 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         T.k.order = order_out;
         T.k.max_radius = P.rmax;
         T.win_cap = P.cap;
-        T.padded = padded;
+        T.layout = layout;
         T.seg = seg + 2 * q;
         T.queue = queues + q;
         T.k.scratch = static_cast<float *>(ctx->scratch.ptr) + (int64_t)k * region;

@@ -12,7 +12,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgpv_b200.so")
+# GPV_LIB selects another build of the library (e.g. one compiled with
+# different tuning macros); the default is the in-tree build.
+LIB_PATH = os.environ.get("GPV_LIB") or os.path.join(HERE, "libgpv_b200.so")
 
 # Record layouts of include/gpv.h
 DESC_DTYPE = np.dtype([("coord", "<f8", (2,)), ("p0", "<f8", (12,)), ("order", "<i4"), ("radius", "<i4")])

@@ -202,3 +202,27 @@ def test_autotune_choices_do_not_change_results(oracle, gpv_mod):
     assert np.array_equal(res["128"]["iterations"], res["256"]["iterations"]) or \
         (res["128"]["iterations"] != res["256"]["iterations"]).mean() < 0.02
     assert np.abs(res["128"]["p"] - res["256"]["p"]).max() < 1e-4
+
+
+@pytest.mark.parametrize("layout", ["rows", "tiles"])
+def test_template_layouts_match_the_oracle(gpv_mod, oracle, layout, monkeypatch):
+    """The padded-row and 8 x 4 tile slot layouts of the tiled kernel (chosen
+    with GPV_TILE_LAYOUT) solve every subset like the compact one."""
+    from gpv import synth
+    W = synth.workload(3, scale_down=8)
+    d = gpv_mod.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
+    F = gpv_mod.Image(image_gs=W["f"], border=20)
+    G = gpv_mod.Image(image_gs=W["g"], border=20)
+    base = gpv_mod.solve_batch(F, G, d)
+    monkeypatch.setenv("GPV_TILE_LAYOUT", layout)
+    got = gpv_mod.solve_batch(F, G, d)
+    monkeypatch.delenv("GPV_TILE_LAYOUT")
+    Cf = oracle.get_c(W["f"].astype(np.float64), 20)
+    Cg = oracle.get_c(W["g"].astype(np.float64), 20)
+    ref = oracle.solve_batch(Cf, Cg, W["f"].shape, 20, d)
+    for a in (base, got):
+        assert np.array_equal(a["status"], ref["status"]) and np.array_equal(a["converged"], ref["converged"])
+        ok = a["status"] == 0
+        assert np.abs(a["p"][ok, :2] - ref["p"][ok, :2]).max() <= 1e-3
+        assert np.abs(a["p"][ok, 2:6] - ref["p"][ok, 2:6]).max() <= 1e-5
+    assert np.array_equal(got["n_px"], base["n_px"])
