@@ -293,6 +293,79 @@ int gpv_image_update(gpv_image *img, const void *px, int32_t dtype) {
     return GPV_SUCCESS;
 }
 
+// ---- colour ingest -----------------------------------------------------------
+
+// RGB8 at rgb_dev -> grey u8 in the image's pixel staging -> coefficients.
+static int image_from_rgb_dev(gpv_image *img, const uint8_t *rgb_dev) {
+    gpv_context *ctx = img->ctx;
+    const size_t bytes = (size_t)img->h * (size_t)img->w;
+    if (bytes > img->px_bytes) {
+        cudaFree(img->px_dev);
+        img->px_dev = nullptr;
+        img->px_bytes = 0;
+        GPV_CUDA_TRY(cudaMalloc(&img->px_dev, bytes));
+        img->px_bytes = bytes;
+    }
+    if (int rc = ingest_launch(rgb_dev, img->h, img->w, static_cast<uint8_t *>(img->px_dev), ctx->stream)) return rc;
+    return prefilter_launch(img, img->px_dev, GPV_U8, ctx->stream);
+}
+
+static int stage_rgb(gpv_image *img, const uint8_t *rgb) {
+    gpv_context *ctx = img->ctx;
+    if (!img->rgb_dev) GPV_CUDA_TRY(cudaMalloc(&img->rgb_dev, (size_t)img->h * (size_t)img->w * 3));
+    GPV_CUDA_TRY(cudaMemcpyAsync(img->rgb_dev, rgb, (size_t)img->h * (size_t)img->w * 3, cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    return GPV_SUCCESS;
+}
+
+int gpv_image_create_rgb8(gpv_context *ctx, const uint8_t *rgb, int64_t h, int64_t w, int32_t border, uint32_t flags,
+                          gpv_image **out) {
+    if (!rgb || !ctx || !out) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    if (h < 3 || w < 3) { set_error("colour ingest needs an image of at least 3 x 3 pixels"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(ctx->device);
+    int rc = image_alloc(ctx, h, w, border, flags, GPV_U8, out);
+    if (rc) return rc;
+    gpv_image *img = *out;
+    rc = stage_rgb(img, rgb);
+    if (!rc) rc = image_from_rgb_dev(img, img->rgb_dev);
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) { set_error(std::string("ingest: ") + cudaGetErrorString(e)); rc = GPV_ERR_CUDA; }
+    }
+    if (rc) { gpv_image_destroy(img); *out = nullptr; }
+    return rc;
+}
+
+int gpv_image_update_rgb8(gpv_image *img, const uint8_t *rgb) {
+    if (!img || !rgb) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    if (img->h < 3 || img->w < 3) { set_error("colour ingest needs an image of at least 3 x 3 pixels"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(img->ctx->device);
+    if (int rc = stage_rgb(img, rgb)) return rc;
+    if (int rc = image_from_rgb_dev(img, img->rgb_dev)) return rc;
+    GPV_CUDA_TRY(cudaStreamSynchronize(img->ctx->stream));
+    return GPV_SUCCESS;
+}
+
+int gpv_image_update_rgb8_device(gpv_image *img, const uint8_t *rgb_dev) {
+    if (!img || !rgb_dev) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    if (img->h < 3 || img->w < 3) { set_error("colour ingest needs an image of at least 3 x 3 pixels"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(img->ctx->device);
+    return image_from_rgb_dev(img, rgb_dev);
+}
+
+int gpv_image_grey(const gpv_image *img, uint8_t *out) {
+    if (!img || !out) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    if (!img->px_dev || img->px_bytes < (size_t)img->h * (size_t)img->w) {
+        set_error("the image holds no staged pixels");
+        return GPV_ERR_INVALID;
+    }
+    DeviceGuard dg(img->ctx->device);
+    GPV_CUDA_TRY(cudaMemcpyAsync(out, img->px_dev, (size_t)img->h * (size_t)img->w, cudaMemcpyDeviceToHost,
+                                 img->ctx->stream));
+    GPV_CUDA_TRY(cudaStreamSynchronize(img->ctx->stream));
+    return GPV_SUCCESS;
+}
+
 int gpv_image_destroy(gpv_image *img) {
     if (!img) return GPV_SUCCESS;
     DeviceGuard dg(img->ctx->device);
@@ -301,6 +374,7 @@ int gpv_image_destroy(gpv_image *img) {
     cudaFree(img->c64);
     cudaFree(img->rowpass);
     cudaFree(img->px_dev);
+    cudaFree(img->rgb_dev);
     gpv_context *ctx = img->ctx;
     delete img;
     context_release(ctx);

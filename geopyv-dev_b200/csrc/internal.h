@@ -98,6 +98,7 @@ struct gpv_image {
     double *rowpass = nullptr;  // FP64 row-pass intermediate (h, cw)
     void *px_dev = nullptr;     // staging for host pixels
     size_t px_bytes = 0;
+    uint8_t *rgb_dev = nullptr;  // staging for colour pixels (h * w * 3)
     uint32_t flags = 0;
 };
 
@@ -133,6 +134,8 @@ int mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements, in
                gpv_subset_result *out, int32_t *rounds, gpv_mesh_stats *stats);
 // The (order, radius class) segments of the tiled solve that a host batch
 // holds (bit q = segment q); lets the launcher skip empty segments.
+// Colour ingest (load_grayscale + gaussian_blur_5x5): RGB8 (h, w, 3) -> u8 grey.
+int ingest_launch(const uint8_t *rgb_dev, int64_t h, int64_t w, uint8_t *grey_dev, cudaStream_t s);
 uint32_t tile_segment_mask(const gpv_subset_desc *desc, int64_t n, int max_radius);
 int solve_noalloc_launch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
                          int64_t n, int max_radius, const gpv_solve_params *prm, gpv_subset_result *out_dev,

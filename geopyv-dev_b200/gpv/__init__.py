@@ -75,31 +75,71 @@ class Image:
     coefficients are computed on the GPU: Image::from_array -> get_c,
     src/image.rs:83-86, :252-327).  ``keep_f64`` keeps an FP64 copy of the
     coefficients for the FP64 solver.
+
+    ``Image(image_rgb=array)`` takes decoded 8-bit colour pixels (h, w, 3) in
+    RGB order and applies Image::from_file's pre-processing on the device
+    (grey level, 5 x 5 Gaussian blur, rounding: src/image.rs:450-534) before
+    the prefilter.  ``Image(filepath=...)`` decodes the file with OpenCV when
+    it is installed and then does the same; lossless formats decode to the
+    same pixels as the reference's decoder, lossy ones (JPEG) may differ by a
+    grey level where the two decoders' inverse DCTs round differently.
     """
 
-    def __init__(self, filepath=None, image_gs=None, border: int = 20, keep_f64: bool = False, ctx: Context | None = None):
-        if filepath is not None and image_gs is not None:
-            raise ValueError("supply exactly one of `filepath` or `image_gs`, not both")
+    def __init__(self, filepath=None, image_gs=None, border: int = 20, keep_f64: bool = False, ctx: Context | None = None,
+                 image_rgb=None):
+        given = [v is not None for v in (filepath, image_gs, image_rgb)]
+        if sum(given) > 1:
+            raise ValueError("supply exactly one of `filepath`, `image_gs` or `image_rgb`")
+        if not any(given):
+            raise ValueError("one of `filepath`, `image_gs` or `image_rgb` is required")
         if filepath is not None:
-            raise NotImplementedError("loading image files is not part of this library; pass image_gs")
-        if image_gs is None:
-            raise ValueError("one of `filepath` or `image_gs` is required")
-        arr = np.asarray(image_gs)
-        if arr.ndim != 2:
-            raise ValueError("image_gs must be 2-D")
-        if arr.dtype not in _lib.DTYPES:
-            arr = arr.astype(np.float64)
-        arr = np.ascontiguousarray(arr)
+            try:
+                import cv2
+            except ImportError as e:  # pragma: no cover - depends on the installation
+                raise NotImplementedError("decoding image files needs OpenCV; pass image_gs or image_rgb") from e
+            bgr = cv2.imread(str(filepath), cv2.IMREAD_COLOR)
+            if bgr is None:
+                raise RuntimeError(f"image load error: cannot read {filepath}")
+            image_rgb = np.ascontiguousarray(bgr[:, :, ::-1])
         self.ctx = ctx or default_context()
-        self.shape = arr.shape
         self.border = border
-        self.dtype = arr.dtype
         h = ct.c_void_p()
         flags = _lib.IMAGE_KEEP_F64 if keep_f64 else 0
-        check(lib().gpv_image_create(self.ctx.handle, ptr(arr), _lib.DTYPES[arr.dtype], arr.shape[0], arr.shape[1],
-                                     border, flags, ct.byref(h)), "gpv_image_create")
+        if image_rgb is not None:
+            rgb = np.ascontiguousarray(image_rgb, dtype=np.uint8)
+            if rgb.ndim != 3 or rgb.shape[2] != 3:
+                raise ValueError("image_rgb must be (h, w, 3) uint8")
+            self.shape = rgb.shape[:2]
+            self.dtype = np.dtype(np.uint8)
+            check(lib().gpv_image_create_rgb8(self.ctx.handle, ptr(rgb), rgb.shape[0], rgb.shape[1], border, flags,
+                                              ct.byref(h)), "gpv_image_create_rgb8")
+        else:
+            arr = np.asarray(image_gs)
+            if arr.ndim != 2:
+                raise ValueError("image_gs must be 2-D")
+            if arr.dtype not in _lib.DTYPES:
+                arr = arr.astype(np.float64)
+            arr = np.ascontiguousarray(arr)
+            self.shape = arr.shape
+            self.dtype = arr.dtype
+            check(lib().gpv_image_create(self.ctx.handle, ptr(arr), _lib.DTYPES[arr.dtype], arr.shape[0], arr.shape[1],
+                                         border, flags, ct.byref(h)), "gpv_image_create")
         self._h = h
         self.keep_f64 = keep_f64
+
+    @property
+    def image_gs(self) -> np.ndarray:
+        """The greyscale pixels of an image built from colour pixels (float64, as the reference's image_gs)."""
+        out = np.empty(self.shape, np.uint8)
+        check(lib().gpv_image_grey(self._h, ptr(out)), "gpv_image_grey")
+        return out.astype(np.float64)
+
+    def update_rgb(self, image_rgb) -> None:
+        """Ingest and prefilter new colour pixels of the same shape in place."""
+        rgb = np.ascontiguousarray(image_rgb, dtype=np.uint8)
+        if rgb.shape != (*self.shape, 3):
+            raise ValueError(f"shape {rgb.shape} != {(*self.shape, 3)}")
+        check(lib().gpv_image_update_rgb8(self._h, ptr(rgb)), "gpv_image_update_rgb8")
 
     @property
     def handle(self):

@@ -109,6 +109,10 @@ SIGNATURES = {
     "gpv_image_coefficients_f32": (ct.c_int, [P, P]),
     "gpv_image_coefficients_f64": (ct.c_int, [P, P]),
     "gpv_image_eval": (ct.c_int, [P, P, I64, I32, P, P]),
+    "gpv_image_create_rgb8": (ct.c_int, [P, P, I64, I64, I32, U32, P]),
+    "gpv_image_update_rgb8": (ct.c_int, [P, P]),
+    "gpv_image_update_rgb8_device": (ct.c_int, [P, P]),
+    "gpv_image_grey": (ct.c_int, [P, P]),
     "gpv_mask_create": (ct.c_int, [P, P, I64, I64, P]),
     "gpv_mask_destroy": (ct.c_int, [P]),
     "gpv_solve_batch": (ct.c_int, [P, P, P, P, I64, P, P]),

@@ -148,6 +148,21 @@ int gpv_image_coefficients_f64(const gpv_image *img, double *out);
 int gpv_image_eval(const gpv_image *img, const double *xy, int64_t n, int32_t precision, double *val,
                    double *grad);
 
+/* ---- colour ingest: Image::from_file's pre-processing --------------------
+ * load_grayscale + gaussian_blur_5x5 (src/image.rs:450-534) on the device,
+ * for decoded 8-bit RGB pixels (h, w, 3) row-major (file decoding itself is
+ * not part of this library): the integer grey level
+ * (2126 R + 7152 G + 722 B + 5000) / 10000, a 5 x 5 Gaussian blur
+ * (sigma 1.1, BORDER_REFLECT_101), rounding and clamping to 0..255 -- bit for
+ * bit the reference's grey image -- then the prefilter.  h, w >= 3. */
+int gpv_image_create_rgb8(gpv_context *ctx, const uint8_t *rgb, int64_t h, int64_t w, int32_t border, uint32_t flags,
+                          gpv_image **out);
+int gpv_image_update_rgb8(gpv_image *img, const uint8_t *rgb);
+/* Same from device pixels, asynchronous on the context stream. */
+int gpv_image_update_rgb8_device(gpv_image *img, const uint8_t *rgb_dev);
+/* The 8-bit greyscale pixels an RGB8 image was built from (h * w bytes). */
+int gpv_image_grey(const gpv_image *img, uint8_t *out);
+
 /* ---- global mask: LocalMask::mask_update (src/masks.rs:199-263) --------- */
 int gpv_mask_create(gpv_context *ctx, const uint8_t *mask, int64_t h, int64_t w, gpv_mask **out);
 int gpv_mask_destroy(gpv_mask *m);

@@ -817,6 +817,41 @@ static void solve_one_fagn(const spline *F, const spline *G, const gpvo_desc *d,
     free(sdi); free(g); free(gc); free(gg); subset_free(&s);
 }
 
+/* load_grayscale + gaussian_blur_5x5 (src/image.rs:450-534) on decoded RGB8
+ * pixels: integer grey level, 5-tap Gaussian (sigma 1.1) horizontal then
+ * vertical with BORDER_REFLECT_101 indices, FP64 left-to-right sums, rounding
+ * half away from zero, clamp to 0..255.  h, w >= 3. */
+static int64_t reflect101(int64_t i, int64_t n) { return i < 0 ? -i : (i >= n ? 2 * (n - 1) - i : i); }
+
+void gpvo_ingest_rgb8(const uint8_t *rgb, int64_t h, int64_t w, uint8_t *out) {
+    double raw[5], k[5], sum = 0.0;
+    for (int i = 0; i < 5; i++) {
+        double x = (double)i - 2.0;
+        raw[i] = exp(-x * x / (2.0 * 1.1 * 1.1));
+    }
+    for (int i = 0; i < 5; i++) sum += raw[i];
+    for (int i = 0; i < 5; i++) k[i] = raw[i] / sum;
+    double *gs = (double *)malloc(sizeof(double) * h * w), *hp = (double *)malloc(sizeof(double) * h * w);
+    for (int64_t i = 0; i < h * w; i++) {
+        const uint8_t *p = rgb + 3 * i;
+        gs[i] = (double)((2126u * p[0] + 7152u * p[1] + 722u * p[2] + 5000u) / 10000u);
+    }
+    for (int64_t i = 0; i < h; i++)
+        for (int64_t j = 0; j < w; j++) {
+            double v = 0.0;
+            for (int q = 0; q < 5; q++) v += k[q] * gs[i * w + reflect101(j + q - 2, w)];
+            hp[i * w + j] = v;
+        }
+    for (int64_t i = 0; i < h; i++)
+        for (int64_t j = 0; j < w; j++) {
+            double v = 0.0;
+            for (int q = 0; q < 5; q++) v += k[q] * hp[reflect101(i + q - 2, h) * w + j];
+            v = round(v);
+            out[i * w + j] = (uint8_t)(v < 0.0 ? 0.0 : (v > 255.0 ? 255.0 : v));
+        }
+    free(gs); free(hp);
+}
+
 /* Batch entry: nthreads OpenMP workers, one subset per task (dynamic). */
 void gpvo_solve_batch(const double *cf, const double *cg, int64_t h, int64_t w, int64_t border,
                       const gpvo_desc *desc, int64_t n, const gpvo_params *prm, const uint8_t *mask,

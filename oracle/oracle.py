@@ -68,6 +68,7 @@ def lib():
         L.gpvo_eta.argtypes = [P, i32, P, P, P, dbl, dbl, P, dbl, dbl, i64, P, P]
         L.gpvo_eta.restype = i32
         L.gpvo_solve_batch.argtypes = [P, P, i64, i64, i64, P, i64, P, P, P, P, i32]
+        L.gpvo_ingest_rgb8.argtypes = [P, i64, i64, P]
         L.gpvo_subset_setup.argtypes = [P, i64, i64, i64, P, i64, P, P, P, P, P]
         L.gpvo_subset_setup.restype = i32
         L.gpvo_max_threads.restype = i32
@@ -226,3 +227,11 @@ def solve_batch(coef_f, coef_g, shape, border, desc, max_norm=1e-5, max_iteratio
     lib().gpvo_solve_batch(_p(_f8(coef_f)), _p(_f8(coef_g)), shape[0], shape[1], border, _p(desc), desc.size,
                            _p(prm), _p(m), _p(out), _p(hist), nthreads or lib().gpvo_max_threads())
     return (out, hist) if history else out
+
+
+def ingest_rgb8(rgb):
+    """load_grayscale + gaussian_blur_5x5 (src/image.rs:450-534): (h, w, 3) uint8 -> (h, w) uint8."""
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    out = np.empty(rgb.shape[:2], np.uint8)
+    lib().gpvo_ingest_rgb8(_p(rgb), rgb.shape[0], rgb.shape[1], _p(out))
+    return out
