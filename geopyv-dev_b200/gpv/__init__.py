@@ -17,7 +17,7 @@ from . import _lib
 from ._lib import (DESC_DTYPE, RESULT_DTYPE, PREC_FP64, PREC_MIXED, SOLVE_ETA, STATUS, GpvError, SolveParams,
                    check, lib, ptr)
 
-__all__ = ["Context", "Image", "Mask", "Subset", "Mesh", "mesh_drive", "SubsetSequence", "Server", "solve_batch", "autotune", "make_desc", "DESC_DTYPE", "RESULT_DTYPE",
+__all__ = ["Context", "Image", "Mask", "Subset", "Mesh", "mesh_drive", "SubsetSequence", "Sequence", "Server", "solve_batch", "autotune", "make_desc", "DESC_DTYPE", "RESULT_DTYPE",
            "GpvError", "PREC_MIXED", "PREC_FP64", "STATUS", "version"]
 
 
@@ -376,6 +376,8 @@ class Subset:
 
 from .mesh import Cancelled, Mesh, mesh_drive  # noqa: E402  (uses the classes above only through arguments)
 from .server import Server, Ticket  # noqa: E402
+from . import sequence  # noqa: E402
+from .sequence import Sequence  # noqa: E402
 
 
 class SubsetSequence:
