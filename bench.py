@@ -64,6 +64,15 @@ def parse():
 
 
 # ---------------------------------------------------------------------------
+def _backend():
+    """NCCL on GPUs; gloo when GPV_BENCH_BACKEND=gloo or no GPU is visible
+    (the CPU tests of the multi-rank path)."""
+    import torch
+    if os.environ.get("GPV_BENCH_BACKEND") == "gloo" or not torch.cuda.is_available():
+        return "gloo"
+    return "nccl"
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -73,9 +82,12 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        if _backend() == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
     return world, rank, local
 
 
@@ -86,13 +98,22 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The largest of the ranks' values (device timing: the slowest rank)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if _backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(units_per_rank, steps, t_ms_local, world):
+    """Whole-job throughput of replicas: every rank's units over the slowest
+    rank's timed region."""
+    t_max = max_over_ranks(t_ms_local, world)
+    return world * units_per_rank * steps / (t_max * 1e-3), t_max
 
 
 class ClockSampler:
@@ -244,7 +265,7 @@ def cpu_baseline(W, args, nthreads=None, seconds=None, rng_seed=7):
     O.solve_batch(Cf, Cg, W["f"].shape, 20, d[perm[:k]], max_norm=1e-5, max_iterations=50, nthreads=nthreads)
     per = (time.perf_counter() - t0) / k
     s = int(min(n - k, max(64, seconds / max(per, 1e-9))))
-    sample = perm[k:k + s]
+    sample = perm[k:k + s] if s > 0 else perm[:k]  # a small batch: time it whole
     t0 = time.perf_counter()
     ref = O.solve_batch(Cf, Cg, W["f"].shape, 20, d[sample], max_norm=1e-5, max_iterations=50, nthreads=nthreads)
     t_solve = time.perf_counter() - t0
@@ -578,8 +599,7 @@ def run_ours(args, world, rank, local):
     barrier(world)
     t_ms = e0.elapsed_time(e1)
     solve_ms = [a.elapsed_time(b) for a, b in solve_ev]
-    t_max = max_over_ranks(t_ms, world)
-    value = world * n * args.steps / (t_max * 1e-3)
+    value, t_max = replica_rate(n, args.steps, t_ms, world)
 
     # ---- e2e through the host C ABI (pinned host buffers) ----
     f_pin = torch.from_numpy(W["f"].view(np.uint8 if px_dtype == np.uint8 else np.int16).copy()).pin_memory()
