@@ -576,6 +576,7 @@ def run_ours(args, world, rank, local):
     tuned = [0, 0, 0]
     if prec == gpv.PREC_MIXED and not os.environ.get("GPV_TILE_THREADS"):
         tuned = gpv.autotune(F, G, desc, sample_per_class=2048)
+    layouts = [lay for _, lay in ctx.tuning()]
     peak_buf = ct.c_double(0.0)
     _lib.check(L.gpv_probe_fp32_peak(ctx.handle, ct.byref(peak_buf)), "probe")
     fp32_peak = peak_buf.value
@@ -688,7 +689,8 @@ def run_ours(args, world, rank, local):
                           f": 2 x {h + 40}x{w + 40} FP32 coefficients + FP64 row passes ({l2_bytes / 1e6:.0f} MB)"
                           " rewritten each step"),
                    "parallelism": f"replicas x{world}",
-                   "tuned_threads_per_subset": {"r<=20": tuned[0], "r21-40": tuned[1], "r>40": tuned[2]}},
+                   "tuned_threads_per_subset": {"r<=20": tuned[0], "r21-40": tuned[1], "r>40": tuned[2]},
+                   "tuned_layout": {"r<=20": layouts[0], "r21-40": layouts[1], "r>40": layouts[2]}},
         "solve_ms": solve_avg_ms, "prefilter_ms": t_max / args.steps - solve_avg_ms,
         "samples_per_s": world * samples * args.steps / (t_max * 1e-3),
         "iterations_mean": float(np.mean(res["iterations"])),

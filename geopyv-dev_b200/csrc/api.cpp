@@ -672,10 +672,12 @@ static void tune_cache_load(gpv_context *ctx) {
     char line[512];
     while (fgets(line, sizeof line, fh)) {
         char name[256];
-        int cls = -1, nt = 0;
-        if (sscanf(line, "%255[^|]|%d|%d", name, &cls, &nt) == 3 && cls >= 0 && cls < 3 &&
-            strcmp(name, prop.name) == 0 && (nt == 128 || nt == 256))
+        int cls = -1, nt = 0, layout = -1;
+        const int got = sscanf(line, "%255[^|]|%d|%d|%d", name, &cls, &nt, &layout);
+        if (got >= 3 && cls >= 0 && cls < 3 && strcmp(name, prop.name) == 0 && (nt == 128 || nt == 256)) {
             ctx->tuned_threads[cls] = nt;  // later lines win
+            ctx->tuned_layout[cls] = (got == 4 && layout >= 0 && layout <= 2) ? layout : -1;
+        }
     }
     fclose(fh);
 }
@@ -694,7 +696,8 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
     p.precision = GPV_PREC_MIXED;
     p.history = nullptr;
     p.flags &= ~(GPV_SOLVE_ETA | GPV_SOLVE_FAGN);  // the tuned kernel is the mixed ICGN one
-    static const int cand[2] = {128, 256};
+    // candidates: threads per block x template layout (compact, 8 x 4 tiles)
+    static const int cand[4][2] = {{128, 0}, {256, 0}, {128, 2}, {256, 2}};
     for (int c = 0; c < 3; c++) {
         if (threads_out) threads_out[c] = 0;
         if (cls[c].empty()) continue;
@@ -704,9 +707,11 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
         for (size_t j = 0; j < k; j++) smp.push_back(cls[c][j * cls[c].size() / k]);
         std::vector<gpv_subset_result> out(smp.size());
         double best = 1e300;
-        int best_nt = 128;
-        for (int t : cand) {
+        int best_nt = 128, best_layout = 0;
+        for (const auto &cd : cand) {
+            const int t = cd[0];
             ctx->force_threads = t;
+            ctx->force_layout = cd[1];
             double ms_best = 1e300;
             for (int rep = 0; rep < 3; rep++) {
                 cudaEvent_t e0, e1;
@@ -720,23 +725,35 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
                 cudaEventElapsedTime(&ms, e0, e1);
                 cudaEventDestroy(e0);
                 cudaEventDestroy(e1);
-                if (rc) { ctx->force_threads = 0; return rc; }
+                if (rc) { ctx->force_threads = 0; ctx->force_layout = -1; return rc; }
                 if (rep > 0) ms_best = std::min(ms_best, (double)ms);
             }
-            if (ms_best < best) { best = ms_best; best_nt = t; }
+            if (ms_best < best) { best = ms_best; best_nt = t; best_layout = cd[1]; }
         }
         ctx->force_threads = 0;
+        ctx->force_layout = -1;
         ctx->tuned_threads[c] = best_nt;
+        ctx->tuned_layout[c] = best_layout;
         if (threads_out) threads_out[c] = best_nt;
         if (const char *path = getenv("GPV_TUNE_CACHE")) {
             cudaDeviceProp prop;
             if (cudaGetDeviceProperties(&prop, ctx->device) == cudaSuccess) {
                 if (FILE *fh = fopen(path, "a")) {
-                    fprintf(fh, "%s|%d|%d\n", prop.name, c, best_nt);
+                    fprintf(fh, "%s|%d|%d|%d\n", prop.name, c, best_nt, best_layout);
                     fclose(fh);
                 }
             }
         }
+    }
+    return GPV_SUCCESS;
+}
+
+int gpv_context_tuning(gpv_context *ctx, int32_t *threads, int32_t *layouts) {
+    if (!ctx) { set_error("ctx is NULL"); return GPV_ERR_INVALID; }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    for (int c = 0; c < 3; c++) {
+        if (threads) threads[c] = ctx->tuned_threads[c];
+        if (layouts) layouts[c] = ctx->tuned_layout[c];
     }
     return GPV_SUCCESS;
 }

@@ -833,13 +833,8 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
     count_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, K.max_radius, cnt);
     scatter_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, K.max_radius, cnt, fill, order_out, seg, K.out);
     GPV_CUDA_TRY(cudaGetLastError());
-    // GPV_TILE_LAYOUT = compact (default) | rows | tiles; the compact layout
-    // measured fastest: the other two remove most bank conflicts but add
-    // empty slots, and the kernel is latency- rather than bank-bound
-    const char *lay = getenv("GPV_TILE_LAYOUT");
-    const int layout = !lay ? kLayoutCompact : (lay[0] == 'r' ? kLayoutRows : (lay[0] == 't' ? kLayoutTiles : kLayoutCompact));
     struct Plan {
-        int rmax = 0, nt = 0, cap = 0, blocks = 0;
+        int rmax = 0, nt = 0, layout = 0, cap = 0, blocks = 0;
         int64_t stride = 0;
         bool live = false;
     };
@@ -853,7 +848,8 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         if (!P.live) continue;
         P.rmax = std::min(kRBoundHost[c], K.max_radius);
         P.nt = tile_threads_for(ctx, P.rmax);
-        P.cap = window_cap(P.rmax, layout);
+        P.layout = tile_layout_for(ctx, P.rmax);
+        P.cap = window_cap(P.rmax, P.layout);
         const size_t smem = sizeof(float) * P.cap;
         const void *fn = P.nt == 256 ? tile_kernel<256>(order) : tile_kernel<128>(order);
         if (int rc = allow_max_dynamic_smem(fn)) return rc;
@@ -884,7 +880,7 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         T.k.order = order_out;
         T.k.max_radius = P.rmax;
         T.win_cap = P.cap;
-        T.layout = layout;
+        T.layout = P.layout;
         T.seg = seg + 2 * q;
         T.queue = queues + q;
         T.k.scratch = static_cast<float *>(ctx->scratch.ptr) + (int64_t)k * region;
@@ -900,6 +896,18 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         GPV_CUDA_TRY(cudaStreamWaitEvent(s, ctx->ev[k], 0));
     }
     return GPV_SUCCESS;
+}
+
+// GPV_TILE_LAYOUT = compact | rows | tiles overrides; the default compact
+// layout measured fastest on the second-order workload: the other two remove
+// most bank conflicts but add empty slots (the autotuner may still pick them
+// for a radius class).
+int tile_layout_for(gpv_context *ctx, int max_radius) {
+    if (const char *lay = getenv("GPV_TILE_LAYOUT"))
+        return lay[0] == 'r' ? kLayoutRows : (lay[0] == 't' ? kLayoutTiles : kLayoutCompact);
+    if (ctx->force_layout >= 0) return ctx->force_layout;
+    const int cls = max_radius <= 20 ? 0 : (max_radius <= 40 ? 1 : 2);
+    return ctx->tuned_layout[cls] >= 0 ? ctx->tuned_layout[cls] : kLayoutCompact;
 }
 
 int tile_threads_for(gpv_context *ctx, int max_radius) {

@@ -81,6 +81,8 @@ struct gpv_context {
     int mixed_blocks_per_sm = 0;
     int tuned_threads[3] = {0, 0, 0};  // autotuned threads per block by radius class
     int force_threads = 0;             // set while the autotuner times a candidate
+    int tuned_layout[3] = {-1, -1, -1};  // autotuned template layout by radius class (-1: compact)
+    int force_layout = -1;               // set while the autotuner times a candidate
     uint32_t seg_mask = 0xFFFFFFFFu;   // tiled-solve segments a host batch holds (all when unknown)
     // owner reference + one per image / mask created on it: the context is
     // freed when gpv_context_destroy and every dependant's destroy have run,
@@ -136,6 +138,11 @@ int mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements, in
 // holds (bit q = segment q); lets the launcher skip empty segments.
 // Colour ingest (load_grayscale + gaussian_blur_5x5): RGB8 (h, w, 3) -> u8 grey.
 int ingest_launch(const uint8_t *rgb_dev, int64_t h, int64_t w, uint8_t *grey_dev, cudaStream_t s);
+// Threads per block / template layout (0 compact, 1 padded rows, 2 tiles) of
+// the tiled solve for subsets up to max_radius: GPV_TILE_THREADS /
+// GPV_TILE_LAYOUT, else a candidate being timed, else the tuned choice.
+int tile_threads_for(gpv_context *ctx, int max_radius);
+int tile_layout_for(gpv_context *ctx, int max_radius);
 uint32_t tile_segment_mask(const gpv_subset_desc *desc, int64_t n, int max_radius);
 int solve_noalloc_launch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
                          int64_t n, int max_radius, const gpv_solve_params *prm, gpv_subset_result *out_dev,

@@ -119,6 +119,7 @@ SIGNATURES = {
     "gpv_solve_batch_device": (ct.c_int, [P, P, P, P, P, I64, P, P, P]),
     "gpv_probe_fp32_peak": (ct.c_int, [P, P]),
     "gpv_autotune": (ct.c_int, [P, P, P, P, I64, P, I32, P]),
+    "gpv_context_tuning": (ct.c_int, [P, P, P]),
     "gpv_solve_batch_noalloc": (ct.c_int, [P, P, P, P, I64, I32, P, P, P]),
     "gpv_mesh_solve": (ct.c_int, [P, P, P, P, I64, P, I64, I32, P, P, P, P]),
     "gpv_sequence_create": (ct.c_int, [P, P, P, P, I64, P, I32, U32, P]),

@@ -368,14 +368,18 @@ int gpv_server_destroy(gpv_server *s);
 
 /* ---- autotuning (no counterpart in the reference) ------------------------
  * Times the candidate launch shapes of the mixed-precision kernel (threads
- * per subset block) on a sample of up to sample_per_class subsets of each
- * radius class (r <= 20, 21..40, > 40) present in desc, keeps the fastest per
- * class in the context, and returns the choices in threads_out[3] (0 = class
+ * per subset block: 128 or 256; template layout: compact scan order or 8 x 4
+ * tiles) on a sample of up to sample_per_class subsets of each radius class
+ * (r <= 20, 21..40, > 40) present in desc, keeps the fastest per class in the
+ * context, and returns the thread choices in threads_out[3] (0 = class
  * absent).  If the environment variable GPV_TUNE_CACHE names a file, the
  * choices are appended to it keyed by device name, and gpv_context_create
  * reads them back. */
 int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc, int64_t n,
                  const gpv_solve_params *params, int32_t sample_per_class, int32_t *threads_out);
+/* The context's tuned choices per radius class: threads (0 = none) and
+ * layout (-1 = none, 0 compact, 1 padded rows, 2 tiles); either may be NULL. */
+int gpv_context_tuning(gpv_context *ctx, int32_t *threads, int32_t *layouts);
 
 /* ---- calibration (no counterpart in the reference) ----------------------
  * Measured FP32 FMA throughput of this device (TFLOP/s, 2 FLOP per FMA) from

@@ -188,6 +188,10 @@ def test_autotune_choices_do_not_change_results(oracle, gpv_mod):
     present = {0: np.any(d["radius"] <= 20), 1: np.any((d["radius"] > 20) & (d["radius"] <= 40)), 2: np.any(d["radius"] > 40)}
     for c in range(3):
         assert tuned[c] in ((128, 256) if present[c] else (0,))
+    choice = F.ctx.tuning()
+    for c in range(3):
+        if present[c]:  # an absent class keeps whatever the shared context held
+            assert choice[c][0] == tuned[c] and choice[c][1] in ("compact", "tiles")
     import os
     res = {}
     for nt in ("128", "256"):
@@ -226,3 +230,19 @@ def test_template_layouts_match_the_oracle(gpv_mod, oracle, layout, monkeypatch)
         assert np.abs(a["p"][ok, :2] - ref["p"][ok, :2]).max() <= 1e-3
         assert np.abs(a["p"][ok, 2:6] - ref["p"][ok, 2:6]).max() <= 1e-5
     assert np.array_equal(got["n_px"], base["n_px"])
+
+
+def test_tune_cache_file_is_read_back(gpv_mod, tmp_path, monkeypatch):
+    """A context reads GPV_TUNE_CACHE lines for its device: "name|class|threads"
+    (layout unset) and "name|class|threads|layout"; later lines win, other
+    devices' lines and malformed ones are ignored."""
+    import torch
+    name = torch.cuda.get_device_name(0)
+    cache = tmp_path / "tune.txt"
+    cache.write_text(f"{name}|0|128\nOther GPU|1|128|0\n{name}|1|128|0\n{name}|1|256|2\n{name}|2|999|0\n")
+    monkeypatch.setenv("GPV_TUNE_CACHE", str(cache))
+    ctx = gpv_mod.Context(0)
+    try:
+        assert ctx.tuning() == [(128, None), (256, "tiles"), (None, None)]
+    finally:
+        ctx.close()
