@@ -40,6 +40,34 @@ void DevBuf::release() {
     bytes = 0;
 }
 
+int HostBuf::ensure(size_t want) {
+    if (want <= bytes && ptr) return GPV_SUCCESS;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    const size_t sz = want < 4096 ? 4096 : want;
+    cudaError_t e = cudaHostAlloc(&ptr, sz, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        set_error(std::string("cudaHostAlloc(") + std::to_string(sz) + "): " + cudaGetErrorString(e));
+        return GPV_ERR_NOMEM;
+    }
+    bytes = sz;
+    return GPV_SUCCESS;
+}
+
+void HostBuf::release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+// Layout of the pinned staging of a host batch of n subsets: descriptors,
+// work order, results, each at a 256-byte boundary.
+static size_t stage_off_order(int64_t n) { return (sizeof(gpv_subset_desc) * (size_t)n + 255) / 256 * 256; }
+static size_t stage_off_out(int64_t n) { return stage_off_order(n) + (sizeof(int32_t) * (size_t)n + 255) / 256 * 256; }
+static size_t stage_bytes(int64_t n) { return stage_off_out(n) + sizeof(gpv_subset_result) * (size_t)n; }
+
 struct short2_h {
     int16_t x, y;
 };
@@ -136,6 +164,7 @@ using namespace gpv;
 extern "C" {
 
 static void tune_cache_load(gpv_context *ctx);
+static void context_release(gpv_context *ctx);
 
 const char *gpv_version(void) { return "gpv-b200 0.1.0 (sm_100a)"; }
 
@@ -151,23 +180,47 @@ size_t gpv_last_error(char *buf, size_t len) {
     return e.size();
 }
 
-int gpv_context_create(int device, gpv_context **out) {
+int gpv_context_create(int device, gpv_context **out) { return gpv_context_create_ex(device, 0, out); }
+
+int gpv_context_create_ex(int device, uint32_t flags, gpv_context **out) {
     if (!out) { set_error("out is NULL"); return GPV_ERR_INVALID; }
     *out = nullptr;
+    if (flags & ~(GPV_CONTEXT_HIGH_PRIORITY | GPV_CONTEXT_PER_SUBSET_BLOCKS)) {
+        set_error("unknown context flags");
+        return GPV_ERR_INVALID;
+    }
     int ndev = 0;
     GPV_CUDA_TRY(cudaGetDeviceCount(&ndev));
     if (device < 0 || device >= ndev) { set_error("device index out of range"); return GPV_ERR_INVALID; }
     DeviceGuard dg(device);
     auto *ctx = new gpv_context();
     ctx->device = device;
+    ctx->flags = flags;
+    int least = 0, greatest = 0;
     cudaError_t e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-    for (int k = 0; k < 2 && e == cudaSuccess; k++) e = cudaStreamCreateWithFlags(&ctx->aux[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    const int prio = (flags & GPV_CONTEXT_HIGH_PRIORITY) ? greatest : least;
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) e = cudaStreamCreateWithPriority(&ctx->aux[k], cudaStreamNonBlocking, prio);
     for (int k = 0; k < 3 && e == cudaSuccess; k++) e = cudaEventCreateWithFlags(&ctx->ev[k], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         set_error(std::string("context: ") + cudaGetErrorString(e));
-        delete ctx;
+        context_release(ctx);
         return GPV_ERR_CUDA;
+    }
+    if (flags & GPV_CONTEXT_PER_SUBSET_BLOCKS) {
+        // claim words of the per-subset scratch slots: one per SM identifier
+        // for each of the three stream regions, zero whenever no solve runs
+        int rc = query_nsmid(&ctx->n_smid);
+        if (!rc) rc = ctx->slot_mask.ensure(sizeof(uint32_t) * 3 * (size_t)ctx->n_smid);
+        if (!rc && cudaMemset(ctx->slot_mask.ptr, 0, sizeof(uint32_t) * 3 * (size_t)ctx->n_smid) != cudaSuccess) {
+            set_error("context: clearing the slot words failed");
+            rc = GPV_ERR_CUDA;
+        }
+        if (rc) {
+            context_release(ctx);
+            return rc;
+        }
     }
     tune_cache_load(ctx);
     *out = ctx;
@@ -177,15 +230,16 @@ int gpv_context_create(int device, gpv_context **out) {
 static void context_release(gpv_context *ctx) {
     if (ctx->refs.fetch_sub(1) != 1) return;
     DeviceGuard dg(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->offs, &ctx->slots, &ctx->tab_off, &ctx->tab_n, &ctx->scratch, &ctx->queue, &ctx->desc_dev, &ctx->out_dev,
-                      &ctx->order_dev, &ctx->hist_dev, &ctx->eval_dev, &ctx->tile_ws})
+                      &ctx->order_dev, &ctx->hist_dev, &ctx->eval_dev, &ctx->tile_ws, &ctx->slot_mask})
         b->release();
+    ctx->h_stage.release();
     for (int k = 0; k < 2; k++)
         if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
     for (int k = 0; k < 3; k++)
         if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
-    cudaStreamDestroy(ctx->stream);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
 
@@ -480,6 +534,7 @@ int gpv_context_reserve(gpv_context *ctx, int64_t n_subsets, int32_t max_radius,
     if (int rc = ctx->out_dev.ensure(sizeof(gpv_subset_result) * (size_t)n_subsets)) return rc;
     if (int rc = ctx->order_dev.ensure(sizeof(int32_t) * (size_t)n_subsets)) return rc;
     if (int rc = ctx->tile_ws.ensure(sizeof(int32_t) * (96 + (size_t)n_subsets))) return rc;
+    if (int rc = ctx->h_stage.ensure(stage_bytes(n_subsets))) return rc;
     (void)max_iterations;
     return GPV_SUCCESS;
 }
@@ -517,9 +572,15 @@ int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, co
     for (int64_t i = 0; i < n; i++)
         if (desc[i].radius > max_r && desc[i].radius <= 4000) max_r = desc[i].radius;
     if (int rc = ensure_tables(ctx, max_r)) return rc;
+    // descriptors, work order and results pass through pinned staging
+    if (int rc = ctx->h_stage.ensure(stage_bytes(n))) return rc;
+    char *stage = static_cast<char *>(ctx->h_stage.ptr);
+    gpv_subset_desc *h_desc = reinterpret_cast<gpv_subset_desc *>(stage);
+    int32_t *order = reinterpret_cast<int32_t *>(stage + stage_off_order(n));
+    gpv_subset_result *h_out = reinterpret_cast<gpv_subset_result *>(stage + stage_off_out(n));
+    std::memcpy(h_desc, desc, sizeof(gpv_subset_desc) * (size_t)n);
     // largest subsets first (longest-processing-time order for the work queue)
     // bucket key = 3 * radius + min(order, 2): larger radius first, order 2 before 1 before 0
-    std::vector<int32_t> order(n);
     {
         const int nk = 3 * (max_r + 1);
         std::vector<int64_t> start(nk + 1, 0);
@@ -542,8 +603,8 @@ int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, co
         hist_dev = static_cast<double *>(ctx->hist_dev.ptr);
         GPV_CUDA_TRY(cudaMemsetAsync(hist_dev, 0, hist_bytes, ctx->stream));
     }
-    GPV_CUDA_TRY(cudaMemcpyAsync(ctx->desc_dev.ptr, desc, sizeof(gpv_subset_desc) * n, cudaMemcpyHostToDevice, ctx->stream));
-    GPV_CUDA_TRY(cudaMemcpyAsync(ctx->order_dev.ptr, order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    GPV_CUDA_TRY(cudaMemcpyAsync(ctx->desc_dev.ptr, h_desc, sizeof(gpv_subset_desc) * n, cudaMemcpyHostToDevice, ctx->stream));
+    GPV_CUDA_TRY(cudaMemcpyAsync(ctx->order_dev.ptr, order, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
     SolveLaunch L;
     L.f = f;
     L.g = g;
@@ -557,15 +618,19 @@ int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, co
     L.out = static_cast<gpv_subset_result *>(ctx->out_dev.ptr);
     L.history = hist_dev;
     L.max_radius = max_r;
-    ctx->seg_mask = tile_segment_mask(desc, n, max_r);  // launch only the segments this batch holds
+    // launch only the segments this batch holds, each sized by its count
+    ctx->seg_mask = tile_segment_counts(desc, n, max_r, ctx->seg_count);
+    ctx->seg_count_valid = true;
     const int rc_launch = solve_launch(ctx, L, ctx->stream);
     ctx->seg_mask = 0xFFFFFFFFu;
+    ctx->seg_count_valid = false;
     if (rc_launch) return rc_launch;
-    GPV_CUDA_TRY(cudaMemcpyAsync(out, ctx->out_dev.ptr, sizeof(gpv_subset_result) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    GPV_CUDA_TRY(cudaMemcpyAsync(h_out, ctx->out_dev.ptr, sizeof(gpv_subset_result) * n, cudaMemcpyDeviceToHost, ctx->stream));
     if (prm->history) {
         GPV_CUDA_TRY(cudaMemcpyAsync(prm->history, hist_dev, hist_bytes, cudaMemcpyDeviceToHost, ctx->stream));
     }
     GPV_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(out, h_out, sizeof(gpv_subset_result) * (size_t)n);
     return GPV_SUCCESS;
 }
 

@@ -53,9 +53,14 @@ struct TileSmem {
 struct TileArgs {
     KArgs k;
     const int32_t *seg;  // [start, count] of this order's segment in k.order
-    int *queue;          // this kernel's work-queue counter
+    int *queue;          // this kernel's work-queue counter (persistent grid)
     int win_cap;         // floats of dynamic shared memory for the window
     int layout;          // template slots: kLayoutCompact, kLayoutRows or kLayoutTiles
+    // one block per subset (slot_mask != nullptr): a block claims one of the
+    // slots_per_sm scratch slots of the SM it starts on (a bit of
+    // slot_mask[smid], n_mask words) and frees it when the subset is done
+    uint32_t *slot_mask;
+    int slots_per_sm, n_mask;
 };
 
 // Template slot layouts: the compact scan order; rows padded to whole warps
@@ -663,18 +668,67 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
     }
 }
 
+// Claim a free scratch slot of the SM this block runs on.  At most
+// slots_per_sm blocks of a launch are resident on an SM (the launch's
+// occupancy), and a block frees its slot before it exits, so a bit is free
+// when a block starts; the wait (bounded) only covers a block that changed
+// SM after a preemption still holding its first SM's slot.  -1: none claimed.
+__device__ int claim_slot(const TileArgs &T) {
+    unsigned smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    if ((int)smid >= T.n_mask) return -1;
+    for (int attempt = 0; attempt < 20000; attempt++) {
+        for (int j = 0; j < T.slots_per_sm; j++) {
+            const unsigned bit = 1u << j;
+            if (!(atomicOr(T.slot_mask + smid, bit) & bit)) return (int)smid * T.slots_per_sm + j;
+        }
+        __nanosleep(1000);
+    }
+    return -1;
+}
+
 // Scratch per block: n_max float4 records + n_max floats (eta resample).
-template <int ORDER, int NT>
+// PER_SUBSET: one block per subset with a claimed scratch slot, else a
+// persistent grid taking subsets from the queue (two instantiations, so
+// each holds one inlined copy of the solve).
+template <int ORDER, int NT, bool PER_SUBSET>
 __global__ void __launch_bounds__(NT, 512 / NT) icgn_tile(TileArgs T) {
     extern __shared__ float4 win4[];
     float *win = reinterpret_cast<float *>(win4);
     __shared__ TileSmem sm;
     const KArgs &A = T.k;
     const int64_t nmax = A.scratch_stride / 5;
+    const int start = T.seg[0], count = T.seg[1];
+    if (PER_SUBSET) {
+        const int item = blockIdx.x;
+        if (item >= count) return;
+        if (threadIdx.x == 0) sm.item = claim_slot(T);
+        __threadfence();
+        __syncthreads();
+        const int slot = sm.item;
+        const int idx = A.order[start + item];
+        const gpv_subset_desc d = A.desc[idx];
+        if (slot < 0) {
+            if (threadIdx.x == 0) write_failed(A, idx, d, 12, GPV_TIMEOUT, 0, 0.0, 0.0);
+            return;
+        }
+        float *base = reinterpret_cast<float *>(A.scratch) + (int64_t)slot * A.scratch_stride;
+        if (d.radius < 1 || d.radius > A.max_radius) {
+            if (threadIdx.x == 0) write_failed(A, idx, d, 12, GPV_INVALID_SUBSET, 0, 0.0, 0.0);
+        } else {
+            tile_subset<ORDER, NT>(T, idx, d, reinterpret_cast<float4 *>(base), base + 4 * nmax, win, sm);
+        }
+        __threadfence();  // every scratch access of the block is done before the slot is free
+        __syncthreads();
+        if (threadIdx.x == 0) {  // the slot is re-read from shared memory (nothing else writes sm.item here)
+            const int own = sm.item;
+            atomicAnd(T.slot_mask + own / T.slots_per_sm, ~(1u << (own % T.slots_per_sm)));
+        }
+        return;
+    }
     float *base = reinterpret_cast<float *>(A.scratch) + (int64_t)blockIdx.x * A.scratch_stride;
     float4 *S4 = reinterpret_cast<float4 *>(base);
     float *Sg = base + 4 * nmax;
-    const int start = T.seg[0], count = T.seg[1];
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) sm.item = atomicAdd(T.queue, 1);
@@ -760,17 +814,32 @@ __global__ void scatter_orders(const gpv_subset_desc *desc, const int32_t *order
     }
 }
 
-template <int NT>
-const void *tile_kernel(int order) {
-    return order == 2 ? (const void *)icgn_tile<2, NT> : (order == 1 ? (const void *)icgn_tile<1, NT>
-                                                                     : (const void *)icgn_tile<0, NT>);
+template <int NT, bool PS>
+const void *tile_kernel_t(int order) {
+    return order == 2 ? (const void *)icgn_tile<2, NT, PS>
+                      : (order == 1 ? (const void *)icgn_tile<1, NT, PS> : (const void *)icgn_tile<0, NT, PS>);
 }
 
-template <int NT>
-void tile_launch_one(int order, int blocks, size_t smem, cudaStream_t s, const TileArgs &T) {
-    if (order == 2) icgn_tile<2, NT><<<blocks, NT, smem, s>>>(T);
-    else if (order == 1) icgn_tile<1, NT><<<blocks, NT, smem, s>>>(T);
-    else icgn_tile<0, NT><<<blocks, NT, smem, s>>>(T);
+const void *tile_kernel(int nt, bool per_subset, int order) {
+    if (nt == 256) return per_subset ? tile_kernel_t<256, true>(order) : tile_kernel_t<256, false>(order);
+    return per_subset ? tile_kernel_t<128, true>(order) : tile_kernel_t<128, false>(order);
+}
+
+template <int NT, bool PS>
+void tile_launch_t(int order, int blocks, size_t smem, cudaStream_t s, const TileArgs &T) {
+    if (order == 2) icgn_tile<2, NT, PS><<<blocks, NT, smem, s>>>(T);
+    else if (order == 1) icgn_tile<1, NT, PS><<<blocks, NT, smem, s>>>(T);
+    else icgn_tile<0, NT, PS><<<blocks, NT, smem, s>>>(T);
+}
+
+void tile_launch_one(int nt, bool per_subset, int order, int blocks, size_t smem, cudaStream_t s, const TileArgs &T) {
+    if (nt == 256) {
+        if (per_subset) tile_launch_t<256, true>(order, blocks, smem, s, T);
+        else tile_launch_t<256, false>(order, blocks, smem, s, T);
+    } else {
+        if (per_subset) tile_launch_t<128, true>(order, blocks, smem, s, T);
+        else tile_launch_t<128, false>(order, blocks, smem, s, T);
+    }
 }
 
 }  // namespace
@@ -810,16 +879,41 @@ static int window_cap(int r, int layout) {
     return side * window_pitch(side, layout);
 }
 
-uint32_t tile_segment_mask(const gpv_subset_desc *desc, int64_t n, int max_radius) {
-    uint32_t mask = 0;
-    for (int64_t i = 0; i < n; i++) {
+static_assert(kTileSegs == kSegs, "segment count");
+
+uint32_t tile_segment_counts(const gpv_subset_desc *desc, int64_t n, int max_radius, int64_t *counts) {
+    for (int q = 0; q < kSegs; q++) counts[q] = 0;
+    for (int64_t i = 0; i < n; i++) {  // segment_of, on the host
         const gpv_subset_desc &d = desc[i];
         if (d.order < 0 || d.order > 2 || d.radius < 1 || d.radius > max_radius) continue;
         int c = 0;
         while (c < kRClasses - 1 && d.radius > kRBoundHost[c]) c++;
-        mask |= 1u << ((2 - d.order) * kRClasses + c);
+        counts[(2 - d.order) * kRClasses + c]++;
     }
+    uint32_t mask = 0;
+    for (int q = 0; q < kSegs; q++)
+        if (counts[q]) mask |= 1u << q;
     return mask;
+}
+
+namespace {
+__global__ void nsmid_kernel(int *out) {
+    unsigned v;
+    asm volatile("mov.u32 %0, %%nsmid;" : "=r"(v));
+    *out = (int)v;
+}
+}  // namespace
+
+int query_nsmid(int *out) {
+    int *d = nullptr;
+    GPV_CUDA_TRY(cudaMalloc(&d, sizeof(int)));
+    nsmid_kernel<<<1, 1>>>(d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    GPV_CUDA_TRY(e);
+    if (*out < 1 || *out > 4096) { set_error("unexpected SM identifier count"); return GPV_ERR_CUDA; }
+    return GPV_SUCCESS;
 }
 
 // Launch one kernel per (order, radius class) segment that can hold
@@ -834,32 +928,44 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
     scatter_orders<<<blocks, 256, 0, s>>>(K.desc, K.order, (int)n, K.max_radius, cnt, fill, order_out, seg, K.out);
     GPV_CUDA_TRY(cudaGetLastError());
     struct Plan {
-        int rmax = 0, nt = 0, layout = 0, cap = 0, blocks = 0;
+        int rmax = 0, nt = 0, layout = 0, cap = 0, blocks = 0, per_sm = 0;
         int64_t stride = 0;
         bool live = false;
     };
     Plan plan[kSegs];
     int64_t region = 0;  // scratch floats per stream: its largest launch
+    // one block per subset when the context asks for it and the host knows
+    // the segment sizes (host batches); else a persistent grid
+    const bool per_subset = (ctx->flags & GPV_CONTEXT_PER_SUBSET_BLOCKS) && ctx->seg_count_valid && ctx->n_smid > 0;
     for (int q = 0; q < kSegs; q++) {
         const int order = 2 - q / kRClasses, c = q % kRClasses;
         const int lo = c == 0 ? 0 : kRBoundHost[c - 1];
         Plan &P = plan[q];
-        P.live = lo < K.max_radius && ((ctx->seg_mask >> q) & 1u);
+        P.live = lo < K.max_radius && ((ctx->seg_mask >> q) & 1u) && (!per_subset || ctx->seg_count[q] > 0);
         if (!P.live) continue;
         P.rmax = std::min(kRBoundHost[c], K.max_radius);
         P.nt = tile_threads_for(ctx, P.rmax);
         P.layout = tile_layout_for(ctx, P.rmax);
         P.cap = window_cap(P.rmax, P.layout);
         const size_t smem = sizeof(float) * P.cap;
-        const void *fn = P.nt == 256 ? tile_kernel<256>(order) : tile_kernel<128>(order);
+        const void *fn = tile_kernel(P.nt, per_subset, order);
         if (int rc = allow_max_dynamic_smem(fn)) return rc;
         int per_sm = 0;
         GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, P.nt, smem));
         if (per_sm < 1) { set_error("subset window does not fit in shared memory"); return GPV_ERR_INVALID; }
-        P.blocks = per_sm * ctx->num_sms;
+        if (per_sm > 32) per_sm = 32;  // slot claim words have 32 bits (never reached: 4 blocks of 128 threads)
+        P.per_sm = per_sm;
         const int64_t nmax = (int64_t)(ctx->h_slot_n[P.rmax] + 31) / 32 * 32;
         P.stride = 5 * nmax;  // float4 record + eta sample per pixel
-        region = std::max(region, (int64_t)P.blocks * P.stride);
+        int64_t slots;
+        if (per_subset) {
+            P.blocks = (int)ctx->seg_count[q];
+            slots = (int64_t)per_sm * ctx->n_smid;
+        } else {
+            P.blocks = per_sm * ctx->num_sms;
+            slots = P.blocks;
+        }
+        region = std::max(region, slots * P.stride);
     }
     if (int rc = ctx->scratch.ensure((size_t)3 * region * sizeof(float))) return rc;
     GPV_CUDA_TRY(cudaEventRecord(ctx->ev[0], s));
@@ -869,7 +975,11 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
     for (int q = 0; q < kSegs; q++) {
         const Plan &P = plan[q];
         if (!P.live) continue;
-        const int k = next;
+        // a persistent grid spreads its segments over three streams, so one
+        // segment's tail overlaps the next one's start; per-subset blocks have
+        // no long tail and stay on the caller's stream (fewer streams share
+        // the device's hardware queues with other contexts' work)
+        const int k = per_subset ? 0 : next;
         next = (next + 1) % 3;
         if (!used[k]) {
             GPV_CUDA_TRY(cudaStreamWaitEvent(st[k], ctx->ev[0], 0));
@@ -885,9 +995,11 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         T.queue = queues + q;
         T.k.scratch = static_cast<float *>(ctx->scratch.ptr) + (int64_t)k * region;
         T.k.scratch_stride = P.stride;
+        T.slot_mask = per_subset ? static_cast<uint32_t *>(ctx->slot_mask.ptr) + (int64_t)k * ctx->n_smid : nullptr;
+        T.slots_per_sm = P.per_sm;
+        T.n_mask = ctx->n_smid;
         const size_t smem = sizeof(float) * P.cap;
-        if (P.nt == 256) tile_launch_one<256>(2 - q / kRClasses, P.blocks, smem, st[k], T);
-        else tile_launch_one<128>(2 - q / kRClasses, P.blocks, smem, st[k], T);
+        tile_launch_one(P.nt, per_subset, 2 - q / kRClasses, P.blocks, smem, st[k], T);
         GPV_CUDA_TRY(cudaGetLastError());
     }
     for (int k = 1; k < 3; k++) {

@@ -39,6 +39,17 @@ struct DevBuf {
     void release();
 };
 
+// Pinned (page-locked) host memory, grown on demand.  Copies between the
+// device and pageable memory go through the driver's own staging and can
+// wait behind other streams' work; from pinned memory they are plain DMA on
+// the caller's stream.
+struct HostBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want);
+    void release();
+};
+
 // Makes `dev` current for a scope and restores the caller's device.
 struct DeviceGuard {
     int prev = -1;
@@ -84,6 +95,12 @@ struct gpv_context {
     int tuned_layout[3] = {-1, -1, -1};  // autotuned template layout by radius class (-1: compact)
     int force_layout = -1;               // set while the autotuner times a candidate
     uint32_t seg_mask = 0xFFFFFFFFu;   // tiled-solve segments a host batch holds (all when unknown)
+    int64_t seg_count[12] = {};        // subsets per segment of that batch (valid with seg_count_valid)
+    bool seg_count_valid = false;
+    uint32_t flags = 0;                // GPV_CONTEXT_*
+    int n_smid = 0;                    // SM identifiers of the device (per-subset blocks)
+    gpv::DevBuf slot_mask;             // per stream region, per SM: claimed scratch slots
+    gpv::HostBuf h_stage;              // pinned staging of host batches: desc | work order | results
     // owner reference + one per image / mask created on it: the context is
     // freed when gpv_context_destroy and every dependant's destroy have run,
     // in whatever order they come
@@ -134,8 +151,6 @@ int probe_fp32_peak(gpv_context *ctx, double *tflops);
 int mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements, int64_t n_elements,
                int32_t nodes_per_element, const gpv_mesh_params *mp, gpv_batch_solver_fn solver, void *solver_user,
                gpv_subset_result *out, int32_t *rounds, gpv_mesh_stats *stats);
-// The (order, radius class) segments of the tiled solve that a host batch
-// holds (bit q = segment q); lets the launcher skip empty segments.
 // Colour ingest (load_grayscale + gaussian_blur_5x5): RGB8 (h, w, 3) -> u8 grey.
 int ingest_launch(const uint8_t *rgb_dev, int64_t h, int64_t w, uint8_t *grey_dev, cudaStream_t s);
 // Threads per block / template layout (0 compact, 1 padded rows, 2 tiles) of
@@ -143,7 +158,13 @@ int ingest_launch(const uint8_t *rgb_dev, int64_t h, int64_t w, uint8_t *grey_de
 // GPV_TILE_LAYOUT, else a candidate being timed, else the tuned choice.
 int tile_threads_for(gpv_context *ctx, int max_radius);
 int tile_layout_for(gpv_context *ctx, int max_radius);
-uint32_t tile_segment_mask(const gpv_subset_desc *desc, int64_t n, int max_radius);
+// Subsets per (order, radius class) segment of the tiled solve in a host
+// batch (counts[kTileSegs]); returns the mask of non-empty segments (bit q =
+// segment q), which lets the launcher skip empty ones.
+constexpr int kTileSegs = 12;
+uint32_t tile_segment_counts(const gpv_subset_desc *desc, int64_t n, int max_radius, int64_t *counts);
+// Number of SM identifiers (%nsmid) of the current device.
+int query_nsmid(int *out);
 int solve_noalloc_launch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
                          int64_t n, int max_radius, const gpv_solve_params *prm, gpv_subset_result *out_dev,
                          cudaStream_t s);

@@ -13,7 +13,13 @@
 // resident on their worker: later requests of the session can skip the
 // reference upload and prefilter and seed every subset from its previous
 // converged warp, as the frame loop of a sequence does (src/sequence.rs:
-// 624-968).  Every wait in this file is bounded.
+// 624-968).  With a priority lane, the first priority_workers workers own
+// high-priority contexts and serve only requests of up to priority_subsets
+// subsets, the others serve the larger ones, and all of them solve with one
+// thread block per subset: a large batch then holds each SM slot for one
+// subset at a time, and the block scheduler hands freed slots to the
+// pending blocks of the high-priority streams first.  Every wait in this
+// file is bounded.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -42,6 +48,7 @@ struct Request {
     size_t footprint = 0;
     int worker = -1;  // session affinity, -1 = any
     int bypassed = 0;
+    bool prepare = false;  // gpv_server_prepare: create the worker's image pair for (h, w, border, dtype)
     Clock::time_point t_submit, t_start, t_done;
     bool done = false;
     int status = GPV_SUCCESS;
@@ -154,6 +161,33 @@ int default_execute(gpv_server *S, Worker &W, Request &q, gpv_subset_result *out
     return GPV_SUCCESS;
 }
 
+// Whether worker W may take request c: its session's worker only; with a
+// priority lane, small requests go to the priority workers and large ones
+// to the others.
+bool eligible(const gpv_server *S, const Worker *W, const Request &c) {
+    if (c.worker >= 0) return c.worker == W->index;
+    if (S->cfg.priority_workers <= 0) return true;
+    const bool small = c.r.n <= S->cfg.priority_subsets;
+    return (W->index < S->cfg.priority_workers) == small;
+}
+
+// Create (or grow) the worker's cached image pair for the request's shape
+// and pixel type, so that requests of that shape allocate nothing.
+int prepare_images(Worker &W, const gpv_request &r) {
+    const size_t esz = r.dtype == GPV_U8 ? 1 : r.dtype == GPV_U16 ? 2 : r.dtype == GPV_F32 ? 4 : 8;
+    std::vector<uint8_t> zeros(esz * (size_t)r.h * (size_t)r.w, 0);
+    auto &pair = W.images[std::make_tuple(r.h, r.w, r.border)];
+    for (gpv_image **img : {&pair.first, &pair.second}) {
+        if (!*img) {
+            if (int rc = gpv_image_create(W.ctx, zeros.data(), r.dtype, r.h, r.w, r.border, 0, img)) return rc;
+        } else if (int rc = gpv_image_update(*img, zeros.data(), r.dtype)) {
+            return rc;
+        }
+    }
+    GPV_CUDA_TRY(cudaStreamSynchronize(W.ctx->stream));
+    return GPV_SUCCESS;
+}
+
 void worker_loop(gpv_server *S, Worker *W) {
     for (;;) {
         std::shared_ptr<Request> q;
@@ -165,7 +199,7 @@ void worker_loop(gpv_server *S, Worker *W) {
                 auto pick = S->queue.end();
                 for (auto it = S->queue.begin(); it != S->queue.end(); ++it) {
                     Request &c = **it;
-                    if (c.worker >= 0 && c.worker != W->index) continue;
+                    if (!eligible(S, W, c)) continue;
                     const bool fits = S->bytes_in_flight + c.footprint <= S->cfg.hbm_budget ||
                                       S->bytes_in_flight == 0;
                     if (fits) {
@@ -175,7 +209,8 @@ void worker_loop(gpv_server *S, Worker *W) {
                     if (c.bypassed >= kMaxBypass) break;  // no more overtaking this one
                 }
                 if (pick != S->queue.end()) {
-                    for (auto it = S->queue.begin(); it != pick; ++it) (*it)->bypassed++;
+                    for (auto it = S->queue.begin(); it != pick; ++it)
+                        if (eligible(S, W, **it)) (*it)->bypassed++;
                     q = *pick;
                     S->queue.erase(pick);
                     S->bytes_in_flight += q->footprint;
@@ -195,7 +230,9 @@ void worker_loop(gpv_server *S, Worker *W) {
         }
         int rc;
         std::string err;
-        if (S->cfg.executor) {
+        if (q->prepare) {
+            rc = S->cfg.executor ? GPV_SUCCESS : prepare_images(*W, q->r);
+        } else if (S->cfg.executor) {
             rc = S->cfg.executor(S->cfg.executor_user, W->index, &q->r, q->desc.data(), out);
         } else {
             rc = default_execute(S, *W, *q, out);
@@ -213,7 +250,9 @@ void worker_loop(gpv_server *S, Worker *W) {
             q->done = true;
             S->bytes_in_flight -= q->footprint;
             S->in_flight--;
-            if (rc) {
+            if (q->prepare) {
+                // not a served request: no statistics
+            } else if (rc) {
                 S->failed++;
             } else {
                 S->completed++;
@@ -253,6 +292,11 @@ int gpv_server_create(const gpv_server_config *cfg, gpv_server **out) {
         set_error("invalid server configuration (1..64 workers)");
         return GPV_ERR_INVALID;
     }
+    if (cfg->priority_workers < 0 || (cfg->priority_workers > 0 && cfg->priority_workers >= cfg->workers) ||
+        (cfg->priority_workers > 0 && cfg->priority_subsets < 1)) {
+        set_error("a priority lane needs 1..workers-1 priority workers and priority_subsets >= 1");
+        return GPV_ERR_INVALID;
+    }
     *out = nullptr;
     auto *S = new gpv_server();
     S->cfg = *cfg;
@@ -267,7 +311,10 @@ int gpv_server_create(const gpv_server_config *cfg, gpv_server **out) {
         auto W = std::make_unique<Worker>();
         W->index = k;
         if (!cfg->executor) {
-            int rc = gpv_context_create(cfg->device, &W->ctx);
+            uint32_t flags = 0;
+            if (cfg->priority_workers > 0)
+                flags = GPV_CONTEXT_PER_SUBSET_BLOCKS | (k < cfg->priority_workers ? GPV_CONTEXT_HIGH_PRIORITY : 0u);
+            int rc = gpv_context_create_ex(cfg->device, flags, &W->ctx);
             // sized once here, the workspace never grows (nor frees) while serving
             if (!rc && cfg->reserve_subsets > 0 && cfg->reserve_radius > 0)
                 rc = gpv_context_reserve(W->ctx, cfg->reserve_subsets, cfg->reserve_radius, 50);
@@ -321,6 +368,50 @@ int gpv_server_submit(gpv_server *S, const gpv_request *r, uint64_t *id) {
     }
     S->cv_work.notify_all();
     return GPV_SUCCESS;
+}
+
+int gpv_server_prepare(gpv_server *S, int64_t h, int64_t w, int32_t border, int32_t dtype, int32_t timeout_ms) {
+    if (!S) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    if (h < 1 || w < 1 || border < 3) { set_error("prepare needs a positive shape and border >= 3"); return GPV_ERR_INVALID; }
+    if (dtype != GPV_U8 && dtype != GPV_U16 && dtype != GPV_F32 && dtype != GPV_F64) {
+        set_error("unknown pixel dtype");
+        return GPV_ERR_INVALID;
+    }
+    std::vector<uint64_t> ids;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->stopping) { set_error("server is shutting down"); return GPV_ERR_INVALID; }
+        for (size_t k = 0; k < S->workers.size(); k++) {
+            auto q = std::make_shared<Request>();
+            q->prepare = true;
+            q->r.h = h;
+            q->r.w = w;
+            q->r.border = border;
+            q->r.dtype = dtype;
+            q->worker = (int)k;
+            q->t_submit = Clock::now();
+            q->id = S->next_id++;
+            S->reqs[q->id] = q;
+            S->queue.push_back(q);
+            ids.push_back(q->id);
+        }
+    }
+    S->cv_work.notify_all();
+    int first_rc = GPV_SUCCESS;
+    std::string first_err;
+    for (uint64_t id : ids) {
+        int32_t st = 0;
+        int rc = gpv_server_wait(S, id, timeout_ms, &st, nullptr);
+        if (!rc && st) rc = st;
+        if (rc && !first_rc) {
+            first_rc = rc;
+            char buf[512];
+            gpv_last_error(buf, sizeof buf);
+            first_err = buf;
+        }
+    }
+    if (first_rc) set_error(first_err);
+    return first_rc;
 }
 
 int gpv_server_wait(gpv_server *S, uint64_t id, int32_t timeout_ms, int32_t *req_status, double *latency_ms) {

@@ -9,7 +9,16 @@ marshals arguments.
 from __future__ import annotations
 
 import ctypes as ct
+import os
 import threading
+
+# Up to 32 hardware work queues instead of the driver's default 8, so that
+# the streams of concurrent contexts (server workers, high-priority streams)
+# do not share in-order queues, where a high-priority kernel would wait for a
+# low-priority one ahead of it.  The driver reads it when CUDA initialises in
+# the process, so it applies when this package is imported before any CUDA
+# use; an explicit setting is kept.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 import numpy as np
 
@@ -28,9 +37,14 @@ def version() -> str:
 class Context:
     """One CUDA device, one stream and the solve workspace (gpv_context)."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, high_priority: bool = False, per_subset_blocks: bool = False):
+        """high_priority: streams at the device's greatest priority;
+        per_subset_blocks: host-batch solves launch one block per subset
+        instead of a persistent grid (gpv_context_create_ex)."""
         h = ct.c_void_p()
-        check(lib().gpv_context_create(device, ct.byref(h)), "gpv_context_create")
+        flags = (_lib.CONTEXT_HIGH_PRIORITY if high_priority else 0) | \
+            (_lib.CONTEXT_PER_SUBSET_BLOCKS if per_subset_blocks else 0)
+        check(lib().gpv_context_create_ex(device, flags, ct.byref(h)), "gpv_context_create_ex")
         self._h = h
         self.device = device
 

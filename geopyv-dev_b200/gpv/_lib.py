@@ -67,7 +67,7 @@ class Request(ct.Structure):
 class ServerConfig(ct.Structure):
     _fields_ = [("hbm_budget", ct.c_size_t), ("workers", ct.c_int32), ("device", ct.c_int32),
                 ("executor", EXECUTOR_FN), ("executor_user", ct.c_void_p), ("reserve_subsets", ct.c_int64),
-                ("reserve_radius", ct.c_int32), ("reserved", ct.c_int32)]
+                ("reserve_radius", ct.c_int32), ("priority_workers", ct.c_int32), ("priority_subsets", ct.c_int64)]
 
 
 class ServerStats(ct.Structure):
@@ -79,6 +79,7 @@ class ServerStats(ct.Structure):
 
 
 REQUEST_REUSE_REFERENCE, REQUEST_SEED_FROM_PREVIOUS = 1, 2
+CONTEXT_HIGH_PRIORITY, CONTEXT_PER_SUBSET_BLOCKS = 1, 2
 
 # enums
 GPV_U8, GPV_U16, GPV_F32, GPV_F64 = 1, 2, 3, 4
@@ -97,6 +98,7 @@ SIGNATURES = {
     "gpv_abi_version": (ct.c_int, []),
     "gpv_last_error": (SZ, [ct.c_char_p, SZ]),
     "gpv_context_create": (ct.c_int, [ct.c_int, P]),
+    "gpv_context_create_ex": (ct.c_int, [ct.c_int, ct.c_uint32, P]),
     "gpv_context_destroy": (ct.c_int, [P]),
     "gpv_context_stream": (P, [P]),
     "gpv_context_reserve": (ct.c_int, [P, I64, I32, I32]),
@@ -125,6 +127,7 @@ SIGNATURES = {
     "gpv_sequence_create": (ct.c_int, [P, P, P, P, I64, P, I32, U32, P]),
     "gpv_server_create": (ct.c_int, [P, P]),
     "gpv_server_submit": (ct.c_int, [P, P, P]),
+    "gpv_server_prepare": (ct.c_int, [P, I64, I64, I32, I32, I32]),
     "gpv_server_wait": (ct.c_int, [P, ct.c_uint64, I32, P, P]),
     "gpv_server_get_stats": (ct.c_int, [P, P]),
     "gpv_server_reset_stats": (ct.c_int, [P]),

@@ -28,13 +28,18 @@ class Ticket:
 
 class Server:
     def __init__(self, workers: int = 4, hbm_budget: int = 0, device: int = 0, executor=None,
-                 reserve_subsets: int = 0, reserve_radius: int = 0):
+                 reserve_subsets: int = 0, reserve_radius: int = 0, priority_workers: int = 0,
+                 priority_subsets: int = 0):
         """executor(worker, request_dict, desc, out) -> int replaces the GPU solve
         (a stand-in for exercising the request loop without a GPU).
-        reserve_subsets / reserve_radius size every worker's workspace up front."""
+        reserve_subsets / reserve_radius size every worker's workspace up front.
+        priority_workers > 0 opens a priority lane: workers 0..priority_workers-1
+        (high-priority streams) serve the requests of at most priority_subsets
+        subsets, the others the larger ones, all with one block per subset."""
         cfg = _lib.ServerConfig()
         cfg.hbm_budget, cfg.workers, cfg.device = hbm_budget, workers, device
         cfg.reserve_subsets, cfg.reserve_radius = reserve_subsets, reserve_radius
+        cfg.priority_workers, cfg.priority_subsets = priority_workers, priority_subsets
         self._cb = None
         if executor is not None:
             def _exec(user, worker, req_p, desc_p, out_p):
@@ -54,6 +59,12 @@ class Server:
         check(lib().gpv_server_create(ct.byref(cfg), ct.byref(h)), "gpv_server_create")
         self._h = h
         self._lock = threading.Lock()
+
+    def prepare(self, shape, dtype, border: int = 20, timeout_ms: int = 120000) -> None:
+        """Create every worker's cached image pair for requests of this shape and
+        pixel type (gpv_server_prepare), so serving them allocates nothing."""
+        check(lib().gpv_server_prepare(self._h, int(shape[0]), int(shape[1]), border,
+                                       _lib.DTYPES[np.dtype(dtype)], timeout_ms), "gpv_server_prepare")
 
     def submit(self, f_px, g_px, desc, border: int = 20, max_norm=1e-5, max_iterations=50, tolerance=0.75,
                session: int = 0, reuse_reference: bool = False, seed_from_previous: bool = False) -> Ticket:

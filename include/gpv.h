@@ -113,6 +113,18 @@ size_t gpv_last_error(char *buf, size_t len);
 
 /* ---- context: one device, one stream, reusable workspace ---------------- */
 int gpv_context_create(int device, gpv_context **out);
+/* Context options (no counterpart in the reference):
+ * GPV_CONTEXT_HIGH_PRIORITY: the context's streams run at the device's
+ *   greatest stream priority, so its kernels' blocks are dispatched before
+ *   pending blocks of ordinary streams as SMs free up;
+ * GPV_CONTEXT_PER_SUBSET_BLOCKS: host-batch solves (gpv_solve_batch and the
+ *   callers built on it) launch one thread block per subset instead of a
+ *   persistent grid, so SMs free up at subset granularity while a large
+ *   batch runs and other streams' work gets them; results are the same
+ *   bytes as the persistent form. */
+#define GPV_CONTEXT_HIGH_PRIORITY 1u
+#define GPV_CONTEXT_PER_SUBSET_BLOCKS 2u
+int gpv_context_create_ex(int device, uint32_t flags, gpv_context **out);
 /* The context's resources are freed once gpv_context_destroy and the destroy
  * of every image and mask created on it have all run, in any order. */
 int gpv_context_destroy(gpv_context *ctx);
@@ -304,7 +316,9 @@ int gpv_mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements
  * `hbm_budget` bytes (0 = 80% of the memory free at creation): requests start
  * in arrival order when they fit; a request that does not fit is overtaken
  * by later ones that do (at most 8 times); one larger than the whole budget
- * runs alone.  A session (nonzero `session`) is served by one worker, in
+ * runs alone.  With a priority lane (priority_workers > 0) small requests
+ * and large ones are served by separate workers, the small ones on
+ * high-priority streams.  A session (nonzero `session`) is served by one worker, in
  * order, and keeps its reference coefficients and its last results on that
  * worker: GPV_REQUEST_REUSE_REFERENCE skips the reference upload and
  * prefilter (f_px may then be NULL), GPV_REQUEST_SEED_FROM_PREVIOUS starts
@@ -344,7 +358,15 @@ typedef struct {
     void *executor_user;
     int64_t reserve_subsets;  /* size each worker's workspace for this many subsets */
     int32_t reserve_radius;   /* of up to this radius (0, 0 = grow on demand)       */
-    int32_t reserved;
+    /* Priority lane (0 = off): workers 0..priority_workers-1 run on
+     * high-priority streams and take the requests of at most
+     * priority_subsets subsets; the other workers take the larger ones, and
+     * every worker solves with one thread block per subset, so a small
+     * request's blocks get SMs as soon as subsets of the large ones finish
+     * instead of after their whole batch.  Session requests stay on their
+     * session's worker whatever their size. */
+    int32_t priority_workers;
+    int64_t priority_subsets;
 } gpv_server_config;
 
 typedef struct {
@@ -357,6 +379,12 @@ typedef struct {
 
 int gpv_server_create(const gpv_server_config *cfg, gpv_server **out);
 int gpv_server_submit(gpv_server *s, const gpv_request *req, uint64_t *id);
+/* Creates (or grows) every worker's cached image pair for requests of shape
+ * h x w, `border` and pixel type `dtype`, waiting up to timeout_ms per
+ * worker, so that serving such requests allocates no device memory (an
+ * allocation or free on the request path can stall every stream of the
+ * device).  Not counted in the statistics. */
+int gpv_server_prepare(gpv_server *s, int64_t h, int64_t w, int32_t border, int32_t dtype, int32_t timeout_ms);
 /* Waits up to timeout_ms for request `id`: GPV_ERR_TIMEOUT if unfinished,
  * GPV_ERR_NOT_FOUND for an unknown or already collected id; otherwise
  * GPV_SUCCESS with the request's own gpv_err in *req_status. */

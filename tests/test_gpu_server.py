@@ -52,6 +52,49 @@ def test_results_alone_equal_results_in_the_mix(gpv_mod):
         assert np.mean(got["converged"]) > 0.95
 
 
+def test_per_subset_blocks_give_the_persistent_bytes(gpv_mod):
+    """One block per subset (any stream priority) returns the bytes of the
+    persistent grid on a batch with every order and radius class, invalid
+    subsets and the eta diagnostic."""
+    rng = np.random.default_rng(17)
+    f, g, d = _request(rng, 1024, np.uint8, 3000, 77)
+    d["radius"] = rng.integers(8, 61, len(d))
+    d["order"] = rng.integers(0, 3, len(d))
+    d["radius"][:3] = 0
+    d["order"][3:6] = 5
+    got = {}
+    for name, kw in (("persistent", {}), ("per_subset", dict(per_subset_blocks=True)),
+                     ("priority", dict(per_subset_blocks=True, high_priority=True))):
+        ctx = gpv_mod.Context(0, **kw)
+        F, G = gpv_mod.Image(image_gs=f, ctx=ctx), gpv_mod.Image(image_gs=g, ctx=ctx)
+        got[name] = gpv_mod.solve_batch(F, G, d, eta=True).copy()
+        if name == "per_subset":  # a second batch on the same context reuses the freed slots
+            again = gpv_mod.solve_batch(F, G, d[::-1].copy(), eta=True)
+            assert again[::-1].tobytes() == got[name].tobytes()
+    assert got["per_subset"].tobytes() == got["persistent"].tobytes()
+    assert got["priority"].tobytes() == got["persistent"].tobytes()
+    assert np.all(got["persistent"]["status"][:6] == 8)
+    assert np.mean(got["persistent"]["converged"][6:]) > 0.9
+
+
+def test_priority_lane_results_equal_results_alone(gpv_mod):
+    rng = np.random.default_rng(23)
+    reqs = []
+    for k, (size, dt) in enumerate([(1024, np.uint8), (256, np.uint8), (512, np.uint16), (256, np.uint16),
+                                    (1024, np.uint16), (512, np.uint8)]):
+        n = [4000, 80, 300, 120, 3500, 200][k]
+        reqs.append(_request(rng, size, dt, n, 700 + k))
+    srv = gpv_mod.Server(workers=4, priority_workers=2, priority_subsets=500)
+    tickets = [srv.submit(f, g, d) for f, g, d in reqs]
+    mixed = [srv.wait(t, 120000).copy() for t in tickets]
+    assert srv.stats()["failed"] == 0
+    srv.close()
+    for (f, g, d), got in zip(reqs, mixed):
+        ctx = gpv_mod.Context(0)
+        alone = gpv_mod.solve_batch(gpv_mod.Image(image_gs=f, ctx=ctx), gpv_mod.Image(image_gs=g, ctx=ctx), d)
+        assert alone.tobytes() == got.tobytes()
+
+
 def test_session_frames_match_the_frame_tracker(gpv_mod):
     from gpv import synth
     Ws = [synth.workload(4, scale_down=4, seed_frame=k) for k in (0, 6, 12, 18, 24)]

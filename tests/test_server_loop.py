@@ -144,3 +144,44 @@ def test_close_serves_what_is_queued(gpv_mod):
         srv.submit(_px(), _px(), _desc(gpv_mod, 1))
     srv.close()
     assert len(rec.log) == 8
+
+
+def test_priority_lane_routes_by_size(gpv_mod):
+    """With a priority lane, requests of at most priority_subsets subsets run
+    on the priority workers only, larger ones on the others, and session
+    requests stay on their session's worker whatever their size."""
+    rec = Recorder(delay=0.005)
+    srv = gpv_mod.Server(workers=5, executor=rec, hbm_budget=1 << 30, priority_workers=2, priority_subsets=8)
+    tickets = []
+    for k in range(24):
+        tickets.append(srv.submit(_px(), _px(), _desc(gpv_mod, 3 + (k % 3) * 5)))  # 3, 8, 13 subsets
+    for k in range(4):
+        tickets.append(srv.submit(_px(), _px(), _desc(gpv_mod, 20), session=5))  # large, pinned to worker 0
+    for t in tickets:
+        srv.wait(t, 10000)
+    srv.close()
+    plain = [(w, n) for w, s, n, _ in rec.log if s == 0]
+    assert len(plain) == 24
+    assert all(w < 2 for w, n in plain if n <= 8) and all(w >= 2 for w, n in plain if n > 8)
+    assert {w for w, s, _, _ in rec.log if s == 5} == {5 % 5}
+
+
+def test_priority_lane_config_checks(gpv_mod):
+    for pw, ps in ((3, 10), (-1, 10), (1, 0)):
+        with pytest.raises(gpv_mod.GpvError, match="priority"):
+            gpv_mod.Server(workers=3, executor=Recorder(), hbm_budget=1 << 30, priority_workers=pw,
+                           priority_subsets=ps)
+
+
+def test_prepare_reaches_every_worker_and_is_not_a_request(gpv_mod):
+    rec = Recorder(delay=0.001)
+    srv = gpv_mod.Server(workers=3, executor=rec, hbm_budget=1 << 30)
+    srv.prepare((H, W), np.uint8)
+    srv.prepare((H, W), np.uint16)
+    st = srv.stats()
+    assert st["completed"] == 0 and st["submitted"] == 0 and not rec.log
+    with pytest.raises(gpv_mod.GpvError, match="border"):
+        srv.prepare((H, W), np.uint8, border=1)
+    srv.wait(srv.submit(_px(), _px(), _desc(gpv_mod, 2)), 10000)
+    assert srv.stats()["completed"] == 1
+    srv.close()
