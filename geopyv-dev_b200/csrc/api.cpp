@@ -68,6 +68,52 @@ static size_t stage_off_order(int64_t n) { return (sizeof(gpv_subset_desc) * (si
 static size_t stage_off_out(int64_t n) { return stage_off_order(n) + (sizeof(int32_t) * (size_t)n + 255) / 256 * 256; }
 static size_t stage_bytes(int64_t n) { return stage_off_out(n) + sizeof(gpv_subset_result) * (size_t)n; }
 
+// Whether [p, p + bytes) is page-locked host memory of one allocation (its
+// two ends pinned, mapped at the same distance on the device side).
+static bool host_pinned(const void *p, size_t bytes) {
+    if (!p || !bytes) return false;
+    cudaPointerAttributes a, b;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    if (a.type != cudaMemoryTypeHost) return false;
+    const char *q = static_cast<const char *>(p) + bytes - 1;
+    if (cudaPointerGetAttributes(&b, q) != cudaSuccess) { cudaGetLastError(); return false; }
+    return b.type == cudaMemoryTypeHost && a.devicePointer && b.devicePointer &&
+           static_cast<const char *>(b.devicePointer) - static_cast<const char *>(a.devicePointer) == (ptrdiff_t)(bytes - 1);
+}
+
+// Host -> device from pageable memory through pinned staging, in chunks, so
+// that the copy of one chunk into the staging overlaps the DMA of the last.
+static int upload_staged(void *dst_dev, const void *src, void *stage, size_t bytes, cudaStream_t s) {
+    const size_t chunk = std::max<size_t>(size_t(2) << 20, (bytes + 7) / 8);
+    for (size_t off = 0; off < bytes; off += chunk) {
+        const size_t len = std::min(chunk, bytes - off);
+        std::memcpy(static_cast<char *>(stage) + off, static_cast<const char *>(src) + off, len);
+        GPV_CUDA_TRY(cudaMemcpyAsync(static_cast<char *>(dst_dev) + off, static_cast<char *>(stage) + off, len,
+                                     cudaMemcpyHostToDevice, s));
+    }
+    return GPV_SUCCESS;
+}
+
+// Device -> host into pageable memory through pinned staging: at most eight
+// chunks, each copied out as soon as its DMA has landed.
+static int download_staged(gpv_context *ctx, void *dst, const void *src_dev, void *stage, size_t bytes, cudaStream_t s) {
+    const size_t chunk = std::max<size_t>(size_t(2) << 20, (bytes + 7) / 8);
+    int m = 0;
+    for (size_t off = 0; off < bytes; off += chunk, m++) {
+        const size_t len = std::min(chunk, bytes - off);
+        GPV_CUDA_TRY(cudaMemcpyAsync(static_cast<char *>(stage) + off, static_cast<const char *>(src_dev) + off, len,
+                                     cudaMemcpyDeviceToHost, s));
+        GPV_CUDA_TRY(cudaEventRecord(ctx->ev_chunk[m], s));
+    }
+    m = 0;
+    for (size_t off = 0; off < bytes; off += chunk, m++) {
+        const size_t len = std::min(chunk, bytes - off);
+        GPV_CUDA_TRY(cudaEventSynchronize(ctx->ev_chunk[m]));
+        std::memcpy(static_cast<char *>(dst) + off, static_cast<char *>(stage) + off, len);
+    }
+    return GPV_SUCCESS;
+}
+
 struct short2_h {
     int16_t x, y;
 };
@@ -203,6 +249,7 @@ int gpv_context_create_ex(int device, uint32_t flags, gpv_context **out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio);
     for (int k = 0; k < 2 && e == cudaSuccess; k++) e = cudaStreamCreateWithPriority(&ctx->aux[k], cudaStreamNonBlocking, prio);
     for (int k = 0; k < 3 && e == cudaSuccess; k++) e = cudaEventCreateWithFlags(&ctx->ev[k], cudaEventDisableTiming);
+    for (int k = 0; k < 8 && e == cudaSuccess; k++) e = cudaEventCreateWithFlags(&ctx->ev_chunk[k], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         set_error(std::string("context: ") + cudaGetErrorString(e));
         context_release(ctx);
@@ -239,6 +286,8 @@ static void context_release(gpv_context *ctx) {
         if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
     for (int k = 0; k < 3; k++)
         if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+    for (int k = 0; k < 8; k++)
+        if (ctx->ev_chunk[k]) cudaEventDestroy(ctx->ev_chunk[k]);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -568,33 +617,16 @@ int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, co
     if (n == 0) return GPV_SUCCESS;
     std::lock_guard<std::mutex> lk(ctx->mu);
     DeviceGuard dg(ctx->device);
-    int max_r = 1;
-    for (int64_t i = 0; i < n; i++)
-        if (desc[i].radius > max_r && desc[i].radius <= 4000) max_r = desc[i].radius;
-    if (int rc = ensure_tables(ctx, max_r)) return rc;
-    // descriptors, work order and results pass through pinned staging
+    // the work order, and descriptors / results not already in pinned memory,
+    // pass through pinned staging (copies from pageable memory go through the
+    // driver's own staging, which can wait behind other streams' work)
     if (int rc = ctx->h_stage.ensure(stage_bytes(n))) return rc;
     char *stage = static_cast<char *>(ctx->h_stage.ptr);
-    gpv_subset_desc *h_desc = reinterpret_cast<gpv_subset_desc *>(stage);
     int32_t *order = reinterpret_cast<int32_t *>(stage + stage_off_order(n));
-    gpv_subset_result *h_out = reinterpret_cast<gpv_subset_result *>(stage + stage_off_out(n));
-    std::memcpy(h_desc, desc, sizeof(gpv_subset_desc) * (size_t)n);
-    // largest subsets first (longest-processing-time order for the work queue)
-    // bucket key = 3 * radius + min(order, 2): larger radius first, order 2 before 1 before 0
-    {
-        const int nk = 3 * (max_r + 1);
-        std::vector<int64_t> start(nk + 1, 0);
-        auto key = [&](int64_t i) -> int {
-            const int r = desc[i].radius, o = desc[i].order;
-            if (r < 1 || r > max_r || o < 0 || o > 2) return 0;
-            return nk - 1 - (3 * r + o);
-        };
-        for (int64_t i = 0; i < n; i++) start[key(i) + 1]++;
-        for (int k = 0; k < nk; k++) start[k + 1] += start[k];
-        for (int64_t i = 0; i < n; i++) order[start[key(i)]++] = (int32_t)i;
-    }
-    if (int rc = ctx->desc_dev.ensure(sizeof(gpv_subset_desc) * n)) return rc;
-    if (int rc = ctx->out_dev.ensure(sizeof(gpv_subset_result) * n)) return rc;
+    const size_t desc_bytes = sizeof(gpv_subset_desc) * (size_t)n, out_bytes = sizeof(gpv_subset_result) * (size_t)n;
+    const bool desc_pinned = host_pinned(desc, desc_bytes), out_pinned = host_pinned(out, out_bytes);
+    if (int rc = ctx->desc_dev.ensure(desc_bytes)) return rc;
+    if (int rc = ctx->out_dev.ensure(out_bytes)) return rc;
     if (int rc = ctx->order_dev.ensure(sizeof(int32_t) * n)) return rc;
     double *hist_dev = nullptr;
     const size_t hist_bytes = sizeof(double) * 3 * (size_t)n * (size_t)(prm->max_iterations > 0 ? prm->max_iterations : 1);
@@ -603,7 +635,44 @@ int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, co
         hist_dev = static_cast<double *>(ctx->hist_dev.ptr);
         GPV_CUDA_TRY(cudaMemsetAsync(hist_dev, 0, hist_bytes, ctx->stream));
     }
-    GPV_CUDA_TRY(cudaMemcpyAsync(ctx->desc_dev.ptr, h_desc, sizeof(gpv_subset_desc) * n, cudaMemcpyHostToDevice, ctx->stream));
+    // the descriptors travel while the host builds the work order
+    if (desc_pinned) {
+        GPV_CUDA_TRY(cudaMemcpyAsync(ctx->desc_dev.ptr, desc, desc_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    } else if (int rc = upload_staged(ctx->desc_dev.ptr, desc, stage, desc_bytes, ctx->stream)) {
+        return rc;
+    }
+    // largest subsets first (longest-processing-time order for the work
+    // queue): a counting sort on key = 3 * radius + order, larger radius
+    // first, order 2 before 1 before 0 (invalid subsets in bucket 0).  One
+    // pass builds the histogram and finds the largest radius; the segment
+    // sizes of the tiled launch come from the histogram.
+    constexpr int kMaxR = 4000;
+    constexpr int nk = 3 * (kMaxR + 1);
+    std::vector<int64_t> start(nk + 1, 0);
+    auto key = [](const gpv_subset_desc &d) -> int {
+        const int r = d.radius, o = d.order;
+        if (r < 1 || r > kMaxR || o < 0 || o > 2) return 0;
+        return nk - 1 - (3 * r + o);
+    };
+    int max_r = 1;
+    for (int64_t i = 0; i < n; i++) {
+        const gpv_subset_desc &d = desc[i];
+        start[key(d) + 1]++;
+        if (d.radius > max_r && d.radius <= kMaxR) max_r = d.radius;
+    }
+    if (int rc = ensure_tables(ctx, max_r)) return rc;
+    uint32_t seg_mask = 0;
+    for (int q = 0; q < kTileSegs; q++) ctx->seg_count[q] = 0;
+    for (int r = 1; r <= max_r; r++)
+        for (int o = 0; o <= 2; o++) {
+            const int64_t c = start[nk - 1 - (3 * r + o) + 1];
+            if (!c) continue;
+            const int q = tile_segment_of(r, o);
+            ctx->seg_count[q] += c;
+            seg_mask |= 1u << q;
+        }
+    for (int k = 0; k < nk; k++) start[k + 1] += start[k];
+    for (int64_t i = 0; i < n; i++) order[start[key(desc[i])]++] = (int32_t)i;
     GPV_CUDA_TRY(cudaMemcpyAsync(ctx->order_dev.ptr, order, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
     SolveLaunch L;
     L.f = f;
@@ -619,18 +688,21 @@ int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, co
     L.history = hist_dev;
     L.max_radius = max_r;
     // launch only the segments this batch holds, each sized by its count
-    ctx->seg_mask = tile_segment_counts(desc, n, max_r, ctx->seg_count);
+    ctx->seg_mask = seg_mask;
     ctx->seg_count_valid = true;
     const int rc_launch = solve_launch(ctx, L, ctx->stream);
     ctx->seg_mask = 0xFFFFFFFFu;
     ctx->seg_count_valid = false;
     if (rc_launch) return rc_launch;
-    GPV_CUDA_TRY(cudaMemcpyAsync(h_out, ctx->out_dev.ptr, sizeof(gpv_subset_result) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    if (out_pinned) {
+        GPV_CUDA_TRY(cudaMemcpyAsync(out, ctx->out_dev.ptr, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    } else if (int rc = download_staged(ctx, out, ctx->out_dev.ptr, stage + stage_off_out(n), out_bytes, ctx->stream)) {
+        return rc;
+    }
     if (prm->history) {
         GPV_CUDA_TRY(cudaMemcpyAsync(prm->history, hist_dev, hist_bytes, cudaMemcpyDeviceToHost, ctx->stream));
     }
     GPV_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    std::memcpy(out, h_out, sizeof(gpv_subset_result) * (size_t)n);
     return GPV_SUCCESS;
 }
 

@@ -881,19 +881,10 @@ static int window_cap(int r, int layout) {
 
 static_assert(kTileSegs == kSegs, "segment count");
 
-uint32_t tile_segment_counts(const gpv_subset_desc *desc, int64_t n, int max_radius, int64_t *counts) {
-    for (int q = 0; q < kSegs; q++) counts[q] = 0;
-    for (int64_t i = 0; i < n; i++) {  // segment_of, on the host
-        const gpv_subset_desc &d = desc[i];
-        if (d.order < 0 || d.order > 2 || d.radius < 1 || d.radius > max_radius) continue;
-        int c = 0;
-        while (c < kRClasses - 1 && d.radius > kRBoundHost[c]) c++;
-        counts[(2 - d.order) * kRClasses + c]++;
-    }
-    uint32_t mask = 0;
-    for (int q = 0; q < kSegs; q++)
-        if (counts[q]) mask |= 1u << q;
-    return mask;
+int tile_segment_of(int r, int o) {  // segment_of, on the host, for a valid subset
+    int c = 0;
+    while (c < kRClasses - 1 && r > kRBoundHost[c]) c++;
+    return (2 - o) * kRClasses + c;
 }
 
 namespace {

@@ -101,6 +101,7 @@ struct gpv_context {
     int n_smid = 0;                    // SM identifiers of the device (per-subset blocks)
     gpv::DevBuf slot_mask;             // per stream region, per SM: claimed scratch slots
     gpv::HostBuf h_stage;              // pinned staging of host batches: desc | work order | results
+    cudaEvent_t ev_chunk[8] = {};      // chunked result downloads through h_stage
     // owner reference + one per image / mask created on it: the context is
     // freed when gpv_context_destroy and every dependant's destroy have run,
     // in whatever order they come
@@ -158,11 +159,12 @@ int ingest_launch(const uint8_t *rgb_dev, int64_t h, int64_t w, uint8_t *grey_de
 // GPV_TILE_LAYOUT, else a candidate being timed, else the tuned choice.
 int tile_threads_for(gpv_context *ctx, int max_radius);
 int tile_layout_for(gpv_context *ctx, int max_radius);
-// Subsets per (order, radius class) segment of the tiled solve in a host
-// batch (counts[kTileSegs]); returns the mask of non-empty segments (bit q =
-// segment q), which lets the launcher skip empty ones.
+// The (order, radius class) segment of the tiled solve that holds a valid
+// subset of radius r and warp order o (0 <= q < kTileSegs); a host batch's
+// per-segment counts let the launcher skip empty segments and size
+// one-block-per-subset grids.
 constexpr int kTileSegs = 12;
-uint32_t tile_segment_counts(const gpv_subset_desc *desc, int64_t n, int max_radius, int64_t *counts);
+int tile_segment_of(int r, int o);
 // Number of SM identifiers (%nsmid) of the current device.
 int query_nsmid(int *out);
 int solve_noalloc_launch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
