@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--no-mesh", action="store_true", help="skip the mesh-propagation leg")
     ap.add_argument("--no-sequence", action="store_true", help="skip the frame-tracking leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch (graph) leg")
     ap.add_argument("--serving-seconds", type=float, default=10.0)
     return ap.parse_args()
 
@@ -352,6 +353,70 @@ def mesh_leg(W, F, G, args, cpu=True):
                              "same_rounds": bool(np.array_equal(ms.rounds, ref["rounds"])),
                              "what": "oracle/mesh_oracle.py over the FP64 C oracle (one OpenMP batch per colour)"}
     return out
+
+
+# ---------------------------------------------------------------------------
+def uneven_leg(device, steps=10):
+    """The uneven batch in one launch: the shear-band workload (2048^2 u8,
+    50k subsets from a mesh refined x4 near the band, radii 15..60
+    log-uniform, 70/30 first/second order) solved through the device C ABI,
+    eagerly and as a replayed CUDA graph (gpv_batch_graph_*); CUDA events on
+    the library stream around `steps` solves, inputs resident."""
+    import ctypes as ct
+
+    import torch
+
+    import gpv
+    from gpv import _lib, synth
+    W = synth.workload(3)
+    ctx = gpv.Context(device)
+    F = gpv.Image(image_gs=W["f"], border=20, ctx=ctx)
+    G = gpv.Image(image_gs=W["g"], border=20, ctx=ctx)
+    desc = gpv.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
+    n = len(desc)
+    ctx.reserve(n, int(desc["radius"].max()), 50)
+    order = np.argsort(-(3 * desc["radius"].astype(np.int64) + desc["order"]), kind="stable").astype(np.int32)
+    d_dev = torch.from_numpy(desc.view(np.uint8).copy()).cuda(device)
+    o_dev = torch.from_numpy(order).cuda(device)
+    out_dev = torch.zeros(n * _lib.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{device}")
+    prm = gpv._params(1e-5, 50, 0.75, False, gpv.PREC_MIXED, None, None)
+    L = _lib.lib()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    args = (ctx.handle, F.handle, G.handle, ct.c_void_p(d_dev.data_ptr()), ct.c_void_p(o_dev.data_ptr()), n,
+            ct.byref(prm), ct.c_void_p(out_dev.data_ptr()))
+
+    def timed(step):
+        for _ in range(3):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    ms_eager = timed(lambda: _lib.check(L.gpv_solve_batch_device(*args, None), "solve"))
+    res = np.frombuffer(out_dev.cpu().numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
+    bg = ct.c_void_p()
+    _lib.check(L.gpv_batch_graph_create(*args, ct.byref(bg)), "graph")
+    ms_graph = timed(lambda: _lib.check(L.gpv_batch_graph_launch(bg, None), "graph launch"))
+    res_g = np.frombuffer(out_dev.cpu().numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
+    L.gpv_batch_graph_destroy(bg)
+    ok = res["converged"] == 1
+    err = np.abs(res["p"][ok, :2] - W["truth_uv"][ok])
+    samples = float(np.sum(res["n_px"].astype(np.float64) * res["iterations"]))
+    return {"workload": W["name"], "subsets": n, "radius": [int(desc["radius"].min()), int(desc["radius"].max())],
+            "order2_frac": float(np.mean(desc["order"] == 2)), "steps": steps,
+            "ms_eager": ms_eager, "subsets_per_s_eager": n / (ms_eager * 1e-3),
+            "ms_graph": ms_graph, "subsets_per_s_graph": n / (ms_graph * 1e-3),
+            "samples_per_s_graph": samples / (ms_graph * 1e-3),
+            "graph_equals_eager": bool(res.tobytes() == res_g.tobytes()),
+            "converged_frac": float(ok.mean()), "iterations_mean": float(res["iterations"].mean()),
+            "median_err_vs_field_px": float(np.median(err)) if ok.any() else None,
+            "timing": "CUDA events on the library stream; device-resident images, descriptors, work order, results; "
+                      "one launch = order partition + one persistent kernel per (order, radius class) segment"}
 
 
 # ---------------------------------------------------------------------------
@@ -683,6 +748,9 @@ def run_ours(args, world, rank, local):
     seq = None
     if not args.no_sequence and args.config == 2 and args.scale_down == 1:
         seq = sequence_leg(ctx)
+    uneven = None
+    if not args.no_uneven and args.config == 2 and args.scale_down == 1:
+        uneven = uneven_leg(local)
     serving = None
     if not args.no_serving and args.config == 2 and args.scale_down == 1:
         serving = serving_leg(seconds=args.serving_seconds)
@@ -740,6 +808,8 @@ def run_ours(args, world, rank, local):
         line["mesh"] = mesh
     if seq is not None:
         line["sequence"] = seq
+    if uneven is not None:
+        line["uneven_batch"] = uneven
     if serving is not None:
         line["serving"] = serving
         line["p50_ms"] = serving["p50_ms"]

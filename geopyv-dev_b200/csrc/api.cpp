@@ -737,6 +737,110 @@ int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image
     return solve_launch(ctx, L, s);
 }
 
+}  // extern "C"
+
+// Addresses of the context workspace a captured solve reads and writes.
+struct WorkspaceAddrs {
+    const void *p[8];
+    bool operator==(const WorkspaceAddrs &o) const { return std::memcmp(p, o.p, sizeof p) == 0; }
+};
+static WorkspaceAddrs workspace_addrs(const gpv_context *ctx) {
+    return WorkspaceAddrs{{ctx->scratch.ptr, ctx->queue.ptr, ctx->tile_ws.ptr, ctx->offs.ptr, ctx->slots.ptr,
+                           ctx->tab_off.ptr, ctx->tab_n.ptr, ctx->slot_mask.ptr}};
+}
+
+struct gpv_batch_graph {
+    gpv_context *ctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    WorkspaceAddrs ws{};
+};
+
+extern "C" {
+
+int gpv_batch_graph_create(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
+                           const int32_t *work_order_dev, int64_t n, const gpv_solve_params *prm,
+                           gpv_subset_result *out_dev, gpv_batch_graph **out) {
+    if (!out) { set_error("out is NULL"); return GPV_ERR_INVALID; }
+    *out = nullptr;
+    if (prm && prm->history) { set_error("a batch graph keeps no iteration history"); return GPV_ERR_INVALID; }
+    if (n < 1) { set_error("a batch graph needs at least one subset"); return GPV_ERR_INVALID; }
+    // the eager run checks the arguments and sizes the workspace
+    if (int rc = gpv_solve_batch_device(ctx, f, g, desc_dev, work_order_dev, n, prm, out_dev, nullptr)) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    GPV_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    SolveLaunch L;
+    L.f = f;
+    L.g = g;
+    L.desc = desc_dev;
+    L.order = work_order_dev;
+    L.n = n;
+    L.prm = prm;
+    L.mask = prm->mask ? prm->mask->dev : nullptr;
+    L.mh = prm->mask ? prm->mask->h : 0;
+    L.mw = prm->mask ? prm->mask->w : 0;
+    L.out = out_dev;
+    L.history = nullptr;
+    L.max_radius = ctx->table_radius;
+    auto *bg = new gpv_batch_graph();
+    bg->ctx = ctx;
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        delete bg;
+        set_error(std::string("stream capture: ") + cudaGetErrorString(e));
+        return GPV_ERR_CUDA;
+    }
+    const int rc = solve_launch(ctx, L, st);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(st, &graph);
+    if (rc || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        delete bg;
+        if (!rc) set_error(std::string("stream capture: ") + cudaGetErrorString(e));
+        return rc ? rc : GPV_ERR_CUDA;
+    }
+    bg->graph = graph;
+    e = cudaGraphInstantiate(&bg->exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        delete bg;
+        set_error(std::string("graph instantiate: ") + cudaGetErrorString(e));
+        return GPV_ERR_CUDA;
+    }
+    bg->ws = workspace_addrs(ctx);
+    ctx->refs.fetch_add(1);  // the graph uses the context's workspace
+    *out = bg;
+    return GPV_SUCCESS;
+}
+
+int gpv_batch_graph_launch(gpv_batch_graph *bg, void *stream) {
+    if (!bg) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    gpv_context *ctx = bg->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!(workspace_addrs(ctx) == bg->ws)) {
+        set_error("the context's workspace moved since the graph was captured (reserve first, or recreate the graph)");
+        return GPV_ERR_INVALID;
+    }
+    DeviceGuard dg(ctx->device);
+    GPV_CUDA_TRY(cudaGraphLaunch(bg->exec, stream ? static_cast<cudaStream_t>(stream) : ctx->stream));
+    return GPV_SUCCESS;
+}
+
+int gpv_batch_graph_destroy(gpv_batch_graph *bg) {
+    if (!bg) return GPV_SUCCESS;
+    gpv_context *ctx = bg->ctx;
+    {
+        DeviceGuard dg(ctx->device);
+        if (bg->exec) cudaGraphExecDestroy(bg->exec);
+        if (bg->graph) cudaGraphDestroy(bg->graph);
+    }
+    delete bg;
+    context_release(ctx);
+    return GPV_SUCCESS;
+}
+
 static int check_pair(const gpv_image *f, const gpv_image *g, const gpv_solve_params *prm);
 
 int gpv_solve_batch_noalloc(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,

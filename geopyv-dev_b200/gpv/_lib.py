@@ -122,6 +122,9 @@ SIGNATURES = {
     "gpv_probe_fp32_peak": (ct.c_int, [P, P]),
     "gpv_autotune": (ct.c_int, [P, P, P, P, I64, P, I32, P]),
     "gpv_context_tuning": (ct.c_int, [P, P, P]),
+    "gpv_batch_graph_create": (ct.c_int, [P, P, P, P, P, I64, P, P, P]),
+    "gpv_batch_graph_launch": (ct.c_int, [P, P]),
+    "gpv_batch_graph_destroy": (ct.c_int, [P]),
     "gpv_solve_batch_noalloc": (ct.c_int, [P, P, P, P, I64, I32, P, P, P]),
     "gpv_mesh_solve": (ct.c_int, [P, P, P, P, I64, P, I64, I32, P, P, P, P]),
     "gpv_sequence_create": (ct.c_int, [P, P, P, P, I64, P, I32, U32, P]),

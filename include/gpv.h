@@ -196,6 +196,25 @@ int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image
                            const gpv_subset_desc *desc_dev, const int32_t *work_order_dev, int64_t n,
                            const gpv_solve_params *params, gpv_subset_result *out_dev, void *stream);
 
+/* ---- one device batch as a CUDA graph (no counterpart in the reference) --
+ * Captures one gpv_solve_batch_device call (same arguments; runs it once
+ * eagerly first, which sizes the context's workspace) as a CUDA graph:
+ * the order partition and one persistent kernel per (order, radius class)
+ * segment on the context's three streams.  A launch replays it on the
+ * current contents of the images, descriptors and work order (same buffers:
+ * update them in place), on `stream` (a cudaStream_t, or NULL for the
+ * context stream), asynchronously.  The graph holds the context's workspace
+ * addresses: a launch after another call on the context has moved them
+ * (a larger batch or radius; reserve first) returns GPV_ERR_INVALID, and it
+ * must not overlap other work of the same context.  History is not
+ * supported. */
+typedef struct gpv_batch_graph gpv_batch_graph;
+int gpv_batch_graph_create(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
+                           const int32_t *work_order_dev, int64_t n, const gpv_solve_params *params,
+                           gpv_subset_result *out_dev, gpv_batch_graph **out);
+int gpv_batch_graph_launch(gpv_batch_graph *bg, void *stream);
+int gpv_batch_graph_destroy(gpv_batch_graph *bg);
+
 /* ---- batched subset solve without device allocation ---------------------
  * No counterpart in the reference: an extra entry point for callers that may
  * not allocate device memory on the solve path (their device memory belongs
