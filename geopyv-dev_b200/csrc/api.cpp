@@ -68,6 +68,14 @@ static size_t stage_off_order(int64_t n) { return (sizeof(gpv_subset_desc) * (si
 static size_t stage_off_out(int64_t n) { return stage_off_order(n) + (sizeof(int32_t) * (size_t)n + 255) / 256 * 256; }
 static size_t stage_bytes(int64_t n) { return stage_off_out(n) + sizeof(gpv_subset_result) * (size_t)n; }
 
+int image_pixels_in(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s, bool staged) {
+    if (int rc = prefilter_launch(img, px_dev, dtype, s)) return rc;
+    img->px_current = staged;
+    if (staged) img->px_dtype = dtype;
+    if (img->grain) return grain_launch(img, px_dev, dtype, s);
+    return GPV_SUCCESS;
+}
+
 // Whether [p, p + bytes) is page-locked host memory of one allocation (its
 // two ends pinned, mapped at the same distance on the device side).
 static bool host_pinned(const void *p, size_t bytes) {
@@ -211,6 +219,7 @@ extern "C" {
 
 static void tune_cache_load(gpv_context *ctx);
 static void context_release(gpv_context *ctx);
+static int grain_alloc(gpv_image *img);
 
 const char *gpv_version(void) { return "gpv-b200 0.1.0 (sm_100a)"; }
 
@@ -321,6 +330,7 @@ static int image_alloc(gpv_context *ctx, int64_t h, int64_t w, int32_t border, u
     cudaError_t e = cudaMalloc(&img->c32, sizeof(float) * img->pitch32 * img->ch);
     if (e == cudaSuccess && (flags & GPV_IMAGE_KEEP_F64)) e = cudaMalloc(&img->c64, sizeof(double) * img->pitch64 * img->ch);
     if (e == cudaSuccess) e = cudaMalloc(&img->rowpass, sizeof(double) * (img->h * img->cw + 2 * 89 + 8));
+    if (e == cudaSuccess && (flags & GPV_IMAGE_GRAIN) && grain_alloc(img) != GPV_SUCCESS) e = cudaErrorMemoryAllocation;
     if (e != cudaSuccess) {
         set_error(std::string("image allocation: ") + cudaGetErrorString(e));
         cudaFree(img->c32);
@@ -351,7 +361,7 @@ int gpv_image_create(gpv_context *ctx, const void *px, int32_t dtype, int64_t h,
         *out = nullptr;
         return GPV_ERR_CUDA;
     }
-    rc = prefilter_launch(img, img->px_dev, dtype, ctx->stream);
+    rc = image_pixels_in(img, img->px_dev, dtype, ctx->stream, true);
     if (rc == GPV_SUCCESS) {
         e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) { set_error(std::string("prefilter: ") + cudaGetErrorString(e)); rc = GPV_ERR_CUDA; }
@@ -366,7 +376,7 @@ int gpv_image_create_device(gpv_context *ctx, const void *px_dev, int32_t dtype,
     DeviceGuard dg(ctx->device);
     int rc = image_alloc(ctx, h, w, border, flags, dtype, out);
     if (rc) return rc;
-    rc = prefilter_launch(*out, px_dev, dtype, ctx->stream);
+    rc = image_pixels_in(*out, px_dev, dtype, ctx->stream, false);
     if (rc) { gpv_image_destroy(*out); *out = nullptr; }
     return rc;
 }
@@ -374,7 +384,7 @@ int gpv_image_create_device(gpv_context *ctx, const void *px_dev, int32_t dtype,
 int gpv_image_update_device(gpv_image *img, const void *px_dev, int32_t dtype) {
     if (!img || !px_dev) { set_error("NULL argument"); return GPV_ERR_INVALID; }
     DeviceGuard dg(img->ctx->device);
-    return prefilter_launch(img, px_dev, dtype, img->ctx->stream);
+    return image_pixels_in(img, px_dev, dtype, img->ctx->stream, px_dev == img->px_dev);
 }
 
 int gpv_image_update(gpv_image *img, const void *px, int32_t dtype) {
@@ -391,7 +401,7 @@ int gpv_image_update(gpv_image *img, const void *px, int32_t dtype) {
         img->px_bytes = bytes;
     }
     GPV_CUDA_TRY(cudaMemcpyAsync(img->px_dev, px, bytes, cudaMemcpyHostToDevice, ctx->stream));
-    if (int rc = prefilter_launch(img, img->px_dev, dtype, ctx->stream)) return rc;
+    if (int rc = image_pixels_in(img, img->px_dev, dtype, ctx->stream, true)) return rc;
     GPV_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return GPV_SUCCESS;
 }
@@ -410,7 +420,7 @@ static int image_from_rgb_dev(gpv_image *img, const uint8_t *rgb_dev) {
         img->px_bytes = bytes;
     }
     if (int rc = ingest_launch(rgb_dev, img->h, img->w, static_cast<uint8_t *>(img->px_dev), ctx->stream)) return rc;
-    return prefilter_launch(img, img->px_dev, GPV_U8, ctx->stream);
+    return image_pixels_in(img, img->px_dev, GPV_U8, ctx->stream, true);
 }
 
 static int stage_rgb(gpv_image *img, const uint8_t *rgb) {
@@ -478,9 +488,56 @@ int gpv_image_destroy(gpv_image *img) {
     cudaFree(img->rowpass);
     cudaFree(img->px_dev);
     cudaFree(img->rgb_dev);
+    cudaFree(img->grain);
+    cudaFree(img->grain_scal);
+    cudaFree(img->grain_ac);
     gpv_context *ctx = img->ctx;
     delete img;
     context_release(ctx);
+    return GPV_SUCCESS;
+}
+
+static int grain_alloc(gpv_image *img) {
+    if (img->grain) return GPV_SUCCESS;
+    cudaError_t e = cudaMalloc(&img->grain, sizeof(float) * 3 * (size_t)img->h * (size_t)img->w);
+    if (e == cudaSuccess) e = cudaMalloc(&img->grain_scal, sizeof(double) * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&img->grain_ac, sizeof(double) * 512);
+    if (e != cudaSuccess) {
+        cudaFree(img->grain);
+        cudaFree(img->grain_scal);
+        cudaFree(img->grain_ac);
+        img->grain = nullptr;
+        img->grain_scal = img->grain_ac = nullptr;
+        set_error(std::string("grain maps: ") + cudaGetErrorString(e));
+        return GPV_ERR_NOMEM;
+    }
+    return GPV_SUCCESS;
+}
+
+int gpv_image_build_grain(gpv_image *img) {
+    if (!img) { set_error("img is NULL"); return GPV_ERR_INVALID; }
+    if (img->grain) return GPV_SUCCESS;
+    if (!img->px_current) {
+        set_error("the image's pixels are not staged (device pixels): create it with GPV_IMAGE_GRAIN");
+        return GPV_ERR_INVALID;
+    }
+    DeviceGuard dg(img->ctx->device);
+    if (int rc = grain_alloc(img)) return rc;
+    return grain_launch(img, img->px_dev, img->px_dtype, img->ctx->stream);
+}
+
+int gpv_image_grain(gpv_image *img, double *out3, int32_t *built, float *maps) {
+    if (!img) { set_error("img is NULL"); return GPV_ERR_INVALID; }
+    if (!img->grain) { set_error("the image keeps no grain maps"); return GPV_ERR_INVALID; }
+    DeviceGuard dg(img->ctx->device);
+    double sc[8];
+    GPV_CUDA_TRY(cudaMemcpyAsync(sc, img->grain_scal, sizeof sc, cudaMemcpyDeviceToHost, img->ctx->stream));
+    if (maps)
+        GPV_CUDA_TRY(cudaMemcpyAsync(maps, img->grain, sizeof(float) * 3 * (size_t)img->h * (size_t)img->w,
+                                     cudaMemcpyDeviceToHost, img->ctx->stream));
+    GPV_CUDA_TRY(cudaStreamSynchronize(img->ctx->stream));
+    if (out3) { out3[0] = sc[1]; out3[1] = sc[2]; out3[2] = sc[3]; }
+    if (built) *built = sc[4] != 0.0;
     return GPV_SUCCESS;
 }
 
@@ -848,8 +905,8 @@ int gpv_solve_batch_noalloc(gpv_context *ctx, const gpv_image *f, const gpv_imag
                             void *stream) {
     if (!ctx) { set_error("ctx is NULL"); return GPV_ERR_INVALID; }
     if (int rc = check_pair(f, g, prm)) return rc;
-    if (prm->precision != GPV_PREC_MIXED || (prm->flags & GPV_SOLVE_FAGN)) {
-        set_error("gpv_solve_batch_noalloc runs the mixed-precision ICGN solve only");
+    if (prm->precision != GPV_PREC_MIXED || (prm->flags & (GPV_SOLVE_FAGN | GPV_SOLVE_RIGID_TEXTURE))) {
+        set_error("gpv_solve_batch_noalloc runs the mixed-precision ICGN solve with the deformable template only");
         return GPV_ERR_INVALID;
     }
     if (n < 0 || (n > 0 && (!desc_dev || !out_dev)) || n > INT32_MAX) { set_error("invalid batch arrays"); return GPV_ERR_INVALID; }
@@ -895,7 +952,7 @@ int gpv_mesh_solve(gpv_context *ctx, const gpv_image *f, const gpv_image *g, con
     S.prm.max_iterations = params->max_iterations;
     S.prm.precision = params->precision;
     S.prm.mask = params->mask;
-    S.prm.flags = params->method == 1 ? GPV_SOLVE_FAGN : 0;
+    S.prm.flags = (params->method == 1 ? GPV_SOLVE_FAGN : 0u) | (params->texture == 1 ? GPV_SOLVE_RIGID_TEXTURE : 0u);
     if (int rc = check_pair(f, g, &S.prm)) return rc;
     return gpv::mesh_drive(nodes, n_nodes, elements, n_elements, nodes_per_element, params, gpu_mesh_solver, &S, out,
                            rounds, stats);
@@ -936,7 +993,7 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
     gpv_solve_params p = *prm;
     p.precision = GPV_PREC_MIXED;
     p.history = nullptr;
-    p.flags &= ~(GPV_SOLVE_ETA | GPV_SOLVE_FAGN);  // the tuned kernel is the mixed ICGN one
+    p.flags &= ~(GPV_SOLVE_ETA | GPV_SOLVE_FAGN | GPV_SOLVE_RIGID_TEXTURE);  // the tuned kernel is the mixed ICGN one
     // candidates: threads per block x template layout (compact, 8 x 4 tiles)
     static const int cand[4][2] = {{128, 0}, {256, 0}, {128, 2}, {256, 2}};
     for (int c = 0; c < 3; c++) {

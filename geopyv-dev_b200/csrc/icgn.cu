@@ -373,6 +373,8 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
         o->status = status;
         o->n_px = n;
         o->has_eta = want_eta;
+        o->texture = 0;
+        o->reserved = 0;
     }
 }
 
@@ -606,6 +608,8 @@ __device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
         o->status = status;
         o->n_px = n;
         o->has_eta = want_eta;
+        o->texture = 0;
+        o->reserved = 0;
     }
 }
 
@@ -739,6 +743,19 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
     A.max_norm = prm->max_norm; A.tolerance = prm->tolerance;
     A.max_iter = prm->max_iterations; A.flags = prm->flags;
     A.out = L.out; A.history = L.history;
+    if (prm->flags & GPV_SOLVE_RIGID_TEXTURE) {
+        if (fp64 || (prm->flags & GPV_SOLVE_FAGN) || use_warp_kernel()) {
+            set_error("the rigid-texture template needs the mixed-precision ICGN solve");
+            return GPV_ERR_INVALID;
+        }
+        if (!L.f->grain) {
+            set_error("the rigid-texture template needs the reference image's grain maps "
+                      "(GPV_IMAGE_GRAIN or gpv_image_build_grain)");
+            return GPV_ERR_INVALID;
+        }
+        A.grain = L.f->grain;
+        A.grain_scal = L.f->grain_scal;
+    }
     const int64_t npx_max = ctx->h_tab_n[L.max_radius];
     if (prm->flags & GPV_SOLVE_FAGN) {  // FP64 arithmetic in either precision mode
         if (fp64) {

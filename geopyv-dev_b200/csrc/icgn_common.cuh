@@ -36,6 +36,8 @@ struct KArgs {
     void *scratch;
     int64_t scratch_stride;  // elements (float for mixed, double for fp64) per worker
     int *queue;
+    const float *grain = nullptr;        // rigid texture: f's grain maps (3 x h x w)
+    const double *grain_scal = nullptr;  // [mean, correlation length, s2, corr, built]
 };
 
 namespace {
@@ -349,6 +351,8 @@ __device__ void write_failed_any(gpv_subset_result *out, int idx, const gpv_subs
     o->status = status;
     o->n_px = 0;
     o->has_eta = 0;
+    o->texture = 0;
+    o->reserved = 0;
 }
 
 __device__ void write_failed(const KArgs &A, int idx, const gpv_subset_desc &d, int m, int status, int npx, double fm,
@@ -371,6 +375,8 @@ __device__ void write_failed(const KArgs &A, int idx, const gpv_subset_desc &d, 
     o->status = status;
     o->n_px = npx;
     o->has_eta = 0;
+    o->texture = 0;
+    o->reserved = 0;
 }
 
 // Omitted-mode diagnostic from per-pixel (f, gx, gy, g) held by a worker;

@@ -41,9 +41,11 @@ struct TileSmem {
     double A[12], S[12];
     double p[12], pprev[12], dp[12], grad[12];
     double red[kMaxTileWarps][16];
+    double redt[kMaxTileWarps][16];  // rigid texture: the template pass's warp sums
     double red2[kMaxTileWarps][80];  // setup: one combined reduction
     double tot[16];
-    double misc[8];
+    double tt[16];  // rigid texture: the template pass's block sums
+    double misc[10];
     int flag[4];
     int item;
     int n_valid;
@@ -193,9 +195,40 @@ __device__ __forceinline__ void unpack_off(float w, float &dx, float &dy) {
     dy = (float)(v >> 16);
 }
 
-template <int ORDER, int NT>
+// The three grain maps (fxx, fyy, fxy; rows x cols FP32) at (x = column,
+// y = row), bilinear, clamped (GrainMaps::sample, src/texture.rs:125-143).
+__device__ __forceinline__ void grain_sample(const float *maps, int rows, int cols, double x, double y, float h[3]) {
+    x = fmin(fmax(x, 0.0), (double)(cols - 1));
+    y = fmin(fmax(y, 0.0), (double)(rows - 1));
+    const int x0 = min((int)floor(x), max(cols - 2, 0)), y0 = min((int)floor(y), max(rows - 2, 0));
+    const int x1 = min(x0 + 1, cols - 1), y1 = min(y0 + 1, rows - 1);
+    const double tx = x - (double)x0, ty = y - (double)y0;
+    const int64_t np = (int64_t)rows * cols;
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+        const float *M = maps + m * np;
+        h[m] = (float)((1.0 - ty) * ((1.0 - tx) * M[(int64_t)y0 * cols + x0] + tx * M[(int64_t)y0 * cols + x1]) +
+                       ty * ((1.0 - tx) * M[(int64_t)y1 * cols + x0] + tx * M[(int64_t)y1 * cols + x1]));
+    }
+}
+
+// Green-Lagrange strain [Exx, Eyy, Exy] (src/texture.rs:200-206).
+__device__ __forceinline__ void green_lagrange(float ux, float vx, float uy, float vy, float &e0, float &e1, float &e2) {
+    e0 = ux + 0.5f * (ux * ux + vx * vx);
+    e1 = vy + 0.5f * (uy * uy + vy * vy);
+    e2 = 0.5f * (uy + vx) + 0.5f * (ux * uy + vx * vy);
+}
+
+// RIGID: the rigid-texture template (Texture::Rigid) when the reference image
+// has measurable speckle: the maps at the subset pixels in setup (Sh: 3
+// arrays of n_max), and every iteration a template pass storing
+// t = f + G(E(p)) per pixel (St) with its warp sums, so the update compares
+// g with the template (src/subset.rs:1151-1168, grain_template
+// src/texture.rs:213-244): t - t_m in the cross term and the gradient, the
+// template's spread instead of delta_f.
+template <int ORDER, int NT, bool RIGID>
 __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d, float4 *S4, float *Sg, float *win,
-                            TileSmem &sm) {
+                            TileSmem &sm, float *Sh, float *St, int64_t nmax) {
     const KArgs &A = T.k;
     using O = Ord<ORDER>;
     constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM;
@@ -211,6 +244,8 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
     const int bx = (int)fxd, by = (int)fyd;
     const float fx = (float)(cx - fxd), fy = (float)(cy - fyd);
     const int B = A.border, ch = A.h + 2 * B;
+    const bool rigid_on = RIGID && A.grain_scal[4] != 0.0;  // uniform: maps built
+    const float s2f = RIGID ? (float)A.grain_scal[2] : 0.f;
 
     // ---- stage f's window ------------------------------------------------
     {
@@ -287,6 +322,13 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                 }
             }
             S4[i] = pack_px(f, gx, gy, o.x, o.y);
+            if (RIGID && rigid_on) {
+                float hv[3];
+                grain_sample(A.grain, A.h, A.w, cx + (double)o.x, cy + (double)o.y, hv);
+                Sh[i] = hv[0];
+                Sh[nmax + i] = hv[1];
+                Sh[2 * nmax + i] = hv[2];
+            }
             const float dx = (float)o.x, dy = (float)o.y;
             const float fs = f - shift;
             acc[0] += 1.f;
@@ -449,6 +491,48 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         }
         // window-relative base: sample (ix, iy) reads win[(iy + B-2 - r0) * ww + (ix + B-2 - c0)]
         const int offx = B - 2 - gc0, offy = B - 2 - gr0;
+        if (RIGID && rigid_on) {
+            // template pass: t per pixel, sums of t - f_m, (t - f_m)^2 and
+            // SDI_j (t - f_m) (their warp sums meet the iteration's reduction)
+            constexpr int NT_ = 2 + M;
+            float ta[NT_];
+#pragma unroll
+            for (int q = 0; q < NT_; q++) ta[q] = 0.f;
+            float e0u = 0.f, e1u = 0.f, e2u = 0.f;
+            if (ORDER == 1) green_lagrange(ux, vx, uy, vy, e0u, e1u, e2u);
+            const float q6 = ORDER == 2 ? (float)sm.p[6 % M] : 0.f, q7 = ORDER == 2 ? (float)sm.p[7 % M] : 0.f;
+            const float q8 = ORDER == 2 ? (float)sm.p[8 % M] : 0.f, q9 = ORDER == 2 ? (float)sm.p[9 % M] : 0.f;
+            const float q10 = ORDER == 2 ? (float)sm.p[10 % M] : 0.f, q11 = ORDER == 2 ? (float)sm.p[11 % M] : 0.f;
+            for (int i = tid; i < npx_t; i += NT) {
+                const float4 rec = S4[i];
+                if (rec.x != rec.x) continue;
+                float dx, dy;
+                unpack_off(rec.w, dx, dy);
+                float e0 = e0u, e1 = e1u, e2 = e2u;
+                if (ORDER == 2)
+                    green_lagrange(ux + q6 * dx + q8 * dy, vx + q7 * dx + q9 * dy, uy + q8 * dx + q10 * dy,
+                                   vy + q9 * dx + q11 * dy, e0, e1, e2);
+                const float h0 = Sh[i], h1 = Sh[nmax + i], h2 = Sh[2 * nmax + i];
+                const float f = rec.x;
+                const float t = f + (-0.5f * s2f * (e0 * h0 + e1 * h1 + 2.0f * e2 * h2) - (e0 + e1) * (f - fmf));
+                St[i] = t;
+                const float ts = t - fmf;
+                ta[0] += ts;
+                ta[1] = fmaf(ts, ts, ta[1]);
+                const float gxt = rec.y * ts, gyt = rec.z * ts;
+#pragma unroll
+                for (int mu = 0; mu < NMU; mu++) {
+                    const float mv = mu_val<float>(mu, dx, dy);
+                    ta[2 + 2 * mu] = fmaf(gxt, mv, ta[2 + 2 * mu]);
+                    ta[3 + 2 * mu] = fmaf(gyt, mv, ta[3 + 2 * mu]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NT_; q++) {
+                const double tq = warp_sum((double)ta[q]);
+                if (lane == 0) sm.redt[wid][q] = tq;
+            }
+        }
         double s1 = 0.0, s2 = 0.0, sfg = 0.0;
         float pb[M];
 #pragma unroll
@@ -491,7 +575,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                         const float gc = g - fmf;
                         p1 += gc;
                         p2 = fmaf(gc, gc, p2);
-                        pfg = fmaf(fv - fmf, gc, pfg);
+                        pfg = fmaf((RIGID && rigid_on ? St[i] : fv) - fmf, gc, pfg);
                         const float gxg = rec.y * gc, gyg = rec.z * gc;
                         pb[0] += gxg;
                         pb[1] += gyg;
@@ -533,6 +617,12 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                 for (int w = 0; w < NT / 32; w++) t += sm.red[w][lane];
                 sm.tot[lane] = t;
             }
+            if (RIGID && rigid_on && lane < 2 + M) {
+                double t = 0.0;
+#pragma unroll
+                for (int w = 0; w < NT / 32; w++) t += sm.redt[w][lane];
+                sm.tt[lane] = t;
+            }
             __syncwarp();
         }
         // (all threads read tot only after the update barrier below)
@@ -541,10 +631,25 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             gmt = sm.tot[0] / dn;
             const double dg2 = sm.tot[1] - sm.tot[0] * gmt;
             dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
-            const double sab = sm.tot[2] - gmt * sa;
-            znssd = 2.0 - 2.0 * sab / (df * dg);
-            const double ratio = df / dg;
-            if (lane < M) sm.grad[lane] = sm.A[lane] - ratio * (sm.tot[3 + lane] - gmt * sm.S[lane]);
+            double sab, dref = df, tmf = 0.0;
+            if (RIGID && rigid_on) {  // the template: t_m = f_m + tmf, spread dref
+                tmf = sm.tt[0] / dn;
+                const double dt2 = sm.tt[1] - sm.tt[0] * tmf;
+                dref = sqrt(dt2 > 0.0 ? dt2 : 0.0);
+                sab = sm.tot[2] - tmf * sm.tot[0];
+            } else {
+                sab = sm.tot[2] - gmt * sa;
+            }
+            znssd = 2.0 - 2.0 * sab / (dref * dg);
+            const double ratio = dref / dg;
+            if (lane < M) {
+                const double aj = (RIGID && rigid_on) ? sm.tt[2 + lane] - tmf * sm.S[lane] : sm.A[lane];
+                sm.grad[lane] = aj - ratio * (sm.tot[3 + lane] - gmt * sm.S[lane]);
+            }
+            if (lane == 0) {
+                sm.misc[8] = tmf;
+                sm.misc[9] = dref;
+            }
             __syncwarp();
             if (lane < M) {
                 double acc = 0.0;
@@ -640,11 +745,13 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             if (rec.x != rec.x) return false;
             float dxf, dyf;
             unpack_off(rec.w, dxf, dyf);
-            f = rec.x; gx = rec.y; gy = rec.z; g = Sg[i]; dx = dxf; dy = dyf;
+            f = (RIGID && rigid_on) ? St[i] : rec.x;  // the template fitted at the last iteration
+            gx = rec.y; gy = rec.z; g = Sg[i]; dx = dxf; dy = dyf;
             return true;
         };
         auto red = [&](double v) { return block_sum1<NT>(v, sm); };
-        eta_sums<ORDER>(npx_t, tid, NT, dn, fm, df, gm_last, dg_last, load, red, eu, ev);
+        const double fm_e = (RIGID && rigid_on) ? fm + sm.misc[8] : fm, df_e = (RIGID && rigid_on) ? sm.misc[9] : df;
+        eta_sums<ORDER>(npx_t, tid, NT, dn, fm_e, df_e, gm_last, dg_last, load, red, eu, ev);
     }
     if (tid == 0) {
         gpv_subset_result *o = A.out + idx;
@@ -665,6 +772,8 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         o->status = status;
         o->n_px = n;
         o->has_eta = want_eta;
+        o->texture = (RIGID && rigid_on) ? 1 : 0;
+        o->reserved = 0;
     }
 }
 
@@ -691,13 +800,14 @@ __device__ int claim_slot(const TileArgs &T) {
 // PER_SUBSET: one block per subset with a claimed scratch slot, else a
 // persistent grid taking subsets from the queue (two instantiations, so
 // each holds one inlined copy of the solve).
-template <int ORDER, int NT, bool PER_SUBSET>
+template <int ORDER, int NT, bool PER_SUBSET, bool RIGID>
 __global__ void __launch_bounds__(NT, 512 / NT) icgn_tile(TileArgs T) {
     extern __shared__ float4 win4[];
     float *win = reinterpret_cast<float *>(win4);
     __shared__ TileSmem sm;
     const KArgs &A = T.k;
-    const int64_t nmax = A.scratch_stride / 5;
+    // per pixel: float4 record, eta sample (+ 3 grain samples, template value)
+    const int64_t nmax = A.scratch_stride / (RIGID ? 9 : 5);
     const int start = T.seg[0], count = T.seg[1];
     if (PER_SUBSET) {
         const int item = blockIdx.x;
@@ -716,7 +826,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) icgn_tile(TileArgs T) {
         if (d.radius < 1 || d.radius > A.max_radius) {
             if (threadIdx.x == 0) write_failed(A, idx, d, 12, GPV_INVALID_SUBSET, 0, 0.0, 0.0);
         } else {
-            tile_subset<ORDER, NT>(T, idx, d, reinterpret_cast<float4 *>(base), base + 4 * nmax, win, sm);
+            tile_subset<ORDER, NT, RIGID>(T, idx, d, reinterpret_cast<float4 *>(base), base + 4 * nmax, win, sm,
+                                          base + 5 * nmax, base + 8 * nmax, nmax);
         }
         __threadfence();  // every scratch access of the block is done before the slot is free
         __syncthreads();
@@ -741,7 +852,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) icgn_tile(TileArgs T) {
             if (threadIdx.x == 0) write_failed(A, idx, d, 12, GPV_INVALID_SUBSET, 0, 0.0, 0.0);
             continue;
         }
-        tile_subset<ORDER, NT>(T, idx, d, S4, Sg, win, sm);
+        tile_subset<ORDER, NT, RIGID>(T, idx, d, S4, Sg, win, sm, base + 5 * nmax, base + 8 * nmax, nmax);
     }
 }
 
@@ -814,26 +925,44 @@ __global__ void scatter_orders(const gpv_subset_desc *desc, const int32_t *order
     }
 }
 
+// Instantiations: every (order, threads, per-subset) for the deformable
+// template; the rigid texture (orders 1 and 2) on persistent grids only.
 template <int NT, bool PS>
 const void *tile_kernel_t(int order) {
-    return order == 2 ? (const void *)icgn_tile<2, NT, PS>
-                      : (order == 1 ? (const void *)icgn_tile<1, NT, PS> : (const void *)icgn_tile<0, NT, PS>);
+    return order == 2 ? (const void *)icgn_tile<2, NT, PS, false>
+                      : (order == 1 ? (const void *)icgn_tile<1, NT, PS, false> : (const void *)icgn_tile<0, NT, PS, false>);
 }
 
-const void *tile_kernel(int nt, bool per_subset, int order) {
+template <int NT>
+const void *tile_kernel_rigid(int order) {
+    return order == 2 ? (const void *)icgn_tile<2, NT, false, true> : (const void *)icgn_tile<1, NT, false, true>;
+}
+
+const void *tile_kernel(int nt, bool per_subset, int order, bool rigid) {
+    if (rigid) return nt == 256 ? tile_kernel_rigid<256>(order) : tile_kernel_rigid<128>(order);
     if (nt == 256) return per_subset ? tile_kernel_t<256, true>(order) : tile_kernel_t<256, false>(order);
     return per_subset ? tile_kernel_t<128, true>(order) : tile_kernel_t<128, false>(order);
 }
 
 template <int NT, bool PS>
 void tile_launch_t(int order, int blocks, size_t smem, cudaStream_t s, const TileArgs &T) {
-    if (order == 2) icgn_tile<2, NT, PS><<<blocks, NT, smem, s>>>(T);
-    else if (order == 1) icgn_tile<1, NT, PS><<<blocks, NT, smem, s>>>(T);
-    else icgn_tile<0, NT, PS><<<blocks, NT, smem, s>>>(T);
+    if (order == 2) icgn_tile<2, NT, PS, false><<<blocks, NT, smem, s>>>(T);
+    else if (order == 1) icgn_tile<1, NT, PS, false><<<blocks, NT, smem, s>>>(T);
+    else icgn_tile<0, NT, PS, false><<<blocks, NT, smem, s>>>(T);
 }
 
-void tile_launch_one(int nt, bool per_subset, int order, int blocks, size_t smem, cudaStream_t s, const TileArgs &T) {
-    if (nt == 256) {
+template <int NT>
+void tile_launch_rigid(int order, int blocks, size_t smem, cudaStream_t s, const TileArgs &T) {
+    if (order == 2) icgn_tile<2, NT, false, true><<<blocks, NT, smem, s>>>(T);
+    else icgn_tile<1, NT, false, true><<<blocks, NT, smem, s>>>(T);
+}
+
+void tile_launch_one(int nt, bool per_subset, int order, bool rigid, int blocks, size_t smem, cudaStream_t s,
+                     const TileArgs &T) {
+    if (rigid) {
+        if (nt == 256) tile_launch_rigid<256>(order, blocks, smem, s, T);
+        else tile_launch_rigid<128>(order, blocks, smem, s, T);
+    } else if (nt == 256) {
         if (per_subset) tile_launch_t<256, true>(order, blocks, smem, s, T);
         else tile_launch_t<256, false>(order, blocks, smem, s, T);
     } else {
@@ -920,6 +1049,7 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
     GPV_CUDA_TRY(cudaGetLastError());
     struct Plan {
         int rmax = 0, nt = 0, layout = 0, cap = 0, blocks = 0, per_sm = 0;
+        bool ps = false, rigid = false;  // one block per subset; rigid-texture template
         int64_t stride = 0;
         bool live = false;
     };
@@ -932,14 +1062,17 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         const int order = 2 - q / kRClasses, c = q % kRClasses;
         const int lo = c == 0 ? 0 : kRBoundHost[c - 1];
         Plan &P = plan[q];
-        P.live = lo < K.max_radius && ((ctx->seg_mask >> q) & 1u) && (!per_subset || ctx->seg_count[q] > 0);
+        // the rigid template runs on persistent grids (orders 1 and 2)
+        P.rigid = (K.flags & GPV_SOLVE_RIGID_TEXTURE) && order >= 1;
+        P.ps = per_subset && !P.rigid;
+        P.live = lo < K.max_radius && ((ctx->seg_mask >> q) & 1u) && (!P.ps || ctx->seg_count[q] > 0);
         if (!P.live) continue;
         P.rmax = std::min(kRBoundHost[c], K.max_radius);
         P.nt = tile_threads_for(ctx, P.rmax);
         P.layout = tile_layout_for(ctx, P.rmax);
         P.cap = window_cap(P.rmax, P.layout);
         const size_t smem = sizeof(float) * P.cap;
-        const void *fn = tile_kernel(P.nt, per_subset, order);
+        const void *fn = tile_kernel(P.nt, P.ps, order, P.rigid);
         if (int rc = allow_max_dynamic_smem(fn)) return rc;
         int per_sm = 0;
         GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, P.nt, smem));
@@ -947,9 +1080,9 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         if (per_sm > 32) per_sm = 32;  // slot claim words have 32 bits (never reached: 4 blocks of 128 threads)
         P.per_sm = per_sm;
         const int64_t nmax = (int64_t)(ctx->h_slot_n[P.rmax] + 31) / 32 * 32;
-        P.stride = 5 * nmax;  // float4 record + eta sample per pixel
+        P.stride = (P.rigid ? 9 : 5) * nmax;  // float4 record + eta sample (+ 3 grain samples, template) per pixel
         int64_t slots;
-        if (per_subset) {
+        if (P.ps) {
             P.blocks = (int)ctx->seg_count[q];
             slots = (int64_t)per_sm * ctx->n_smid;
         } else {
@@ -970,7 +1103,7 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         // segment's tail overlaps the next one's start; per-subset blocks have
         // no long tail and stay on the caller's stream (fewer streams share
         // the device's hardware queues with other contexts' work)
-        const int k = per_subset ? 0 : next;
+        const int k = P.ps ? 0 : next;
         next = (next + 1) % 3;
         if (!used[k]) {
             GPV_CUDA_TRY(cudaStreamWaitEvent(st[k], ctx->ev[0], 0));
@@ -986,11 +1119,11 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         T.queue = queues + q;
         T.k.scratch = static_cast<float *>(ctx->scratch.ptr) + (int64_t)k * region;
         T.k.scratch_stride = P.stride;
-        T.slot_mask = per_subset ? static_cast<uint32_t *>(ctx->slot_mask.ptr) + (int64_t)k * ctx->n_smid : nullptr;
+        T.slot_mask = P.ps ? static_cast<uint32_t *>(ctx->slot_mask.ptr) + (int64_t)k * ctx->n_smid : nullptr;
         T.slots_per_sm = P.per_sm;
         T.n_mask = ctx->n_smid;
         const size_t smem = sizeof(float) * P.cap;
-        tile_launch_one(P.nt, per_subset, 2 - q / kRClasses, P.blocks, smem, st[k], T);
+        tile_launch_one(P.nt, P.ps, 2 - q / kRClasses, P.rigid, P.blocks, smem, st[k], T);
         GPV_CUDA_TRY(cudaGetLastError());
     }
     for (int k = 1; k < 3; k++) {

@@ -353,6 +353,8 @@ __device__ void mixed_subset(const KArgs &A, int idx, const gpv_subset_desc &d, 
         o->status = status;
         o->n_px = n;
         o->has_eta = want_eta;
+        o->texture = 0;
+        o->reserved = 0;
     }
 }
 

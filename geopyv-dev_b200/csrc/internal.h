@@ -120,6 +120,13 @@ struct gpv_image {
     size_t px_bytes = 0;
     uint8_t *rgb_dev = nullptr;  // staging for colour pixels (h * w * 3)
     uint32_t flags = 0;
+    int32_t px_dtype = -1;     // pixel type of px_dev
+    bool px_current = false;   // px_dev holds the pixels behind the coefficients
+    // rigid-texture speckle statistics (grain.cu): fxx, fyy, fxy maps (3 h w
+    // FP32) and [mean, correlation length, s2, corr, built] on the device
+    float *grain = nullptr;
+    double *grain_scal = nullptr;
+    double *grain_ac = nullptr;  // autocorrelation lag sums (2 x 256)
 };
 
 struct gpv_mask {
@@ -131,6 +138,11 @@ struct gpv_mask {
 namespace gpv {
 // prefilter.cu
 int prefilter_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s);
+// New pixels into an image: prefilter, and the grain maps when it keeps them.
+// staged: px_dev is the image's own staging (it then holds the pixels).
+int image_pixels_in(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s, bool staged);
+// grain.cu: correlation length, s2, corr and the three maps of img from its pixels
+int grain_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s);
 // icgn.cu
 struct SolveLaunch {
     const gpv_image *f, *g;

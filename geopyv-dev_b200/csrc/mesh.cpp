@@ -372,6 +372,10 @@ int mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements, in
         set_error("mesh solves use subset_order 1 or 2 and radius >= 1");
         return GPV_ERR_INVALID;
     }
+    if (mp->texture != 0 && mp->texture != 1) {
+        set_error("texture must be 0 (deformable) or 1 (rigid)");
+        return GPV_ERR_INVALID;
+    }
     if (mp->method != 0 && mp->method != 1) {
         set_error("method must be 0 (ICGN) or 1 (FAGN)");
         return GPV_ERR_INVALID;

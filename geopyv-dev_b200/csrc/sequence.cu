@@ -59,7 +59,7 @@ namespace {
 int frame_work(gpv_sequence *s, bool seed) {
     gpv_context *ctx = s->ctx;
     cudaStream_t st = ctx->stream;
-    if (int rc = prefilter_launch(s->g, s->px_dev, s->dtype, st)) return rc;
+    if (int rc = image_pixels_in(s->g, s->px_dev, s->dtype, st, false)) return rc;
     if (seed) {
         seed_from_previous<<<(unsigned)((s->n + 255) / 256), 256, 0, st>>>(s->desc_dev, s->out_dev, (int)s->n);
         GPV_CUDA_TRY(cudaGetLastError());

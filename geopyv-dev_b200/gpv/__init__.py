@@ -96,7 +96,8 @@ class Image:
     ``Image(image_gs=array, border=20)`` as python/src/py_image.rs:42-64 (the
     coefficients are computed on the GPU: Image::from_array -> get_c,
     src/image.rs:83-86, :252-327).  ``keep_f64`` keeps an FP64 copy of the
-    coefficients for the FP64 solver.
+    coefficients for the FP64 solver; ``grain`` keeps the rigid-texture grain
+    maps (GrainMaps, src/texture.rs:31-143), rebuilt with every update.
 
     ``Image(image_rgb=array)`` takes decoded 8-bit colour pixels (h, w, 3) in
     RGB order and applies Image::from_file's pre-processing on the device
@@ -108,7 +109,7 @@ class Image:
     """
 
     def __init__(self, filepath=None, image_gs=None, border: int = 20, keep_f64: bool = False, ctx: Context | None = None,
-                 image_rgb=None):
+                 image_rgb=None, grain: bool = False):
         given = [v is not None for v in (filepath, image_gs, image_rgb)]
         if sum(given) > 1:
             raise ValueError("supply exactly one of `filepath`, `image_gs` or `image_rgb`")
@@ -126,7 +127,7 @@ class Image:
         self.ctx = ctx or default_context()
         self.border = border
         h = ct.c_void_p()
-        flags = _lib.IMAGE_KEEP_F64 if keep_f64 else 0
+        flags = (_lib.IMAGE_KEEP_F64 if keep_f64 else 0) | (_lib.IMAGE_GRAIN if grain else 0)
         if image_rgb is not None:
             rgb = np.ascontiguousarray(image_rgb, dtype=np.uint8)
             if rgb.ndim != 3 or rgb.shape[2] != 3:
@@ -155,6 +156,25 @@ class Image:
         out = np.empty(self.shape, np.uint8)
         check(lib().gpv_image_grey(self._h, ptr(out)), "gpv_image_grey")
         return out.astype(np.float64)
+
+    def build_grain(self) -> None:
+        """Build (once) and keep the rigid-texture grain maps of this image
+        (gpv_image_build_grain); a solve with texture="rigid" calls it on the
+        reference image."""
+        check(lib().gpv_image_build_grain(self._h), "gpv_image_build_grain")
+
+    def grain(self, maps: bool = False) -> dict:
+        """The grain statistics: correlation length, s2, smoothing correction,
+        whether the image has measurable speckle, and (maps=True) the
+        (3, h, w) FP32 maps fxx, fyy, fxy."""
+        out = (ct.c_double * 3)()
+        built = ct.c_int32()
+        m = np.empty((3,) + tuple(self.shape), np.float32) if maps else None
+        check(lib().gpv_image_grain(self._h, out, ct.byref(built), ptr(m)), "gpv_image_grain")
+        r = dict(correlation_length=out[0], s2=out[1], corr=out[2], built=bool(built.value))
+        if maps:
+            r["maps"] = m
+        return r
 
     def update_rgb(self, image_rgb) -> None:
         """Ingest and prefilter new colour pixels of the same shape in place."""
@@ -274,10 +294,14 @@ def make_desc(coords, radius, order, p0=None) -> np.ndarray:
     return d
 
 
-def _params(max_norm, max_iterations, tolerance, eta, precision, mask, history_buf, method="icgn"):
+def _params(max_norm, max_iterations, tolerance, eta, precision, mask, history_buf, method="icgn",
+            texture="deformable"):
     if method not in ("icgn", "fagn"):
         raise ValueError(f"method must be 'icgn' or 'fagn', got {method!r}")
-    flags = (SOLVE_ETA if eta else 0) | (_lib.SOLVE_FAGN if method == "fagn" else 0)
+    if texture not in ("deformable", "rigid"):  # check_texture (python/src/py_mesh.rs:954-961)
+        raise ValueError(f"texture must be 'deformable' or 'rigid', got {texture!r}")
+    flags = (SOLVE_ETA if eta else 0) | (_lib.SOLVE_FAGN if method == "fagn" else 0) | \
+        (_lib.SOLVE_RIGID_TEXTURE if texture == "rigid" else 0)
     return SolveParams(max_norm=max_norm, tolerance=tolerance, max_iterations=max_iterations,
                        flags=flags, precision=precision, reserved=0,
                        mask=(mask.handle if mask is not None else None),
@@ -285,13 +309,18 @@ def _params(max_norm, max_iterations, tolerance, eta, precision, mask, history_b
 
 
 def solve_batch(f_img: Image, g_img: Image, desc, max_norm=1e-5, max_iterations=50, tolerance=0.75, eta=False,
-                precision=PREC_MIXED, global_mask: Mask | None = None, history=False, method="icgn"):
+                precision=PREC_MIXED, global_mask: Mask | None = None, history=False, method="icgn",
+                texture="deformable"):
     """Batched Subset::new + solve_icgn_result on the GPU; returns a RESULT_DTYPE array
-    (and the (n, max_iterations, 3) history of (norm, zncc, znssd) when asked)."""
+    (and the (n, max_iterations, 3) history of (norm, zncc, znssd) when asked).
+    texture="rigid" fits the rigid-texture template (its ``texture`` field
+    says whether a subset did)."""
     desc = np.ascontiguousarray(desc, dtype=DESC_DTYPE)
     out = np.zeros(desc.size, RESULT_DTYPE)
     hist = np.zeros((desc.size, max(max_iterations, 1), 3)) if history else None
-    prm = _params(max_norm, max_iterations, tolerance, eta, precision, global_mask, hist, method)
+    prm = _params(max_norm, max_iterations, tolerance, eta, precision, global_mask, hist, method, texture)
+    if texture == "rigid":
+        f_img.build_grain()
     check(lib().gpv_solve_batch(f_img.ctx.handle, f_img.handle, g_img.handle, ptr(desc), desc.size,
                                 ct.byref(prm), ptr(out)), "gpv_solve_batch")
     return (out, hist) if history else out
@@ -330,21 +359,23 @@ class Subset:
         self.solved = False
 
     def solve(self, p_0=None, solver=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED,
-              algorithm=None):
-        """Subset.solve: ``algorithm`` (or ``solver``) "icgn" (default) or "fagn"."""
+              algorithm=None, texture="deformable"):
+        """Subset.solve: ``algorithm`` (or ``solver``) "icgn" (default) or "fagn";
+        ``texture`` "deformable" (default) or "rigid"."""
         method = algorithm or solver or "icgn"
         if method not in ("icgn", "fagn"):
             raise ValueError(f"algorithm must be 'icgn' or 'fagn', got {method!r}")
-        self._solve(method, p_0, max_norm, max_iterations, tolerance, precision)
+        self._solve(method, p_0, max_norm, max_iterations, tolerance, precision, texture)
 
-    def solve_icgn(self, p_0=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED):
-        self._solve("icgn", p_0, max_norm, max_iterations, tolerance, precision)
+    def solve_icgn(self, p_0=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED,
+                   texture="deformable"):
+        self._solve("icgn", p_0, max_norm, max_iterations, tolerance, precision, texture)
 
     def solve_fagn(self, p_0=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED):
         """Forward additive Gauss-Newton (Subset::solve_fagn, src/subset.rs:1011-1020, 1228-1334)."""
         self._solve("fagn", p_0, max_norm, max_iterations, tolerance, precision)
 
-    def _solve(self, method, p_0, max_norm, max_iterations, tolerance, precision):
+    def _solve(self, method, p_0, max_norm, max_iterations, tolerance, precision, texture="deformable"):
         m = {0: 2, 1: 6, 2: 12}[self.subset_order]
         p0 = np.zeros(m)
         if p_0 is not None:  # resized to the order's length (src/subset.rs:1134-1136)
@@ -353,7 +384,7 @@ class Subset:
         d = make_desc([self.coord], self.local_mask.size, self.subset_order, p0[None, :])
         out, hist = solve_batch(self.f_img, self.g_img, d, max_norm=max_norm, max_iterations=max_iterations,
                                 tolerance=tolerance, eta=True, precision=precision, global_mask=self.global_mask,
-                                history=True, method=method)
+                                history=True, method=method, texture=texture)
         r = out[0]
         st = int(r["status"])
         if st in (1, 2):  # Subset::new errors (src/subset.rs:853-892) -> RuntimeError (python/src/lib.rs:18-38)
@@ -380,6 +411,8 @@ class Subset:
 
     c_zncc = property(lambda s: float(s._get("c_zncc")))
     c_znssd = property(lambda s: float(s._get("c_znssd")))
+    # SolveResult::texture: the template the solve fitted
+    texture = property(lambda s: "rigid" if int(s._get("texture")) else "deformable")
     iterations = property(lambda s: int(s._get("iterations")))
     converged = property(lambda s: bool(s._get("converged")))
     quality_ok = property(lambda s: bool(s._get("quality_ok")))

@@ -22,9 +22,9 @@ RESULT_DTYPE = np.dtype([
     ("p", "<f8", (12,)), ("c_zncc", "<f8"), ("c_znssd", "<f8"), ("norm", "<f8"),
     ("eta_u", "<f8"), ("eta_v", "<f8"), ("f_m", "<f8"), ("delta_f", "<f8"), ("sssig", "<f8"),
     ("sigma", "<f8"), ("iterations", "<i4"), ("converged", "<i4"), ("quality_ok", "<i4"),
-    ("status", "<i4"), ("n_px", "<i4"), ("has_eta", "<i4"),
+    ("status", "<i4"), ("n_px", "<i4"), ("has_eta", "<i4"), ("texture", "<i4"), ("reserved", "<i4"),
 ])
-assert DESC_DTYPE.itemsize == 120 and RESULT_DTYPE.itemsize == 192
+assert DESC_DTYPE.itemsize == 120 and RESULT_DTYPE.itemsize == 200
 
 
 class SolveParams(ct.Structure):
@@ -43,7 +43,8 @@ class MeshParams(ct.Structure):
                 ("max_norm", ct.c_double), ("tolerance", ct.c_double), ("root_rel_eps", ct.c_double),
                 ("max_iterations", ct.c_int32), ("subset_order", ct.c_int32), ("radius", ct.c_int32),
                 ("precision", ct.c_int32), ("layer_rg", ct.c_int32), ("batch_factor", ct.c_int32),
-                ("max_workers", ct.c_int32), ("method", ct.c_int32), ("mask", ct.c_void_p),
+                ("max_workers", ct.c_int32), ("method", ct.c_int32), ("texture", ct.c_int32),
+                ("reserved", ct.c_int32), ("mask", ct.c_void_p),
                 ("progress", PROGRESS_FN), ("progress_user", ct.c_void_p)]
 
 
@@ -52,7 +53,7 @@ class MeshStats(ct.Structure):
                 ("retries", ct.c_int64), ("rounds", ct.c_int64), ("seed_node", ct.c_int64)]
 
 
-assert ct.sizeof(MeshParams) == 200 and ct.sizeof(MeshStats) == 56
+assert ct.sizeof(MeshParams) == 208 and ct.sizeof(MeshStats) == 56
 
 EXECUTOR_FN = ct.CFUNCTYPE(ct.c_int, ct.c_void_p, ct.c_int32, ct.c_void_p, ct.c_void_p, ct.c_void_p)
 
@@ -84,8 +85,8 @@ CONTEXT_HIGH_PRIORITY, CONTEXT_PER_SUBSET_BLOCKS = 1, 2
 # enums
 GPV_U8, GPV_U16, GPV_F32, GPV_F64 = 1, 2, 3, 4
 PREC_MIXED, PREC_FP64 = 0, 1
-SOLVE_ETA, SOLVE_HISTORY, SOLVE_FAGN = 1, 2, 4
-IMAGE_KEEP_F64 = 1
+SOLVE_ETA, SOLVE_HISTORY, SOLVE_FAGN, SOLVE_RIGID_TEXTURE = 1, 2, 4, 8
+IMAGE_KEEP_F64, IMAGE_GRAIN = 1, 2
 STATUS = {0: "OK", 1: "EMPTY_MASK", 2: "FEATURELESS", 3: "SINGULAR_H", 4: "SINGULAR_WDELTA", 5: "NONFINITE",
           6: "TIMEOUT", 7: "CANCELLED", 8: "INVALID_SUBSET"}
 DTYPES = {np.dtype(np.uint8): GPV_U8, np.dtype(np.uint16): GPV_U16, np.dtype(np.float32): GPV_F32,
@@ -106,6 +107,8 @@ SIGNATURES = {
     "gpv_image_create_device": (ct.c_int, [P, P, I32, I64, I64, I32, U32, P]),
     "gpv_image_update_device": (ct.c_int, [P, P, I32]),
     "gpv_image_update": (ct.c_int, [P, P, I32]),
+    "gpv_image_build_grain": (ct.c_int, [P]),
+    "gpv_image_grain": (ct.c_int, [P, P, P, P]),
     "gpv_image_destroy": (ct.c_int, [P]),
     "gpv_image_shape": (ct.c_int, [P, P, P, P]),
     "gpv_image_coefficients_f32": (ct.c_int, [P, P]),

@@ -23,7 +23,8 @@ from ._lib import DESC_DTYPE, PREC_MIXED, RESULT_DTYPE, GpvError, MeshParams, Me
 
 
 def _mesh_params(radius, seed_coord, seed_warp, seed_tolerance, max_norm, max_iterations, subset_order, tolerance,
-                 preconditioning, batch_factor, root_rel_eps, max_workers, precision, mask, progress, method="icgn"):
+                 preconditioning, batch_factor, root_rel_eps, max_workers, precision, mask, progress, method="icgn",
+                 texture="deformable"):
     if subset_order not in (1, 2):
         raise ValueError("subset_order must be 1 or 2 for a mesh (p_len = 6 * subset_order)")
     if preconditioning not in ("RG", "layer-RG"):
@@ -40,6 +41,9 @@ def _mesh_params(radius, seed_coord, seed_warp, seed_tolerance, max_norm, max_it
     if method not in ("icgn", "fagn"):
         raise ValueError(f"method must be 'icgn' or 'fagn', got {method!r}")
     m.method = 1 if method == "fagn" else 0
+    if texture not in ("deformable", "rigid"):  # check_texture (python/src/py_mesh.rs:954-961)
+        raise ValueError(f"texture must be 'deformable' or 'rigid', got {texture!r}")
+    m.texture = 1 if texture == "rigid" else 0
     m.layer_rg = int(preconditioning == "layer-RG")
     m.batch_factor = batch_factor
     # layer_rg_max_workers=None: the reference sizes rounds by its global
@@ -135,12 +139,14 @@ class Mesh:
               layer_rg_max_workers=None, precision=PREC_MIXED, progress=None):
         """Mesh.solve (python/src/py_mesh.rs:215-291).  `local_mask` is a
         ``gpv.Mask("local", shape="circle", size=r)`` or the radius itself."""
-        if masking != "uniform" or texture != "deformable":
-            raise NotImplementedError("only masking='uniform', texture='deformable' run on the GPU")
+        if masking != "uniform":
+            raise NotImplementedError("only masking='uniform' runs on the GPU")
         radius = int(getattr(local_mask, "size", local_mask))
         m, keep = _mesh_params(radius, seed_coord, seed_warp, seed_tolerance, max_norm, max_iterations, subset_order,
                                tolerance, preconditioning, layer_rg_batch_factor, layer_rg_root_rel_eps,
-                               layer_rg_max_workers, precision, self.mask, progress, method)
+                               layer_rg_max_workers, precision, self.mask, progress, method, texture)
+        if texture == "rigid":
+            self.f_img.build_grain()
         out = np.zeros(len(self.nodes), RESULT_DTYPE)
         rounds = np.zeros(len(self.nodes), np.int32)
         st = MeshStats()

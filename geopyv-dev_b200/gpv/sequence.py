@@ -116,11 +116,11 @@ class Sequence:
         self.border, self.ctx, self.rgb, self.mask = border, ctx, rgb, mask
         self.solution = None
 
-    def _image(self, k):
+    def _image(self, k, grain=False):
         from . import Image
         if self.rgb:
-            return Image(image_rgb=self.frames[k], border=self.border, ctx=self.ctx)
-        return Image(image_gs=self.frames[k], border=self.border, ctx=self.ctx)
+            return Image(image_rgb=self.frames[k], border=self.border, ctx=self.ctx, grain=grain)
+        return Image(image_gs=self.frames[k], border=self.border, ctx=self.ctx, grain=grain)
 
     def _load(self, img, k):
         if self.rgb:
@@ -131,7 +131,7 @@ class Sequence:
     def solve(self, local_mask, seed_coord, seed_warp=None, seed_tolerance=0.9, max_norm=1e-5, max_iterations=50,
               subset_order=1, tolerance=0.75, method="icgn", guide=True, sequential=False, override=False,
               preconditioning="RG", layer_rg_batch_factor=4, layer_rg_root_rel_eps=0.02, layer_rg_max_workers=None,
-              precision=0, progress=None):
+              precision=0, progress=None, texture="deformable"):
         """Sequence::solve (src/sequence.rs:624-968) with the options guide,
         sequential and override; returns and keeps a dict with one entry per
         solved pair (f_index, g_index, results, rounds, seed_coord) and the
@@ -145,7 +145,10 @@ class Sequence:
             v = np.asarray(seed_warp, dtype=np.float64).ravel()[:warp_len]
             sw[:len(v)] = v
         f_index, g_index = 0, 1
-        F, G = self._image(f_index), self._image(g_index)
+        # with the rigid texture both images keep grain maps: a sequential
+        # update makes the target the next reference
+        rigid = texture == "rigid"
+        F, G = self._image(f_index, rigid), self._image(g_index, rigid and sequential)
         pairs, override_log = [], []
         reference_updates = [False] * n_pairs
         mesh_override = pending_ref_update = False
@@ -157,7 +160,8 @@ class Sequence:
                       tolerance=0.0 if mesh_override else tolerance, method=method,
                       override_active=mesh_override, preconditioning=preconditioning,
                       layer_rg_batch_factor=layer_rg_batch_factor, layer_rg_root_rel_eps=layer_rg_root_rel_eps,
-                      layer_rg_max_workers=layer_rg_max_workers, precision=precision, progress=progress)
+                      layer_rg_max_workers=layer_rg_max_workers, precision=precision, progress=progress,
+                      texture=texture)
             try:
                 mesh.solve(local_mask, **kw)
             except Cancelled:

@@ -63,9 +63,21 @@ typedef enum {
                                 (solve_fagn_result, src/subset.rs:1228-1334);
                                 FP64 arithmetic in either precision mode, on the
                                 FP64 coefficients when precision is FP64     */
+#define GPV_SOLVE_RIGID_TEXTURE 8u /* Texture::Rigid (src/texture.rs,
+                                src/subset.rs:1062-1097, 1151-1168): fit g to the
+                                template f + G(E(p)) rebuilt every iteration
+                                from the reference image's grain maps (f needs
+                                them: GPV_IMAGE_GRAIN or gpv_image_build_grain);
+                                orders 1 and 2, mixed-precision ICGN only.  An
+                                image without measurable speckle keeps the
+                                deformable template (result texture = 0), as the
+                                reference falls back.  The branch for known
+                                soil grains (soil properties) is not part of
+                                this library. */
 
 /* gpv_image_create flags */
 #define GPV_IMAGE_KEEP_F64 1u /* also keep FP64 coefficients (needed by GPV_PREC_FP64) */
+#define GPV_IMAGE_GRAIN 2u    /* also keep the rigid-texture grain maps, rebuilt with every new set of pixels */
 
 typedef struct gpv_context gpv_context;
 typedef struct gpv_image gpv_image;
@@ -95,7 +107,9 @@ typedef struct {
     double *history;      /* host, n * max_iterations * 3 doubles, or NULL */
 } gpv_solve_params;
 
-/* SolveResult fields (src/subset.rs:145-191) + Subset scalars.  192 bytes. */
+/* SolveResult fields (src/subset.rs:145-191) + Subset scalars.  200 bytes.
+ * texture: 1 when the solve fitted the rigid-texture template
+ * (SolveResult::texture = Texture::Rigid), else 0. */
 typedef struct {
     double p[12];
     double c_zncc, c_znssd, norm;
@@ -103,6 +117,7 @@ typedef struct {
     double f_m, delta_f, sssig, sigma;
     int32_t iterations, converged, quality_ok, status;
     int32_t n_px, has_eta;
+    int32_t texture, reserved;
 } gpv_subset_result;
 
 /* ---- library ----------------------------------------------------------- */
@@ -150,6 +165,16 @@ int gpv_image_update_device(gpv_image *img, const void *px_dev, int32_t dtype);
  * when px is page-locked).  Synchronous. */
 int gpv_image_update(gpv_image *img, const void *px, int32_t dtype);
 int gpv_image_destroy(gpv_image *img);
+/* Rigid texture (GrainMaps::build, src/texture.rs:99-115, with the speckle
+ * correlation length of src/seam.rs:255-301): builds the grain maps of an
+ * image from its staged pixels (an image created or last updated from host
+ * or colour pixels; device pixels need GPV_IMAGE_GRAIN at creation) and keeps
+ * them up to date with later updates.  Asynchronous on the context stream. */
+int gpv_image_build_grain(gpv_image *img);
+/* The grain statistics (synchronises the context stream): out3 = correlation
+ * length, s2, smoothing correction; *built = 0 when the image has no
+ * measurable speckle; maps (host, 3 x h x w FP32: fxx, fyy, fxy) or NULL. */
+int gpv_image_grain(gpv_image *img, double *out3, int32_t *built, float *maps);
 int gpv_image_shape(const gpv_image *img, int64_t *h, int64_t *w, int32_t *border);
 /* Download coefficients C (h+2b, w+2b) row-major: FP32 always, FP64 if kept. */
 int gpv_image_coefficients_f32(const gpv_image *img, float *out);
@@ -283,7 +308,7 @@ typedef int (*gpv_batch_solver_fn)(void *user, const gpv_subset_desc *desc, int6
                                    gpv_subset_result *out);
 
 /* SolveConfig + SeedConfig + LayerRgConfig (src/mesh.rs:222-262, :339-356;
- * python/src/py_mesh.rs:215-225 defaults in brackets).  200 bytes. */
+ * python/src/py_mesh.rs:215-225 defaults in brackets).  208 bytes. */
 typedef struct {
     double seed_coord[2];
     double seed_warp[12];     /* first 6 * subset_order used          [0]    */
@@ -300,6 +325,9 @@ typedef struct {
     int32_t max_workers;      /* the worker count rounds are sized by (the
                                  reference's rayon pool size), >= 1          */
     int32_t method;           /* 0 = ICGN, 1 = FAGN (SolveMethod, :284-288)  */
+    int32_t texture;          /* 0 = deformable, 1 = rigid (Texture, :317-330;
+                                 gpv_mesh_solve: GPV_SOLVE_RIGID_TEXTURE)    */
+    int32_t reserved;
     const gpv_mask *mask;     /* global mask or NULL (gpv_mesh_solve only)   */
     gpv_progress_fn progress; /* or NULL */
     void *progress_user;

@@ -52,13 +52,17 @@ typedef struct {
     double f_m, delta_f, sssig, sigma;
     int32_t iterations, converged, quality_ok, status;
     int32_t n_px, has_eta;
+    int32_t texture, reserved; /* 1: fitted to the rigid-texture template */
 } gpvo_result;
 
 typedef struct {
     double max_norm;
     double tolerance;
     int32_t max_iterations;
-    int32_t flags; /* bit 0: eta diagnostic; bit 2: FAGN instead of ICGN */
+    int32_t flags; /* bit 0: eta diagnostic; bit 2: FAGN instead of ICGN; bit 3: rigid texture */
+    double s2;            /* rigid texture: blob width^2 (px^2) */
+    const double *grain;  /* rigid texture: fxx, fyy, fxy maps (3 x gh x gw), or NULL */
+    int64_t gh, gw;
 } gpvo_params;
 
 enum {
@@ -575,6 +579,178 @@ int gpvo_eta(const double coord[2], int order, const double *fc, const double *g
 }
 
 /* ================================================================== */
+/* Rigid-texture template (src/texture.rs, src/seam.rs:255-301)        */
+/* ================================================================== */
+
+/* Speckle correlation length (correlation_length, src/seam.rs:255-301):
+ * the centred side x side crop (side = min(512, rows, cols), even) with its
+ * mean removed, its circular autocorrelation along x and y at lags
+ * 0..side/2-1 (the reference takes them from |FFT|^2; here as direct lag
+ * sums), profile = mean of the two / lag 0, and the lag where it first
+ * falls below 0.5, interpolated linearly.  0 ok, 1 image too small, 2 the
+ * profile never falls to 0.5. */
+int gpvo_correlation_length(const double *a, int64_t rows, int64_t cols, double *ell) {
+    int64_t side = rows < cols ? rows : cols;
+    if (side > 512) side = 512;
+    side &= ~(int64_t)1;
+    if (side < 16) return 1;
+    const int64_t half = side / 2, cy = rows / 2, cx = cols / 2;
+    double *crop = (double *)malloc(sizeof(double) * side * side);
+    for (int64_t r = 0; r < side; r++)
+        for (int64_t c = 0; c < side; c++) crop[r * side + c] = a[(cy - half + r) * cols + (cx - half + c)];
+    double mean = 0.0;
+    for (int64_t i = 0; i < side * side; i++) mean += crop[i];
+    mean /= (double)(side * side);
+    for (int64_t i = 0; i < side * side; i++) crop[i] -= mean;
+    double *ax = (double *)malloc(sizeof(double) * half), *ay = (double *)malloc(sizeof(double) * half);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t k = 0; k < half; k++) {
+        double sx = 0.0, sy = 0.0;
+        for (int64_t r = 0; r < side; r++)
+            for (int64_t c = 0; c < side; c++) {
+                const double v = crop[r * side + c];
+                sx += v * crop[r * side + (c + k) % side];
+                sy += v * crop[((r + k) % side) * side + c];
+            }
+        ax[k] = sx;
+        ay[k] = sy;
+    }
+    int rc = 2;
+    double prev = 1.0;
+    for (int64_t k = 0; k < half; k++) {
+        const double prof = 0.5 * (ax[k] + ay[k]) / ax[0];
+        if (prof < 0.5) {
+            *ell = (double)k - 1.0 + (prev - 0.5) / (prev - prof);
+            rc = 0;
+            break;
+        }
+        prev = prof;
+    }
+    free(crop); free(ax); free(ay);
+    return rc;
+}
+
+/* Gaussian kernel of width sigma, radius ceil(4 sigma), derivative order 0,
+ * 1 or 2, as correlation weights normalised by the Gaussian's sum
+ * (kernel_with, src/texture.rs:49-68).  Returns the radius. */
+int gpvo_gauss_kernel(int order, double sigma, double *k) {
+    const int r = (int)ceil(4.0 * sigma);
+    const double s2 = sigma * sigma;
+    double norm = 0.0;
+    for (int i = -r; i <= r; i++) norm += exp(-(double)(i * i) / (2.0 * s2));
+    for (int i = -r; i <= r; i++) {
+        const double t = (double)i, gi = exp(-(double)(i * i) / (2.0 * s2));
+        const double v = order == 0 ? gi : (order == 1 ? t / s2 * gi : (t * t / (s2 * s2) - 1.0 / s2) * gi);
+        k[i + r] = v / norm;
+    }
+    return r;
+}
+
+/* Correlate rows (along x) or columns of a (rows x cols) with k (2r+1
+ * taps), replicating edge pixels; a left-to-right sum of products
+ * (filter_1d, src/texture.rs:70-93). */
+static void filter_1d(const double *a, int64_t rows, int64_t cols, const double *k, int r, int along_rows, double *out) {
+#pragma omp parallel for schedule(static)
+    for (int64_t y = 0; y < rows; y++)
+        for (int64_t x = 0; x < cols; x++) {
+            double s = 0.0;
+            for (int j = 0; j <= 2 * r; j++) {
+                const int64_t t = j - r;
+                double v;
+                if (along_rows) {
+                    int64_t xx = x + t;
+                    xx = xx < 0 ? 0 : (xx > cols - 1 ? cols - 1 : xx);
+                    v = a[y * cols + xx];
+                } else {
+                    int64_t yy = y + t;
+                    yy = yy < 0 ? 0 : (yy > rows - 1 ? rows - 1 : yy);
+                    v = a[yy * cols + x];
+                }
+                s += k[j] * v;
+            }
+            out[y * cols + x] = s;
+        }
+}
+
+/* GrainMaps::build (src/texture.rs:99-115) after the correlation length:
+ * with SMOOTH = 1, fxx = cols(rows(a, k2), k0) corr, fyy = cols(rows(a, k0),
+ * k2) corr, fxy = cols(rows(a, k1), k1) corr.  maps: 3 x rows x cols. */
+void gpvo_grain_maps(const double *a, int64_t rows, int64_t cols, double corr, double *maps) {
+    double k[3][9];
+    int r = 0;
+    for (int o = 0; o < 3; o++) r = gpvo_gauss_kernel(o, 1.0, k[o]);
+    const int64_t np = rows * cols;
+    double *h = (double *)malloc(sizeof(double) * np), *t = (double *)malloc(sizeof(double) * np);
+    const int pairs[3][2] = {{2, 0}, {0, 2}, {1, 1}};  /* (row kernel, column kernel) of fxx, fyy, fxy */
+    for (int m = 0; m < 3; m++) {
+        filter_1d(a, rows, cols, k[pairs[m][0]], r, 1, h);
+        filter_1d(h, rows, cols, k[pairs[m][1]], r, 0, t);
+        for (int64_t i = 0; i < np; i++) maps[m * np + i] = t[i] * corr;
+    }
+    free(h); free(t);
+}
+
+/* Bilinear sample of the three maps at (x = column, y = row), clamped
+ * (GrainMaps::sample, src/texture.rs:125-143). */
+static void grain_sample(const double *maps, int64_t rows, int64_t cols, double x, double y, double h[3]) {
+    x = x < 0.0 ? 0.0 : (x > (double)(cols - 1) ? (double)(cols - 1) : x);
+    y = y < 0.0 ? 0.0 : (y > (double)(rows - 1) ? (double)(rows - 1) : y);
+    int64_t x0 = (int64_t)floor(x), y0 = (int64_t)floor(y);
+    if (x0 > cols - 2) x0 = cols - 2 < 0 ? 0 : cols - 2;
+    if (y0 > rows - 2) y0 = rows - 2 < 0 ? 0 : rows - 2;
+    const int64_t x1 = x0 + 1 < cols - 1 ? x0 + 1 : cols - 1, y1 = y0 + 1 < rows - 1 ? y0 + 1 : rows - 1;
+    const double tx = x - (double)x0, ty = y - (double)y0;
+    for (int m = 0; m < 3; m++) {
+        const double *M = maps + m * rows * cols;
+        h[m] = (1.0 - ty) * ((1.0 - tx) * M[y0 * cols + x0] + tx * M[y0 * cols + x1]) +
+               ty * ((1.0 - tx) * M[y1 * cols + x0] + tx * M[y1 * cols + x1]);
+    }
+}
+
+/* Green-Lagrange strain [Exx, Eyy, Exy] (src/texture.rs:200-206). */
+static void green_lagrange(double ux, double vx, double uy, double vy, double e[3]) {
+    e[0] = ux + 0.5 * (ux * ux + vx * vx);
+    e[1] = vy + 0.5 * (uy * uy + vy * vy);
+    e[2] = 0.5 * (uy + vx) + 0.5 * (ux * uy + vx * vy);
+}
+
+/* The template f + G(E(p)) with base = the subset mean, its mean and spread
+ * (grain_template, src/texture.rs:213-244; rigid_template, src/subset.rs:
+ * 1399-1411).  xy: (n,2) offsets of the pixels from the centre. */
+static void rigid_template(const double *f, double f_m, const double *h, double s2, const double *p, int m,
+                           const double *xy, int64_t n, double *t, double *t_m, double *delta_t) {
+    double e[3];
+    if (m <= 7) green_lagrange(p[2], p[3], p[4], p[5], e);
+    for (int64_t i = 0; i < n; i++) {
+        if (m > 7) {
+            const double dx = xy[2 * i], dy = xy[2 * i + 1];
+            green_lagrange(p[2] + p[6] * dx + p[8] * dy, p[3] + p[7] * dx + p[9] * dy, p[4] + p[8] * dx + p[10] * dy,
+                           p[5] + p[9] * dx + p[11] * dy, e);
+        }
+        const double *hi = h + 3 * i;
+        t[i] = f[i] + (-0.5 * s2 * (e[0] * hi[0] + e[1] * hi[1] + 2.0 * e[2] * hi[2]) - (e[0] + e[1]) * (f[i] - f_m));
+    }
+    double sum = 0.0;
+    for (int64_t i = 0; i < n; i++) sum += t[i];
+    *t_m = sum / (double)n;
+    double ss = 0.0;
+    for (int64_t i = 0; i < n; i++) ss += (t[i] - *t_m) * (t[i] - *t_m);
+    *delta_t = sqrt(ss);
+}
+
+/* grain_template alone (src/texture.rs:213-244) for the template tests:
+ * out = f + G(E(p)); m = 2 returns f. */
+void gpvo_grain_template(const double *f, double f_m, const double *h, double s2, const double *p, int m,
+                         const double *xy, int64_t n, double *out) {
+    if (m == 2) {
+        memcpy(out, f, sizeof(double) * n);
+        return;
+    }
+    double t_m, dt;
+    rigid_template(f, f_m, h, s2, p, m, xy, n, out, &t_m, &dt);
+}
+
+/* ================================================================== */
 /* Subset::new + solve_icgn_result (src/subset.rs:836-919, 1117-1219)  */
 /* ================================================================== */
 typedef struct {
@@ -677,7 +853,25 @@ static void solve_one(const spline *F, const spline *G, const gpvo_desc *d, cons
     double *g = (double *)calloc(n, sizeof(double));
     int converged = 0, iters = 0, status = ST_OK;
     double last_norm = 0.0, c_zncc = 0.0, c_znssd = 4.0;
+    /* rigid texture (grain_setup, src/subset.rs:1062-1097, the branch without
+     * soil properties): the maps at the subset pixels, and the template
+     * rebuilt from the current warp at every iteration */
+    const int rigid = (prm->flags & 8) && order >= 1 && prm->grain;
+    double *hmap = NULL, *tf = NULL, *off = NULL, tf_m = s.f_m, delta_tf = s.delta_f;
+    const double *fv = s.f;
+    if (rigid) {
+        hmap = (double *)malloc(sizeof(double) * 3 * n);
+        tf = (double *)malloc(sizeof(double) * n);
+        off = (double *)malloc(sizeof(double) * 2 * n);
+        for (int64_t i = 0; i < n; i++) {
+            grain_sample(prm->grain, prm->gh, prm->gw, s.fc[2 * i], s.fc[2 * i + 1], hmap + 3 * i);
+            off[2 * i] = s.fc[2 * i] - d->coord[0];
+            off[2 * i + 1] = s.fc[2 * i + 1] - d->coord[1];
+        }
+        fv = tf;
+    }
     for (int it = 1; it <= prm->max_iterations; it++) {
+        if (rigid) rigid_template(s.f, s.f_m, hmap, prm->s2, p, m, off, n, tf, &tf_m, &delta_tf);
         for (int64_t i = 0; i < n; i++) {       /* apply_warp_into + eval (:1158-1161) */
             double xw, yw;
             warp_point(d->coord, p, m, s.fc[2 * i], s.fc[2 * i + 1], &xw, &yw);
@@ -689,12 +883,13 @@ static void solve_one(const spline *F, const spline *G, const gpvo_desc *d, cons
         double gss = 0.0;
         for (int64_t i = 0; i < n; i++) gss += (g[i] - g_m) * (g[i] - g_m);
         double delta_g = sqrt(gss);
-        /* delta_p_and_znssd_icgn (:418-446) */
-        double ratio = s.delta_f / delta_g, zacc = 0.0;
+        /* delta_p_and_znssd_icgn (:418-446), against the template when rigid */
+        const double f_m_t = rigid ? tf_m : s.f_m, df_t = rigid ? delta_tf : s.delta_f;
+        double ratio = df_t / delta_g, zacc = 0.0;
         for (int k = 0; k < m; k++) grad_z[k] = 0.0;
         for (int64_t i = 0; i < n; i++) {
-            double a = s.f[i] - s.f_m, b = g[i] - g_m;
-            double z = a / s.delta_f - b / delta_g;
+            double a = fv[i] - f_m_t, b = g[i] - g_m;
+            double z = a / df_t - b / delta_g;
             zacc += z * z;
             double br = a - ratio * b;
             for (int k = 0; k < m; k++) grad_z[k] += sdi[i * m + k] * br;
@@ -725,10 +920,13 @@ static void solve_one(const spline *F, const spline *G, const gpvo_desc *d, cons
         for (int64_t i = 0; i < n; i++) gs += g[i];
         double g_m = gs / (double)n, gss = 0.0;
         for (int64_t i = 0; i < n; i++) gss += (g[i] - g_m) * (g[i] - g_m);
-        gpvo_eta(d->coord, order, s.fc, s.grad, s.f, s.f_m, s.delta_f, g, g_m, sqrt(gss), n, &r->eta_u, &r->eta_v);
+        gpvo_eta(d->coord, order, s.fc, s.grad, fv, rigid ? tf_m : s.f_m, rigid ? delta_tf : s.delta_f, g, g_m,
+                 sqrt(gss), n, &r->eta_u, &r->eta_v);
         r->has_eta = 1;
     }
+    r->texture = rigid;
     free(g); free(sdi); subset_free(&s);
+    free(hmap); free(tf); free(off);
 }
 
 /* Subset::solve_fagn_result (src/subset.rs:1228-1334): per iteration the

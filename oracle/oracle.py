@@ -24,9 +24,10 @@ RESULT_DTYPE = np.dtype([
     ("p", "<f8", (12,)), ("c_zncc", "<f8"), ("c_znssd", "<f8"), ("norm", "<f8"),
     ("eta_u", "<f8"), ("eta_v", "<f8"), ("f_m", "<f8"), ("delta_f", "<f8"), ("sssig", "<f8"),
     ("sigma", "<f8"), ("iterations", "<i4"), ("converged", "<i4"), ("quality_ok", "<i4"),
-    ("status", "<i4"), ("n_px", "<i4"), ("has_eta", "<i4"),
+    ("status", "<i4"), ("n_px", "<i4"), ("has_eta", "<i4"), ("texture", "<i4"), ("reserved", "<i4"),
 ])
-PARAMS_DTYPE = np.dtype([("max_norm", "<f8"), ("tolerance", "<f8"), ("max_iterations", "<i4"), ("flags", "<i4")])
+PARAMS_DTYPE = np.dtype([("max_norm", "<f8"), ("tolerance", "<f8"), ("max_iterations", "<i4"), ("flags", "<i4"),
+                         ("s2", "<f8"), ("grain", "<u8"), ("gh", "<i8"), ("gw", "<i8")])
 
 _lib = None
 
@@ -56,6 +57,12 @@ def lib():
         L.gpvo_mask_update.restype = i64
         L.gpvo_apply_warp.argtypes = [P, P, i32, P, i64, P]
         L.gpvo_steepest_descent.argtypes = [P, P, P, i64, i32, P]
+        L.gpvo_correlation_length.argtypes = [P, i64, i64, P]
+        L.gpvo_correlation_length.restype = i32
+        L.gpvo_gauss_kernel.argtypes = [i32, dbl, P]
+        L.gpvo_gauss_kernel.restype = i32
+        L.gpvo_grain_maps.argtypes = [P, i64, i64, dbl, P]
+        L.gpvo_grain_template.argtypes = [P, dbl, P, dbl, P, i32, P, i64, P]
         L.gpvo_compose.argtypes = [P, P, i32, P]
         L.gpvo_compose.restype = i32
         L.gpvo_norm.argtypes = [P, i32, dbl]
@@ -214,19 +221,72 @@ def subset_setup(coef, shape, border, coord, radius, mask=None):
 
 
 def solve_batch(coef_f, coef_g, shape, border, desc, max_norm=1e-5, max_iterations=50, tolerance=0.75,
-                eta=False, mask=None, history=False, nthreads=0, method="icgn"):
+                eta=False, mask=None, history=False, nthreads=0, method="icgn", grain=None):
     """Batched Subset::new + solve_icgn_result (src/subset.rs:836-919, 1117-1219),
-    or solve_fagn_result (:1228-1334) with method="fagn"."""
+    or solve_fagn_result (:1228-1334) with method="fagn".  grain = (maps, s2)
+    from grain() fits the rigid-texture template (ICGN; order 1 and 2)."""
     desc = np.ascontiguousarray(desc, dtype=DESC_DTYPE)
     prm = np.zeros(1, PARAMS_DTYPE)
-    flags = int(eta) | (4 if method == "fagn" else 0)
+    flags = int(eta) | (4 if method == "fagn" else 0) | (8 if grain is not None else 0)
     prm["max_norm"], prm["tolerance"], prm["max_iterations"], prm["flags"] = max_norm, tolerance, max_iterations, flags
+    if grain is not None and grain[0] is not None:
+        maps = np.ascontiguousarray(grain[0], dtype=np.float64)
+        prm["s2"], prm["grain"], prm["gh"], prm["gw"] = grain[1], maps.ctypes.data, maps.shape[1], maps.shape[2]
     out = np.zeros(desc.size, RESULT_DTYPE)
     hist = np.zeros((desc.size, max_iterations, 3)) if history else None
     m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
     lib().gpvo_solve_batch(_p(_f8(coef_f)), _p(_f8(coef_g)), shape[0], shape[1], border, _p(desc), desc.size,
                            _p(prm), _p(m), _p(out), _p(hist), nthreads or lib().gpvo_max_threads())
     return (out, hist) if history else out
+
+
+def correlation_length(image):
+    """correlation_length (src/seam.rs:255-301): the speckle correlation length
+    of a reference image (px), or None (too small / never falls to 0.5)."""
+    a = _f8(image)
+    ell = ct.c_double()
+    rc = lib().gpvo_correlation_length(_p(a), a.shape[0], a.shape[1], ct.byref(ell))
+    return ell.value if rc == 0 else None
+
+
+def gauss_kernel(order, sigma=1.0):
+    """kernel_with (src/texture.rs:49-68)."""
+    k = np.empty(2 * int(np.ceil(4.0 * sigma)) + 1)
+    lib().gpvo_gauss_kernel(order, float(sigma), _p(k))
+    return k
+
+
+def grain(image):
+    """GrainMaps::build (src/texture.rs:99-115): (maps (3, h, w) = fxx, fyy,
+    fxy scaled by the smoothing correction, s2), or (None, None) when the
+    image has no measurable speckle."""
+    a = _f8(image)
+    ell = correlation_length(a)
+    if ell is None:
+        return None, None
+    s2 = ell * ell / (2.0 * np.log(2.0))
+    if not (np.isfinite(s2) and s2 > 0):
+        return None, None
+    corr = ((s2 / 2.0 + 1.0) / (s2 / 2.0)) ** 2
+    maps = np.empty((3,) + a.shape)
+    lib().gpvo_grain_maps(_p(a), a.shape[0], a.shape[1], corr, _p(maps))
+    return maps, s2
+
+
+def grain_maps(image, corr=1.0):
+    """The three filtered maps (fxx, fyy, fxy) times corr (src/texture.rs:108-114)."""
+    a = _f8(image)
+    maps = np.empty((3,) + a.shape)
+    lib().gpvo_grain_maps(_p(a), a.shape[0], a.shape[1], float(corr), _p(maps))
+    return maps
+
+
+def grain_template(f, f_m, h, s2, p, xy):
+    """grain_template (src/texture.rs:213-244) with base = the subset mean."""
+    f, h, p, xy = _f8(f), _f8(h), _f8(p), _f8(xy)
+    out = np.empty_like(f)
+    lib().gpvo_grain_template(_p(f), float(f_m), _p(h), float(s2), _p(p), p.size, _p(xy), f.size, _p(out))
+    return out
 
 
 def ingest_rgb8(rgb):

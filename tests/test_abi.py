@@ -39,7 +39,7 @@ def test_library_exports_every_declared_symbol(gpv_mod):
 def test_record_layouts(gpv_mod, oracle):
     from gpv import _lib
     assert _lib.DESC_DTYPE.itemsize == 120
-    assert _lib.RESULT_DTYPE.itemsize == 192
+    assert _lib.RESULT_DTYPE.itemsize == 200
     assert ct.sizeof(_lib.SolveParams) == 48
     assert _lib.SolveParams.mask.offset == 32 and _lib.SolveParams.history.offset == 40
     # the oracle reads the same records

@@ -1,0 +1,116 @@
+"""The rigid-texture template on the GPU against the oracle.
+
+* Grain statistics: the device maps equal the oracle's (FP64 sums with the
+  same rounding, stored as FP32) bit for bit; the correlation length, s2 and
+  the smoothing correction agree to 1e-12 relative; updates rebuild them.
+* Rigid solves (mixed precision) on the reference's rigid-blob shear pair
+  (src/texture.rs:424-437): displacement within 1e-3 px and gradient terms
+  within 1e-5 of the FP64 oracle's rigid solve, identical flags, texture = 1;
+  better than the deformable template at order 1 (src/texture.rs:481-500);
+  the deformable template for order 0 and for an image without measurable
+  speckle; refused for the FP64 and FAGN forms.
+"""
+import numpy as np
+import pytest
+
+import texture_cases as TC
+
+pytestmark = pytest.mark.gpu
+
+
+def test_grain_maps_equal_the_oracle(gpv_mod, oracle):
+    from gpv import synth
+    f, _ = TC.shear_pair(0.05)
+    W = synth.workload(1, scale_down=4)
+    for arr in (f, W["f"]):  # FP64 pixels and u8 pixels
+        img = gpv_mod.Image(image_gs=arr, border=8, grain=True)
+        got = img.grain(maps=True)
+        ell = oracle.correlation_length(arr.astype(np.float64))
+        maps, s2 = oracle.grain(arr.astype(np.float64))
+        assert got["built"]
+        assert abs(got["correlation_length"] - ell) < 1e-12 * ell
+        assert abs(got["s2"] - s2) < 1e-12 * s2
+        assert np.array_equal(got["maps"], maps.astype(np.float32))
+    # an update rebuilds them; a flat image has none
+    img = gpv_mod.Image(image_gs=f, border=8, grain=True)
+    img.update(W["f"][:200, :200].astype(np.float64))
+    assert abs(img.grain()["correlation_length"] - oracle.correlation_length(W["f"][:200, :200].astype(np.float64))) < 1e-9
+    flat = gpv_mod.Image(image_gs=np.full((64, 64), 128.0), border=8, grain=True)
+    assert not flat.grain()["built"]
+
+
+def _solve_both(gpv_mod, oracle, gamma, order):
+    f, g = TC.shear_pair(gamma)
+    F = gpv_mod.Image(image_gs=f, border=8)
+    G = gpv_mod.Image(image_gs=g, border=8)
+    d = TC.grid_desc(gpv_mod, gamma, order)
+    kw = dict(max_norm=1e-6, max_iterations=100, tolerance=0.75)
+    gd = gpv_mod.solve_batch(F, G, d, **kw)
+    gr = gpv_mod.solve_batch(F, G, d, texture="rigid", eta=True, **kw)
+    maps, s2 = oracle.grain(f)
+    cf, cg = oracle.get_c(f, 8), oracle.get_c(g, 8)
+    od = oracle.solve_batch(cf, cg, f.shape, 8, d, **kw)
+    orr = oracle.solve_batch(cf, cg, f.shape, 8, d, grain=(maps, s2), eta=True, **kw)
+    return gd, gr, od, orr
+
+
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("gamma", [0.0, 0.05])
+def test_rigid_solve_matches_the_oracle(gpv_mod, oracle, order, gamma):
+    gd, gr, od, orr = _solve_both(gpv_mod, oracle, gamma, order)
+    assert np.all(gr["texture"] == 1) and np.all(orr["texture"] == 1) and np.all(gd["texture"] == 0)
+    for a, b in ((gr, orr), (gd, od)):
+        ok = b["status"] == 0
+        assert np.array_equal(a["status"], b["status"]) and np.array_equal(a["converged"], b["converged"])
+        assert np.abs(a["p"][ok, :2] - b["p"][ok, :2]).max() <= 1e-3
+        assert np.abs(a["p"][ok, 2:6] - b["p"][ok, 2:6]).max() <= 1e-5
+        assert np.abs(a["c_zncc"][ok] - b["c_zncc"][ok]).max() < 1e-5
+    assert np.abs(gr["eta_u"] - orr["eta_u"]).max() < 2e-3 and np.all(gr["has_eta"] == 1)
+    if gamma > 0 and order == 1:  # src/texture.rs:481-500
+        assert gr["c_znssd"].mean() < gd["c_znssd"].mean()
+        assert np.abs(gr["p"][:, 4] - gamma).mean() < np.abs(gd["p"][:, 4] - gamma).mean()
+
+
+def test_rigid_falls_back_and_is_refused_where_unsupported(gpv_mod):
+    from gpv import synth
+    W = synth.workload(1, scale_down=4)
+    F = gpv_mod.Image(image_gs=W["f"], border=20, keep_f64=True)
+    G = gpv_mod.Image(image_gs=W["g"], border=20, keep_f64=True)
+    d = gpv_mod.make_desc(W["coords"][:40], 25, 0, W["p0"][:40])
+    r = gpv_mod.solve_batch(F, G, d, texture="rigid")  # order 0: deformable
+    assert np.all(r["texture"] == 0) and np.mean(r["converged"]) > 0.9
+    d1 = gpv_mod.make_desc(W["coords"][:40], 25, 1, W["p0"][:40])
+    with pytest.raises(gpv_mod.GpvError):
+        gpv_mod.solve_batch(F, G, d1, texture="rigid", precision=gpv_mod.PREC_FP64)
+    with pytest.raises(gpv_mod.GpvError):
+        gpv_mod.solve_batch(F, G, d1, texture="rigid", method="fagn")
+    with pytest.raises(ValueError):
+        gpv_mod.solve_batch(F, G, d1, texture="grainy")
+    # no measurable speckle (a smooth ramp): the deformable template, texture 0
+    y, x = np.mgrid[0:128, 0:128].astype(np.float64)
+    ramp = 50.0 + 0.5 * x + 0.3 * y + 10.0 * np.sin(x / 7.0) * np.cos(y / 9.0)
+    R = gpv_mod.Image(image_gs=ramp, border=8)
+    dr = gpv_mod.make_desc([[64.0, 64.0], [60.5, 70.25]], 20, 1)
+    a = gpv_mod.solve_batch(R, R, dr, texture="rigid")
+    b = gpv_mod.solve_batch(R, R, dr)
+    assert not R.grain()["built"] and np.all(a["texture"] == 0)
+    assert np.abs(a["p"] - b["p"]).max() < 1e-9 and np.array_equal(a["iterations"], b["iterations"])
+
+
+def test_rigid_mesh_solve(gpv_mod, oracle):
+    """Mesh.solve(texture="rigid") (python/src/py_mesh.rs:279-290) on the shear pair."""
+    f, g = TC.shear_pair(0.05)
+    F = gpv_mod.Image(image_gs=f, border=8)
+    G = gpv_mod.Image(image_gs=g, border=8)
+    xs = np.linspace(40, 160, 5)
+    nodes = np.array([[x, y] for y in xs for x in xs])
+    elements = []
+    for j in range(4):
+        for i in range(4):
+            a, b, c, e = j * 5 + i, j * 5 + i + 1, (j + 1) * 5 + i, (j + 1) * 5 + i + 1
+            elements += [[a, b, e], [a, e, c]]
+    mesh = gpv_mod.Mesh(nodes, np.array(elements), F, G)
+    mesh.solve(15, seed_coord=(100.3, 100.6), max_norm=1e-6, max_iterations=100, texture="rigid")
+    res = mesh.results
+    assert np.all(res["texture"] == 1) and np.all(res["converged"] == 1)
+    assert np.abs(res["p"][:, 4] - 0.05).max() < 0.02

@@ -219,7 +219,10 @@ def test_oracle_fixture_unchanged(oracle):
     import gpv  # noqa: F401
     z = np.load(os.path.join(HERE, "golden", "oracle_small.npz"))
     d = z["desc"].view(oracle.DESC_DTYPE)
-    res0 = z["result"].view(oracle.RESULT_DTYPE)
+    # the fixture holds the 192-byte records written before the texture field
+    legacy = np.dtype([(k, oracle.RESULT_DTYPE.fields[k][0]) for k in oracle.RESULT_DTYPE.names
+                       if k not in ("texture", "reserved")])
+    res0 = z["result"].view(legacy)
     Cf = oracle.get_c(z["f"].astype(np.float64), 20)
     Cg = oracle.get_c(z["g"].astype(np.float64), 20)
     res = oracle.solve_batch(Cf, Cg, z["f"].shape, 20, d, max_norm=1e-5, max_iterations=15, eta=True)

@@ -20,7 +20,7 @@ def _desc(gpv, n):
 def _footprint(h, w, n, border=20, esz=1):
     cw, ch = w + 2 * border, h + 2 * border
     pitch = (cw + 31) // 32 * 32
-    return 2 * 4 * pitch * ch + 2 * 8 * h * cw + 2 * esz * h * w + n * (120 + 192 + 4)
+    return 2 * 4 * pitch * ch + 2 * 8 * h * cw + 2 * esz * h * w + n * (120 + 200 + 4)
 
 
 class Recorder:

@@ -69,7 +69,7 @@ def test_noalloc_matches_device_entry_point(gpv_mod, config, scale):
     prm = _lib.SolveParams(max_norm=1e-5, tolerance=0.75, max_iterations=50, flags=0, precision=_lib.PREC_MIXED,
                            reserved=0, mask=None, history=None)
     s = torch.cuda.Stream()
-    out = torch.zeros(n * 192, dtype=torch.uint8, device="cuda")  # caller-owned output
+    out = torch.zeros(n * 200, dtype=torch.uint8, device="cuda")  # caller-owned output
     ref = _run("device", ctx, F, G, d_dev, n, prm, None, s, out)
     first = _run("noalloc", ctx, F, G, d_dev, n, prm, 32, s, out)   # first call does the one-time set-up
     torch.cuda.synchronize()
@@ -92,7 +92,7 @@ def test_noalloc_limits(gpv_mod):
     prm = _lib.SolveParams(max_norm=1e-5, tolerance=0.75, max_iterations=50, flags=0, precision=_lib.PREC_MIXED,
                            reserved=0, mask=None, history=None)
     s = torch.cuda.Stream()
-    out = torch.zeros(len(d) * 192, dtype=torch.uint8, device="cuda")
+    out = torch.zeros(len(d) * 200, dtype=torch.uint8, device="cuda")
     rc = _lib.lib().gpv_solve_batch_noalloc(ctx.handle, F.handle, G.handle, ct.c_void_p(d_dev.data_ptr()), len(d), 40,
                                             ct.byref(prm), ct.c_void_p(out.data_ptr()), ct.c_void_p(s.cuda_stream))
     assert rc == -1 and "max_radius 40" in _lib.last_error()
