@@ -221,11 +221,15 @@ __device__ __forceinline__ void green_lagrange(float ux, float vx, float uy, flo
 
 // RIGID: the rigid-texture template (Texture::Rigid) when the reference image
 // has measurable speckle: the maps at the subset pixels in setup (Sh: 3
-// arrays of n_max), and every iteration a template pass storing
-// t = f + G(E(p)) per pixel (St) with its warp sums, so the update compares
-// g with the template (src/subset.rs:1151-1168, grain_template
-// src/texture.rs:213-244): t - t_m in the cross term and the gradient, the
-// template's spread instead of delta_f.
+// arrays of n_max), and every iteration a template pass storing the
+// correction G(E(p)) per pixel (St; the template is t = f + G,
+// grain_template src/texture.rs:213-244) with its warp sums, so the update
+// compares g with the template (src/subset.rs:1151-1168): t - t_m in the
+// cross term and the gradient, the template's spread instead of delta_f.
+// The template's sums are formed as the setup's fixed FP64 sums of f - f_m
+// plus per-iteration sums of the small G (sum G, sum G^2, sum (f - f_m) G,
+// sum SDI_j G), so the FP32 rounding of the per-iteration pass scales with
+// the strain and vanishes at zero strain, as the deformable sums do.
 template <int ORDER, int NT, bool RIGID>
 __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d, float4 *S4, float *Sg, float *win,
                             TileSmem &sm, float *Sh, float *St, int64_t nmax) {
@@ -492,9 +496,9 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         // window-relative base: sample (ix, iy) reads win[(iy + B-2 - r0) * ww + (ix + B-2 - c0)]
         const int offx = B - 2 - gc0, offy = B - 2 - gr0;
         if (RIGID && rigid_on) {
-            // template pass: t per pixel, sums of t - f_m, (t - f_m)^2 and
-            // SDI_j (t - f_m) (their warp sums meet the iteration's reduction)
-            constexpr int NT_ = 2 + M;
+            // template pass: G per pixel, sums of G, G^2, (f - f_m) G and
+            // SDI_j G (their warp sums meet the iteration's reduction)
+            constexpr int NT_ = 3 + M;
             float ta[NT_];
 #pragma unroll
             for (int q = 0; q < NT_; q++) ta[q] = 0.f;
@@ -513,18 +517,18 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                     green_lagrange(ux + q6 * dx + q8 * dy, vx + q7 * dx + q9 * dy, uy + q8 * dx + q10 * dy,
                                    vy + q9 * dx + q11 * dy, e0, e1, e2);
                 const float h0 = Sh[i], h1 = Sh[nmax + i], h2 = Sh[2 * nmax + i];
-                const float f = rec.x;
-                const float t = f + (-0.5f * s2f * (e0 * h0 + e1 * h1 + 2.0f * e2 * h2) - (e0 + e1) * (f - fmf));
-                St[i] = t;
-                const float ts = t - fmf;
-                ta[0] += ts;
-                ta[1] = fmaf(ts, ts, ta[1]);
-                const float gxt = rec.y * ts, gyt = rec.z * ts;
+                const float fc = rec.x - fmf;
+                const float G = -0.5f * s2f * (e0 * h0 + e1 * h1 + 2.0f * e2 * h2) - (e0 + e1) * fc;
+                St[i] = G;
+                ta[0] += G;
+                ta[1] = fmaf(G, G, ta[1]);
+                ta[2] = fmaf(fc, G, ta[2]);
+                const float gxt = rec.y * G, gyt = rec.z * G;
 #pragma unroll
                 for (int mu = 0; mu < NMU; mu++) {
                     const float mv = mu_val<float>(mu, dx, dy);
-                    ta[2 + 2 * mu] = fmaf(gxt, mv, ta[2 + 2 * mu]);
-                    ta[3 + 2 * mu] = fmaf(gyt, mv, ta[3 + 2 * mu]);
+                    ta[3 + 2 * mu] = fmaf(gxt, mv, ta[3 + 2 * mu]);
+                    ta[4 + 2 * mu] = fmaf(gyt, mv, ta[4 + 2 * mu]);
                 }
             }
 #pragma unroll
@@ -575,7 +579,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                         const float gc = g - fmf;
                         p1 += gc;
                         p2 = fmaf(gc, gc, p2);
-                        pfg = fmaf((RIGID && rigid_on ? St[i] : fv) - fmf, gc, pfg);
+                        pfg = fmaf((RIGID && rigid_on ? (fv - fmf) + St[i] : fv - fmf), gc, pfg);
                         const float gxg = rec.y * gc, gyg = rec.z * gc;
                         pb[0] += gxg;
                         pb[1] += gyg;
@@ -617,7 +621,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                 for (int w = 0; w < NT / 32; w++) t += sm.red[w][lane];
                 sm.tot[lane] = t;
             }
-            if (RIGID && rigid_on && lane < 2 + M) {
+            if (RIGID && rigid_on && lane < 3 + M) {
                 double t = 0.0;
 #pragma unroll
                 for (int w = 0; w < NT / 32; w++) t += sm.redt[w][lane];
@@ -632,9 +636,9 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             const double dg2 = sm.tot[1] - sm.tot[0] * gmt;
             dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
             double sab, dref = df, tmf = 0.0;
-            if (RIGID && rigid_on) {  // the template: t_m = f_m + tmf, spread dref
+            if (RIGID && rigid_on) {  // the template t = f + G: t_m = f_m + tmf, spread dref
                 tmf = sm.tt[0] / dn;
-                const double dt2 = sm.tt[1] - sm.tt[0] * tmf;
+                const double dt2 = saa + 2.0 * sm.tt[2] + sm.tt[1] - sm.tt[0] * tmf;
                 dref = sqrt(dt2 > 0.0 ? dt2 : 0.0);
                 sab = sm.tot[2] - tmf * sm.tot[0];
             } else {
@@ -643,7 +647,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             znssd = 2.0 - 2.0 * sab / (dref * dg);
             const double ratio = dref / dg;
             if (lane < M) {
-                const double aj = (RIGID && rigid_on) ? sm.tt[2 + lane] - tmf * sm.S[lane] : sm.A[lane];
+                const double aj = (RIGID && rigid_on) ? sm.A[lane] + sm.tt[3 + lane] - tmf * sm.S[lane] : sm.A[lane];
                 sm.grad[lane] = aj - ratio * (sm.tot[3 + lane] - gmt * sm.S[lane]);
             }
             if (lane == 0) {
@@ -745,7 +749,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             if (rec.x != rec.x) return false;
             float dxf, dyf;
             unpack_off(rec.w, dxf, dyf);
-            f = (RIGID && rigid_on) ? St[i] : rec.x;  // the template fitted at the last iteration
+            f = (RIGID && rigid_on) ? (double)rec.x + (double)St[i] : rec.x;  // the template fitted at the last iteration
             gx = rec.y; gy = rec.z; g = Sg[i]; dx = dxf; dy = dyf;
             return true;
         };
@@ -984,19 +988,26 @@ int tile_threads_for(gpv_context *ctx, int max_radius);
 // setting it to each launch's own size would let concurrent launches of the
 // same kernel with different windows (two contexts, two host threads) undo
 // each other's setting between the set and the launch.
-static int allow_max_dynamic_smem(const void *fn) {
+// *max_bytes receives that limit.
+static int allow_max_dynamic_smem(const void *fn, int *max_bytes) {
     static std::mutex mu;
-    static std::set<std::pair<int, const void *>> done;
+    static std::map<std::pair<int, const void *>, int> done;
     int dev = 0;
     GPV_CUDA_TRY(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(mu);
-    if (done.count({dev, fn})) return GPV_SUCCESS;
+    auto it = done.find({dev, fn});
+    if (it != done.end()) {
+        *max_bytes = it->second;
+        return GPV_SUCCESS;
+    }
     int optin = 0;
     GPV_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     cudaFuncAttributes fa;
     GPV_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
-    GPV_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
-    done.insert({dev, fn});
+    const int allowed = optin - (int)fa.sharedSizeBytes;
+    GPV_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, allowed));
+    done[{dev, fn}] = allowed;
+    *max_bytes = allowed;
     return GPV_SUCCESS;
 }
 
@@ -1071,9 +1082,13 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         P.nt = tile_threads_for(ctx, P.rmax);
         P.layout = tile_layout_for(ctx, P.rmax);
         P.cap = window_cap(P.rmax, P.layout);
-        const size_t smem = sizeof(float) * P.cap;
         const void *fn = tile_kernel(P.nt, P.ps, order, P.rigid);
-        if (int rc = allow_max_dynamic_smem(fn)) return rc;
+        int max_bytes = 0;
+        if (int rc = allow_max_dynamic_smem(fn, &max_bytes)) return rc;
+        // a window larger than the block can hold is not staged: those
+        // subsets read g's coefficients from global memory
+        P.cap = std::min(P.cap, max_bytes / (int)sizeof(float) / 4 * 4);
+        const size_t smem = sizeof(float) * P.cap;
         int per_sm = 0;
         GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, P.nt, smem));
         if (per_sm < 1) { set_error("subset window does not fit in shared memory"); return GPV_ERR_INVALID; }

@@ -44,7 +44,10 @@ def _solve_both(gpv_mod, oracle, gamma, order):
     F = gpv_mod.Image(image_gs=f, border=8)
     G = gpv_mod.Image(image_gs=g, border=8)
     d = TC.grid_desc(gpv_mod, gamma, order)
-    kw = dict(max_norm=1e-6, max_iterations=100, tolerance=0.75)
+    # max_norm 1e-5, the mixed form's bar in every parity test: at zero strain
+    # its FP32 interpolation keeps second-order norms of these radius-15
+    # subsets above 1e-6, with either template
+    kw = dict(max_norm=1e-5, max_iterations=100, tolerance=0.75)
     gd = gpv_mod.solve_batch(F, G, d, **kw)
     gr = gpv_mod.solve_batch(F, G, d, texture="rigid", eta=True, **kw)
     maps, s2 = oracle.grain(f)
@@ -86,13 +89,14 @@ def test_rigid_falls_back_and_is_refused_where_unsupported(gpv_mod):
         gpv_mod.solve_batch(F, G, d1, texture="rigid", method="fagn")
     with pytest.raises(ValueError):
         gpv_mod.solve_batch(F, G, d1, texture="grainy")
-    # no measurable speckle (a smooth ramp): the deformable template, texture 0
-    y, x = np.mgrid[0:128, 0:128].astype(np.float64)
-    ramp = 50.0 + 0.5 * x + 0.3 * y + 10.0 * np.sin(x / 7.0) * np.cos(y / 9.0)
-    R = gpv_mod.Image(image_gs=ramp, border=8)
-    dr = gpv_mod.make_desc([[64.0, 64.0], [60.5, 70.25]], 20, 1)
-    a = gpv_mod.solve_batch(R, R, dr, texture="rigid")
-    b = gpv_mod.solve_batch(R, R, dr)
+    # textured but too small to measure a correlation length (src/texture.rs:555-566):
+    # the deformable template, texture 0, the deformable solve's result
+    y, x = np.mgrid[0:14, 0:14].astype(np.float64)
+    small = 100.0 + 40.0 * np.sin(0.9 * x) * np.cos(0.7 * y)
+    R = gpv_mod.Image(image_gs=small, border=8)
+    dr = gpv_mod.make_desc([[7.0, 7.0]], 3, 1)
+    a = gpv_mod.solve_batch(R, R, dr, texture="rigid", tolerance=0.0, max_iterations=20)
+    b = gpv_mod.solve_batch(R, R, dr, tolerance=0.0, max_iterations=20)
     assert not R.grain()["built"] and np.all(a["texture"] == 0)
     assert np.abs(a["p"] - b["p"]).max() < 1e-9 and np.array_equal(a["iterations"], b["iterations"])
 
@@ -110,7 +114,7 @@ def test_rigid_mesh_solve(gpv_mod, oracle):
             a, b, c, e = j * 5 + i, j * 5 + i + 1, (j + 1) * 5 + i, (j + 1) * 5 + i + 1
             elements += [[a, b, e], [a, e, c]]
     mesh = gpv_mod.Mesh(nodes, np.array(elements), F, G)
-    mesh.solve(15, seed_coord=(100.3, 100.6), max_norm=1e-6, max_iterations=100, texture="rigid")
+    mesh.solve(15, seed_coord=(100.3, 100.6), max_norm=1e-5, max_iterations=100, texture="rigid")
     res = mesh.results
     assert np.all(res["texture"] == 1) and np.all(res["converged"] == 1)
     assert np.abs(res["p"][:, 4] - 0.05).max() < 0.02
