@@ -379,6 +379,30 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
 }
 
 // =====================================================================
+// The grain maps (FP32, rows x cols) at (x = column, y = row), bilinear in
+// FP64, clamped (GrainMaps::sample, src/texture.rs:125-143).
+__device__ __forceinline__ void grain_sample_f64(const float *maps, int rows, int cols, double x, double y, double h[3]) {
+    x = fmin(fmax(x, 0.0), (double)(cols - 1));
+    y = fmin(fmax(y, 0.0), (double)(rows - 1));
+    const int x0 = min((int)floor(x), max(cols - 2, 0)), y0 = min((int)floor(y), max(rows - 2, 0));
+    const int x1 = min(x0 + 1, cols - 1), y1 = min(y0 + 1, rows - 1);
+    const double tx = x - (double)x0, ty = y - (double)y0;
+    const int64_t np = (int64_t)rows * cols;
+    for (int m = 0; m < 3; m++) {
+        const float *Mp = maps + m * np;
+        h[m] = (1.0 - ty) * ((1.0 - tx) * (double)Mp[(int64_t)y0 * cols + x0] + tx * (double)Mp[(int64_t)y0 * cols + x1]) +
+               ty * ((1.0 - tx) * (double)Mp[(int64_t)y1 * cols + x0] + tx * (double)Mp[(int64_t)y1 * cols + x1]);
+    }
+}
+
+// Green-Lagrange strain [Exx, Eyy, Exy] (src/texture.rs:200-206), FP64.
+__device__ __forceinline__ void green_lagrange_f64(double ux, double vx, double uy, double vy, double &e0, double &e1,
+                                                   double &e2) {
+    e0 = ux + 0.5 * (ux * ux + vx * vx);
+    e1 = vy + 0.5 * (uy * uy + vy * vy);
+    e2 = 0.5 * (uy + vx) + 0.5 * (ux * uy + vx * vy);
+}
+
 // Forward additive Gauss-Newton (solve_fagn_result, src/subset.rs:1228-1334)
 // =====================================================================
 // One block per subset, FP64 arithmetic on FP64 coefficients when the images
@@ -391,7 +415,7 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
 // ZNSSD.  Scratch per pixel: f, df/dx, df/dy, g, dg/dx, dg/dy.
 template <int ORDER, typename C>
 __device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, double *S, int64_t nmax, BlockSmem &sm,
-                            const C *Fc, const C *Gc, int64_t pitch) {
+                            const C *Fc, const C *Gc, int64_t pitch, bool rigid_req) {
     using O = Ord<ORDER>;
     constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM;
     const int tid = threadIdx.x, nthr = blockDim.x;
@@ -454,7 +478,52 @@ __device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
     int iters = 0, status = GPV_OK;
     bool converged = false;
     double c_zncc = 0.0, c_znssd = 4.0, last_norm = 0.0, gm_last = 0.0, dg_last = 0.0;
+    // rigid texture (src/subset.rs:1257-1262): the grain maps at the subset
+    // pixels, and at every iteration the template t = f + G(E(p)) with its
+    // mean and spread in place of f, f_m and delta_f (two passes, FP64)
+    const bool rigid = rigid_req && ORDER >= 1 && A.grain_scal[4] != 0.0;
+    double *Sh = S + 6 * nmax, *St = S + 9 * nmax;
+    double tm = fm, dt = df;
+    if (rigid) {
+        for (int i = tid; i < npx_t; i += nthr) {
+            if (Sf[i] != Sf[i]) continue;
+            const short2 o = po[i];
+            double hv[3];
+            grain_sample_f64(A.grain, A.h, A.w, cx + (double)o.x, cy + (double)o.y, hv);
+            Sh[i] = hv[0]; Sh[nmax + i] = hv[1]; Sh[2 * nmax + i] = hv[2];
+        }
+    }
+    const double s2g = rigid ? A.grain_scal[2] : 0.0;
     for (int it = 1; it <= A.max_iter; it++) {
+        if (rigid) {
+            double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+            if (ORDER == 1) green_lagrange_f64(p[2 % M], p[3 % M], p[4 % M], p[5 % M], e0, e1, e2);
+            double st = 0.0;
+            for (int i = tid; i < npx_t; i += nthr) {
+                const double f = Sf[i];
+                if (f != f) continue;
+                if (ORDER == 2) {
+                    const short2 o = po[i];
+                    const double dx = o.x, dy = o.y;
+                    green_lagrange_f64(p[2 % M] + p[6 % M] * dx + p[8 % M] * dy, p[3 % M] + p[7 % M] * dx + p[9 % M] * dy,
+                                       p[4 % M] + p[8 % M] * dx + p[10 % M] * dy, p[5 % M] + p[9 % M] * dx + p[11 % M] * dy,
+                                       e0, e1, e2);
+                }
+                const double t = f + (-0.5 * s2g * (e0 * Sh[i] + e1 * Sh[nmax + i] + 2.0 * e2 * Sh[2 * nmax + i]) -
+                                      (e0 + e1) * (f - fm));
+                St[i] = t;
+                st += t;
+            }
+            st = block_sum1(st, sm);
+            tm = st / dn;
+            double stt = 0.0;
+            for (int i = tid; i < npx_t; i += nthr) {
+                if (Sf[i] != Sf[i]) continue;
+                stt += (St[i] - tm) * (St[i] - tm);
+            }
+            stt = block_sum1(stt, sm);
+            dt = sqrt(stt);
+        }
         // target value + gradient at the warped positions (:1265-1279)
         double sg = 0.0;
         for (int i = tid; i < npx_t; i += nthr) {
@@ -494,7 +563,7 @@ __device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
         const double dg = sqrt(sgg);
         // Hessian moments, residual gradient and ZNSSD in one sweep
         const double gcx = cx + p[0], gcy = cy + p[1];
-        const double ratio = dg / df;
+        const double ratio = dg / dt;
         double mom[3 * NMOM], acc[M + 1];
 #pragma unroll
         for (int q = 0; q < 3 * NMOM; q++) mom[q] = 0.0;
@@ -529,8 +598,8 @@ __device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
 #pragma unroll
                     for (int q = 0; q < 3; q++) mom[q * NMOM + mom_idx(dgr - bb, bb)] += hh[q] * mono;
                 }
-            const double a = f - fm, bq = g - gm;
-            const double z = a / df - bq / dg;
+            const double a = (rigid ? St[i] : f) - tm, bq = g - gm;
+            const double z = a / dt - bq / dg;
             acc[M] += z * z;
             const double res = a * ratio - bq;
 #pragma unroll
@@ -582,12 +651,13 @@ __device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
         auto load = [&](int i, double &f, double &gx, double &gy, double &g, double &dx, double &dy) -> bool {
             f = Sf[i];
             if (f != f) return false;
+            if (rigid) f = St[i];  // the template of the last iteration
             const short2 o = po[i];
             gx = Sgx[i]; gy = Sgy[i]; g = Sg[i]; dx = o.x; dy = o.y;
             return true;
         };
         auto red = [&](double v) { return block_sum1(v, sm); };
-        eta_sums<ORDER>(npx_t, tid, nthr, dn, fm, df, gm_last, dg_last, load, red, eu, ev);
+        eta_sums<ORDER>(npx_t, tid, nthr, dn, tm, dt, gm_last, dg_last, load, red, eu, ev);
     }
     if (tid == 0) {
         gpv_subset_result *o = A.out + idx;
@@ -608,7 +678,7 @@ __device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
         o->status = status;
         o->n_px = n;
         o->has_eta = want_eta;
-        o->texture = 0;
+        o->texture = rigid ? 1 : 0;
         o->reserved = 0;
     }
 }
@@ -617,7 +687,9 @@ __global__ void __launch_bounds__(kFp64Threads) fagn_kernel(KArgs A) {
     __shared__ BlockSmem sm;
     __shared__ int item_s;
     double *S = reinterpret_cast<double *>(A.scratch) + (int64_t)blockIdx.x * A.scratch_stride;
-    const int64_t nmax = A.scratch_stride / 6;
+    const bool rigid = (A.flags & GPV_SOLVE_RIGID_TEXTURE) != 0;
+    // per pixel: f, f_x, f_y, g, g_x, g_y (+ 3 grain samples and the template)
+    const int64_t nmax = A.scratch_stride / (rigid ? 10 : 6);
     const bool c64 = A.f64 != nullptr && A.g64 != nullptr;
     for (;;) {
         __syncthreads();
@@ -633,15 +705,15 @@ __global__ void __launch_bounds__(kFp64Threads) fagn_kernel(KArgs A) {
         }
         if (c64) {
             switch (d.order) {
-                case 0: fagn_subset<0, double>(A, idx, d, S, nmax, sm, A.f64, A.g64, A.pitch64); break;
-                case 1: fagn_subset<1, double>(A, idx, d, S, nmax, sm, A.f64, A.g64, A.pitch64); break;
-                default: fagn_subset<2, double>(A, idx, d, S, nmax, sm, A.f64, A.g64, A.pitch64); break;
+                case 0: fagn_subset<0, double>(A, idx, d, S, nmax, sm, A.f64, A.g64, A.pitch64, rigid); break;
+                case 1: fagn_subset<1, double>(A, idx, d, S, nmax, sm, A.f64, A.g64, A.pitch64, rigid); break;
+                default: fagn_subset<2, double>(A, idx, d, S, nmax, sm, A.f64, A.g64, A.pitch64, rigid); break;
             }
         } else {
             switch (d.order) {
-                case 0: fagn_subset<0, float>(A, idx, d, S, nmax, sm, A.f32, A.g32, A.pitch32); break;
-                case 1: fagn_subset<1, float>(A, idx, d, S, nmax, sm, A.f32, A.g32, A.pitch32); break;
-                default: fagn_subset<2, float>(A, idx, d, S, nmax, sm, A.f32, A.g32, A.pitch32); break;
+                case 0: fagn_subset<0, float>(A, idx, d, S, nmax, sm, A.f32, A.g32, A.pitch32, rigid); break;
+                case 1: fagn_subset<1, float>(A, idx, d, S, nmax, sm, A.f32, A.g32, A.pitch32, rigid); break;
+                default: fagn_subset<2, float>(A, idx, d, S, nmax, sm, A.f32, A.g32, A.pitch32, rigid); break;
             }
         }
     }
@@ -744,8 +816,8 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
     A.max_iter = prm->max_iterations; A.flags = prm->flags;
     A.out = L.out; A.history = L.history;
     if (prm->flags & GPV_SOLVE_RIGID_TEXTURE) {
-        if (fp64 || (prm->flags & GPV_SOLVE_FAGN) || use_warp_kernel()) {
-            set_error("the rigid-texture template needs the mixed-precision ICGN solve");
+        if (!(prm->flags & GPV_SOLVE_FAGN) && (fp64 || use_warp_kernel())) {
+            set_error("the rigid-texture template needs the mixed-precision ICGN solve or FAGN");
             return GPV_ERR_INVALID;
         }
         if (!L.f->grain) {
@@ -769,7 +841,7 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
         GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fagn_kernel, kFp64Threads, 0));
         if (per_sm < 1) per_sm = 1;
         const int workers = ctx->num_sms * per_sm;
-        const int64_t stride = 6 * ((npx_max + 31) / 32 * 32);
+        const int64_t stride = ((prm->flags & GPV_SOLVE_RIGID_TEXTURE) ? 10 : 6) * ((npx_max + 31) / 32 * 32);
         if (int rc = ctx->scratch.ensure((size_t)workers * stride * sizeof(double))) return rc;
         if (int rc = ctx->queue.ensure(64)) return rc;
         A.scratch = ctx->scratch.ptr;

@@ -68,7 +68,8 @@ typedef enum {
                                 template f + G(E(p)) rebuilt every iteration
                                 from the reference image's grain maps (f needs
                                 them: GPV_IMAGE_GRAIN or gpv_image_build_grain);
-                                orders 1 and 2, mixed-precision ICGN only.  An
+                                orders 1 and 2; mixed-precision ICGN and FAGN
+                                (not the FP64 ICGN form).  An
                                 image without measurable speckle keeps the
                                 deformable template (result texture = 0), as the
                                 reference falls back.  The branch for known

@@ -959,7 +959,25 @@ static void solve_one_fagn(const spline *F, const spline *G, const gpvo_desc *d,
     for (int k = 0; k < m; k++) p[k] = d->p0[k];
     int converged = 0, iters = 0, status = ST_OK;
     double last_norm = 0.0, c_zncc = 0.0, c_znssd = 4.0;
+    /* rigid texture (src/subset.rs:1257-1262): the template rebuilt from the
+     * current warp at every iteration, in place of f, f_m, delta_f */
+    const int rigid = (prm->flags & 8) && order >= 1 && prm->grain;
+    double *hmap = NULL, *tf = NULL, *off = NULL, tf_m = s.f_m, delta_tf = s.delta_f;
+    const double *fv = s.f;
+    if (rigid) {
+        hmap = (double *)malloc(sizeof(double) * 3 * n);
+        tf = (double *)malloc(sizeof(double) * n);
+        off = (double *)malloc(sizeof(double) * 2 * n);
+        for (int64_t i = 0; i < n; i++) {
+            grain_sample(prm->grain, prm->gh, prm->gw, s.fc[2 * i], s.fc[2 * i + 1], hmap + 3 * i);
+            off[2 * i] = s.fc[2 * i] - d->coord[0];
+            off[2 * i + 1] = s.fc[2 * i + 1] - d->coord[1];
+        }
+        fv = tf;
+    }
     for (int it = 1; it <= prm->max_iterations; it++) {
+        if (rigid) rigid_template(s.f, s.f_m, hmap, prm->s2, p, m, off, n, tf, &tf_m, &delta_tf);
+        const double f_m_t = rigid ? tf_m : s.f_m, df_t = rigid ? delta_tf : s.delta_f;
         double g_center[2] = {d->coord[0] + p[0], d->coord[1] + p[1]};
         for (int64_t i = 0; i < n; i++) {
             warp_point(d->coord, p, m, s.fc[2 * i], s.fc[2 * i + 1], &gc[2 * i], &gc[2 * i + 1]);
@@ -981,7 +999,7 @@ static void solve_one_fagn(const spline *F, const spline *G, const gpvo_desc *d,
         for (int k = 0; k < m; k++) grad_z[k] = 0.0;
         for (int k = 0; k < m; k++)
             for (int64_t i = 0; i < n; i++)
-                grad_z[k] += sdi[i * m + k] * ((s.f[i] - s.f_m) * (delta_g / s.delta_f) - (g[i] - g_m));
+                grad_z[k] += sdi[i * m + k] * ((fv[i] - f_m_t) * (delta_g / df_t) - (g[i] - g_m));
         if (!invert(H, m, Hi)) { status = ST_SINGULAR_H; break; }  /* the reference panics */
         for (int k = 0; k < m; k++) {
             double acc = 0.0;
@@ -990,7 +1008,7 @@ static void solve_one_fagn(const spline *F, const spline *G, const gpvo_desc *d,
         }
         for (int k = 0; k < m; k++) p[k] += dp[k];
         double nrm = gpvo_norm(dp, m, size);
-        double z = gpvo_znssd(s.f, g, n, s.f_m, g_m, s.delta_f, delta_g);
+        double z = gpvo_znssd(fv, g, n, f_m_t, g_m, df_t, delta_g);
         c_znssd = z;
         c_zncc = 1.0 - z / 2.0;
         iters = it;
@@ -1009,10 +1027,13 @@ static void solve_one_fagn(const spline *F, const spline *G, const gpvo_desc *d,
         for (int64_t i = 0; i < n; i++) gs += g[i];
         double g_m = gs / (double)n, gss = 0.0;
         for (int64_t i = 0; i < n; i++) gss += (g[i] - g_m) * (g[i] - g_m);
-        gpvo_eta(d->coord, order, s.fc, s.grad, s.f, s.f_m, s.delta_f, g, g_m, sqrt(gss), n, &r->eta_u, &r->eta_v);
+        gpvo_eta(d->coord, order, s.fc, s.grad, fv, rigid ? tf_m : s.f_m, rigid ? delta_tf : s.delta_f, g, g_m,
+                 sqrt(gss), n, &r->eta_u, &r->eta_v);
         r->has_eta = 1;
     }
+    r->texture = rigid;
     free(sdi); free(g); free(gc); free(gg); subset_free(&s);
+    free(hmap); free(tf); free(off);
 }
 
 /* load_grayscale + gaussian_blur_5x5 (src/image.rs:450-534) on decoded RGB8

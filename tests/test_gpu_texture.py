@@ -7,8 +7,9 @@
   (src/texture.rs:424-437): displacement within 1e-3 px and gradient terms
   within 1e-5 of the FP64 oracle's rigid solve, identical flags, texture = 1;
   better than the deformable template at order 1 (src/texture.rs:481-500);
-  the deformable template for order 0 and for an image without measurable
-  speckle; refused for the FP64 and FAGN forms.
+  FAGN with the rigid template against the oracle's; the deformable template
+  for order 0 and for an image without measurable speckle; refused for the
+  FP64 ICGN form.
 """
 import numpy as np
 import pytest
@@ -74,6 +75,30 @@ def test_rigid_solve_matches_the_oracle(gpv_mod, oracle, order, gamma):
         assert np.abs(gr["p"][:, 4] - gamma).mean() < np.abs(gd["p"][:, 4] - gamma).mean()
 
 
+@pytest.mark.parametrize("order", [1, 2])
+def test_rigid_fagn_matches_the_oracle(gpv_mod, oracle, order):
+    """FAGN with the rigid template (src/subset.rs:1228-1334), FP64 arithmetic:
+    on FP64 coefficients within 1e-6 px of the oracle (the maps are held in
+    FP32, the oracle's in FP64), on FP32 coefficients within the mixed bar."""
+    gamma = 0.05
+    f, g = TC.shear_pair(gamma)
+    d = TC.grid_desc(gpv_mod, gamma, order)
+    kw = dict(max_norm=1e-6, max_iterations=100, tolerance=0.75, method="fagn", texture="rigid")
+    maps, s2 = oracle.grain(f)
+    cf, cg = oracle.get_c(f, 8), oracle.get_c(g, 8)
+    ref = oracle.solve_batch(cf, cg, f.shape, 8, d, grain=(maps, s2), eta=True,
+                             **{k: v for k, v in kw.items() if k != "texture"})
+    assert np.all(ref["texture"] == 1)
+    for keep, prec, tol in ((True, gpv_mod.PREC_FP64, 1e-6), (False, gpv_mod.PREC_MIXED, 1e-3)):
+        F = gpv_mod.Image(image_gs=f, border=8, keep_f64=keep)
+        G = gpv_mod.Image(image_gs=g, border=8, keep_f64=keep)
+        r = gpv_mod.solve_batch(F, G, d, precision=prec, eta=True, **kw)
+        assert np.all(r["texture"] == 1)
+        assert np.array_equal(r["converged"], ref["converged"]) and np.array_equal(r["status"], ref["status"])
+        assert np.abs(r["p"][:, :2] - ref["p"][:, :2]).max() <= tol
+        assert np.abs(r["p"][:, 2:6] - ref["p"][:, 2:6]).max() <= tol * 1e-2
+
+
 def test_rigid_falls_back_and_is_refused_where_unsupported(gpv_mod):
     from gpv import synth
     W = synth.workload(1, scale_down=4)
@@ -85,8 +110,6 @@ def test_rigid_falls_back_and_is_refused_where_unsupported(gpv_mod):
     d1 = gpv_mod.make_desc(W["coords"][:40], 25, 1, W["p0"][:40])
     with pytest.raises(gpv_mod.GpvError):
         gpv_mod.solve_batch(F, G, d1, texture="rigid", precision=gpv_mod.PREC_FP64)
-    with pytest.raises(gpv_mod.GpvError):
-        gpv_mod.solve_batch(F, G, d1, texture="rigid", method="fagn")
     with pytest.raises(ValueError):
         gpv_mod.solve_batch(F, G, d1, texture="grainy")
     # textured but too small to measure a correlation length (src/texture.rs:555-566):

@@ -118,3 +118,25 @@ def test_rigid_icgn_matches_deformable_at_zero_strain(oracle, order):
     assert np.all(rd["converged"] == 1) and np.all(rr["converged"] == 1)
     assert abs(np.abs(rd["p"][:, 4]).mean() - np.abs(rr["p"][:, 4]).mean()) < 1e-6
     assert abs(rd["c_znssd"].mean() - rr["c_znssd"].mean()) < 1e-9
+
+
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("gamma", [0.0, 0.05, 0.1])
+def test_rigid_fagn_helps_on_rigid_speckle_shear(oracle, order, gamma):
+    """src/texture.rs:513-530: FAGN with the rigid template converges
+    everywhere, matches the deformable fit at zero strain and fits better
+    under shear at order 1."""
+    import gpv
+    f, g = TC.shear_pair(gamma)
+    cf, cg = oracle.get_c(f, 8), oracle.get_c(g, 8)
+    d = TC.grid_desc(gpv, gamma, order)
+    maps, s2 = oracle.grain(f)
+    kw = dict(max_norm=1e-6, max_iterations=100, tolerance=0.75, method="fagn")
+    rd = oracle.solve_batch(cf, cg, f.shape, 8, d, **kw)
+    rr = oracle.solve_batch(cf, cg, f.shape, 8, d, grain=(maps, s2), **kw)
+    assert np.all(rr["converged"] == 1) and np.all(rr["texture"] == 1)
+    ed, er = np.abs(rd["p"][:, 4] - gamma).mean(), np.abs(rr["p"][:, 4] - gamma).mean()
+    if gamma == 0.0:
+        assert abs(ed - er) < 1e-6 and abs(rd["c_znssd"].mean() - rr["c_znssd"].mean()) < 1e-9
+    elif order == 1:
+        assert rr["c_znssd"].mean() < rd["c_znssd"].mean() and er < ed
