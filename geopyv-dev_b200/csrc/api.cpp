@@ -489,6 +489,7 @@ int gpv_image_destroy(gpv_image *img) {
     cudaFree(img->px_dev);
     cudaFree(img->rgb_dev);
     cudaFree(img->grain);
+    cudaFree(img->grain64);
     cudaFree(img->grain_scal);
     cudaFree(img->grain_ac);
     gpv_context *ctx = img->ctx;
@@ -500,14 +501,16 @@ int gpv_image_destroy(gpv_image *img) {
 static int grain_alloc(gpv_image *img) {
     if (img->grain) return GPV_SUCCESS;
     cudaError_t e = cudaMalloc(&img->grain, sizeof(float) * 3 * (size_t)img->h * (size_t)img->w);
+    if (e == cudaSuccess && img->c64) e = cudaMalloc(&img->grain64, sizeof(double) * 3 * (size_t)img->h * (size_t)img->w);
     if (e == cudaSuccess) e = cudaMalloc(&img->grain_scal, sizeof(double) * 8);
     if (e == cudaSuccess) e = cudaMalloc(&img->grain_ac, sizeof(double) * 512);
     if (e != cudaSuccess) {
         cudaFree(img->grain);
+        cudaFree(img->grain64);
         cudaFree(img->grain_scal);
         cudaFree(img->grain_ac);
         img->grain = nullptr;
-        img->grain_scal = img->grain_ac = nullptr;
+        img->grain64 = img->grain_scal = img->grain_ac = nullptr;
         set_error(std::string("grain maps: ") + cudaGetErrorString(e));
         return GPV_ERR_NOMEM;
     }

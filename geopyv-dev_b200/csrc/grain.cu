@@ -19,7 +19,8 @@
 //   weights and replicated edges (filter_1d, :70-93).  Each output is a
 //   left-to-right FP64 sum of products with explicitly rounded multiplies
 //   and adds (no fused multiply-add), as the reference's loop computes it;
-//   stored as FP32 for the mixed-precision solve.  A block makes a 32 x 8
+//   stored as FP32 for the mixed-precision solve, and in FP64 as well for an
+//   image that keeps FP64 coefficients (the FP64 solve forms).  A block makes a 32 x 8
 //   tile from its pixels plus a 4-pixel apron staged in shared memory.
 //
 // Everything runs on the image's stream with no host synchronisation: the
@@ -116,7 +117,8 @@ __global__ void grain_finalize(const double *ac, int half, double *scal) {
     }
 }
 
-__global__ void grain_maps(const void *px, int dtype, int h, int w, GrainTaps t, const double *scal, float *maps) {
+__global__ void grain_maps(const void *px, int dtype, int h, int w, GrainTaps t, const double *scal, float *maps,
+                           double *maps64) {
     __shared__ double a[kTh + 2 * kR][kTw + 2 * kR];
     __shared__ double rp[3][kTh + 2 * kR][kTw];  // row passes with k0, k1, k2
     if (scal[4] == 0.0) return;
@@ -150,7 +152,9 @@ __global__ void grain_maps(const void *px, int dtype, int h, int w, GrainTaps t,
         double s = 0.0;
 #pragma unroll
         for (int j = 0; j < kTaps; j++) s = __dadd_rn(s, __dmul_rn(t.k[colk[m]][j], rp[rowk[m]][threadIdx.y + j][threadIdx.x]));
-        maps[m * np + (int64_t)y * w + x] = (float)__dmul_rn(s, corr);
+        const double v = __dmul_rn(s, corr);
+        maps[m * np + (int64_t)y * w + x] = (float)v;
+        if (maps64) maps64[m * np + (int64_t)y * w + x] = v;
     }
 }
 
@@ -182,7 +186,8 @@ int grain_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s) 
     crop_lags<<<dim3(half, 2), kRedThreads, 0, s>>>(px_dev, dtype, w, r0, c0, side, img->grain_scal, img->grain_ac);
     grain_finalize<<<1, 1, 0, s>>>(img->grain_ac, half, img->grain_scal);
     dim3 grid((unsigned)((w + kTw - 1) / kTw), (unsigned)((h + kTh - 1) / kTh));
-    grain_maps<<<grid, dim3(kTw, kTh), 0, s>>>(px_dev, dtype, (int)h, (int)w, grain_taps(), img->grain_scal, img->grain);
+    grain_maps<<<grid, dim3(kTw, kTh), 0, s>>>(px_dev, dtype, (int)h, (int)w, grain_taps(), img->grain_scal, img->grain,
+                                               img->grain64);
     GPV_CUDA_TRY(cudaGetLastError());
     return GPV_SUCCESS;
 }

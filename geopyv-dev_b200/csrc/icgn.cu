@@ -125,8 +125,34 @@ __device__ bool gj_inverse_serial(const double *Ain, double *Ainv) {
     return true;
 }
 
+// The grain maps (rows x cols, FP32 or FP64) at (x = column, y = row),
+// bilinear in FP64, clamped (GrainMaps::sample, src/texture.rs:125-143).
+template <typename T>
+__device__ __forceinline__ void grain_sample_f64(const T *maps, int rows, int cols, double x, double y, double h[3]) {
+    x = fmin(fmax(x, 0.0), (double)(cols - 1));
+    y = fmin(fmax(y, 0.0), (double)(rows - 1));
+    const int x0 = min((int)floor(x), max(cols - 2, 0)), y0 = min((int)floor(y), max(rows - 2, 0));
+    const int x1 = min(x0 + 1, cols - 1), y1 = min(y0 + 1, rows - 1);
+    const double tx = x - (double)x0, ty = y - (double)y0;
+    const int64_t np = (int64_t)rows * cols;
+    for (int m = 0; m < 3; m++) {
+        const T *Mp = maps + m * np;
+        h[m] = (1.0 - ty) * ((1.0 - tx) * (double)Mp[(int64_t)y0 * cols + x0] + tx * (double)Mp[(int64_t)y0 * cols + x1]) +
+               ty * ((1.0 - tx) * (double)Mp[(int64_t)y1 * cols + x0] + tx * (double)Mp[(int64_t)y1 * cols + x1]);
+    }
+}
+
+// Green-Lagrange strain [Exx, Eyy, Exy] (src/texture.rs:200-206), FP64.
+__device__ __forceinline__ void green_lagrange_f64(double ux, double vx, double uy, double vy, double &e0, double &e1,
+                                                   double &e2) {
+    e0 = ux + 0.5 * (ux * ux + vx * vx);
+    e1 = vy + 0.5 * (uy * uy + vy * vy);
+    e2 = 0.5 * (uy + vx) + 0.5 * (ux * uy + vx * vy);
+}
+
 template <int ORDER>
-__device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, double *S, int64_t nmax, BlockSmem &sm) {
+__device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, double *S, int64_t nmax, BlockSmem &sm,
+                            bool rigid_req) {
     using O = Ord<ORDER>;
     constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM;
     const int tid = threadIdx.x, nthr = blockDim.x;
@@ -229,7 +255,53 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
     int iters = 0, status = GPV_OK;
     bool converged = false;
     double c_zncc = 0.0, c_znssd = 4.0, last_norm = 0.0, gm_last = 0.0, dg_last = 0.0;
+    // rigid texture (src/subset.rs:1151-1168): the grain maps at the subset
+    // pixels, and at every iteration the template t = f + G(E(p)) with its
+    // mean and spread in place of f, f_m and delta_f (two passes, FP64)
+    const bool rigid = rigid_req && ORDER >= 1 && A.grain_scal[4] != 0.0;
+    double *Sh = S + 4 * nmax, *St = S + 7 * nmax;
+    double tm = fm, dt = df;
+    if (rigid) {
+        for (int i = tid; i < npx_t; i += nthr) {
+            if (Sf[i] != Sf[i]) continue;
+            const short2 o = po[i];
+            double hv[3];
+            if (A.grain64) grain_sample_f64(A.grain64, A.h, A.w, cx + (double)o.x, cy + (double)o.y, hv);
+            else grain_sample_f64(A.grain, A.h, A.w, cx + (double)o.x, cy + (double)o.y, hv);
+            Sh[i] = hv[0]; Sh[nmax + i] = hv[1]; Sh[2 * nmax + i] = hv[2];
+        }
+    }
+    const double s2g = rigid ? A.grain_scal[2] : 0.0;
     for (int it = 1; it <= A.max_iter; it++) {
+        if (rigid) {
+            double e0 = 0.0, e1 = 0.0, e2 = 0.0;
+            if (ORDER == 1) green_lagrange_f64(p[2 % M], p[3 % M], p[4 % M], p[5 % M], e0, e1, e2);
+            double st = 0.0;
+            for (int i = tid; i < npx_t; i += nthr) {
+                const double f = Sf[i];
+                if (f != f) continue;
+                if (ORDER == 2) {
+                    const short2 o = po[i];
+                    const double dx = o.x, dy = o.y;
+                    green_lagrange_f64(p[2 % M] + p[6 % M] * dx + p[8 % M] * dy, p[3 % M] + p[7 % M] * dx + p[9 % M] * dy,
+                                       p[4 % M] + p[8 % M] * dx + p[10 % M] * dy, p[5 % M] + p[9 % M] * dx + p[11 % M] * dy,
+                                       e0, e1, e2);
+                }
+                const double t = f + (-0.5 * s2g * (e0 * Sh[i] + e1 * Sh[nmax + i] + 2.0 * e2 * Sh[2 * nmax + i]) -
+                                      (e0 + e1) * (f - fm));
+                St[i] = t;
+                st += t;
+            }
+            st = block_sum1(st, sm);
+            tm = st / dn;
+            double stt = 0.0;
+            for (int i = tid; i < npx_t; i += nthr) {
+                if (Sf[i] != Sf[i]) continue;
+                stt += (St[i] - tm) * (St[i] - tm);
+            }
+            stt = block_sum1(stt, sm);
+            dt = sqrt(stt);
+        }
         // apply_warp_into + eval (:1158-1161)
         double sg = 0.0;
         for (int i = tid; i < npx_t; i += nthr) {
@@ -267,7 +339,7 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
         sgg = block_sum1(sgg, sm);
         const double dg = sqrt(sgg);
         // delta_p_and_znssd_icgn (:418-446)
-        const double ratio = df / dg;
+        const double ratio = dt / dg;
         double acc[M + 1];
 #pragma unroll
         for (int k = 0; k <= M; k++) acc[k] = 0.0;
@@ -275,8 +347,8 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
             const double f = Sf[i];
             if (f != f) continue;
             const short2 o = po[i];
-            const double a = f - fm, b = Sg[i] - gm;
-            const double z = a / df - b / dg;
+            const double a = (rigid ? St[i] : f) - tm, b = Sg[i] - gm;
+            const double z = a / dt - b / dg;
             acc[M] += z * z;
             const double br = a - ratio * b;
             const double gx = Sgx[i], gy = Sgy[i], dx = o.x, dy = o.y;
@@ -347,12 +419,13 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
         auto load = [&](int i, double &f, double &gx, double &gy, double &g, double &dx, double &dy) -> bool {
             f = Sf[i];
             if (f != f) return false;
+            if (rigid) f = St[i];  // the template of the last iteration
             const short2 o = po[i];
             gx = Sgx[i]; gy = Sgy[i]; g = Sg[i]; dx = o.x; dy = o.y;
             return true;
         };
         auto red = [&](double v) { return block_sum1(v, sm); };
-        eta_sums<ORDER>(npx_t, tid, nthr, dn, fm, df, gm_last, dg_last, load, red, eu, ev);
+        eta_sums<ORDER>(npx_t, tid, nthr, dn, tm, dt, gm_last, dg_last, load, red, eu, ev);
     }
     if (tid == 0) {
         gpv_subset_result *o = A.out + idx;
@@ -373,36 +446,12 @@ __device__ void fp64_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
         o->status = status;
         o->n_px = n;
         o->has_eta = want_eta;
-        o->texture = 0;
+        o->texture = rigid ? 1 : 0;
         o->reserved = 0;
     }
 }
 
 // =====================================================================
-// The grain maps (FP32, rows x cols) at (x = column, y = row), bilinear in
-// FP64, clamped (GrainMaps::sample, src/texture.rs:125-143).
-__device__ __forceinline__ void grain_sample_f64(const float *maps, int rows, int cols, double x, double y, double h[3]) {
-    x = fmin(fmax(x, 0.0), (double)(cols - 1));
-    y = fmin(fmax(y, 0.0), (double)(rows - 1));
-    const int x0 = min((int)floor(x), max(cols - 2, 0)), y0 = min((int)floor(y), max(rows - 2, 0));
-    const int x1 = min(x0 + 1, cols - 1), y1 = min(y0 + 1, rows - 1);
-    const double tx = x - (double)x0, ty = y - (double)y0;
-    const int64_t np = (int64_t)rows * cols;
-    for (int m = 0; m < 3; m++) {
-        const float *Mp = maps + m * np;
-        h[m] = (1.0 - ty) * ((1.0 - tx) * (double)Mp[(int64_t)y0 * cols + x0] + tx * (double)Mp[(int64_t)y0 * cols + x1]) +
-               ty * ((1.0 - tx) * (double)Mp[(int64_t)y1 * cols + x0] + tx * (double)Mp[(int64_t)y1 * cols + x1]);
-    }
-}
-
-// Green-Lagrange strain [Exx, Eyy, Exy] (src/texture.rs:200-206), FP64.
-__device__ __forceinline__ void green_lagrange_f64(double ux, double vx, double uy, double vy, double &e0, double &e1,
-                                                   double &e2) {
-    e0 = ux + 0.5 * (ux * ux + vx * vx);
-    e1 = vy + 0.5 * (uy * uy + vy * vy);
-    e2 = 0.5 * (uy + vx) + 0.5 * (ux * uy + vx * vy);
-}
-
 // Forward additive Gauss-Newton (solve_fagn_result, src/subset.rs:1228-1334)
 // =====================================================================
 // One block per subset, FP64 arithmetic on FP64 coefficients when the images
@@ -489,7 +538,8 @@ __device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
             if (Sf[i] != Sf[i]) continue;
             const short2 o = po[i];
             double hv[3];
-            grain_sample_f64(A.grain, A.h, A.w, cx + (double)o.x, cy + (double)o.y, hv);
+            if (A.grain64) grain_sample_f64(A.grain64, A.h, A.w, cx + (double)o.x, cy + (double)o.y, hv);
+            else grain_sample_f64(A.grain, A.h, A.w, cx + (double)o.x, cy + (double)o.y, hv);
             Sh[i] = hv[0]; Sh[nmax + i] = hv[1]; Sh[2 * nmax + i] = hv[2];
         }
     }
@@ -723,7 +773,9 @@ __global__ void __launch_bounds__(kFp64Threads) icgn_fp64(KArgs A) {
     __shared__ BlockSmem sm;
     __shared__ int item_s;
     double *S = reinterpret_cast<double *>(A.scratch) + (int64_t)blockIdx.x * A.scratch_stride;
-    const int64_t nmax = A.scratch_stride / 4;
+    const bool rigid = (A.flags & GPV_SOLVE_RIGID_TEXTURE) != 0;
+    // per pixel: f, f_x, f_y, g (+ 3 grain samples and the template)
+    const int64_t nmax = A.scratch_stride / (rigid ? 8 : 4);
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) item_s = atomicAdd(A.queue, 1);
@@ -737,9 +789,9 @@ __global__ void __launch_bounds__(kFp64Threads) icgn_fp64(KArgs A) {
             continue;
         }
         switch (d.order) {
-            case 0: fp64_subset<0>(A, idx, d, S, nmax, sm); break;
-            case 1: fp64_subset<1>(A, idx, d, S, nmax, sm); break;
-            default: fp64_subset<2>(A, idx, d, S, nmax, sm); break;
+            case 0: fp64_subset<0>(A, idx, d, S, nmax, sm, rigid); break;
+            case 1: fp64_subset<1>(A, idx, d, S, nmax, sm, rigid); break;
+            default: fp64_subset<2>(A, idx, d, S, nmax, sm, rigid); break;
         }
     }
 }
@@ -816,8 +868,8 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
     A.max_iter = prm->max_iterations; A.flags = prm->flags;
     A.out = L.out; A.history = L.history;
     if (prm->flags & GPV_SOLVE_RIGID_TEXTURE) {
-        if (!(prm->flags & GPV_SOLVE_FAGN) && (fp64 || use_warp_kernel())) {
-            set_error("the rigid-texture template needs the mixed-precision ICGN solve or FAGN");
+        if (!(prm->flags & GPV_SOLVE_FAGN) && !fp64 && use_warp_kernel()) {
+            set_error("the rigid-texture template is not built into the warp-per-subset kernel");
             return GPV_ERR_INVALID;
         }
         if (!L.f->grain) {
@@ -826,6 +878,7 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
             return GPV_ERR_INVALID;
         }
         A.grain = L.f->grain;
+        A.grain64 = L.f->grain64;
         A.grain_scal = L.f->grain_scal;
     }
     const int64_t npx_max = ctx->h_tab_n[L.max_radius];
@@ -875,7 +928,7 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
         threads = kMixedWarps * 32;
         elem = sizeof(float);
     }
-    const int64_t stride = 4 * ((npx_max + 31) / 32 * 32);
+    const int64_t stride = ((fp64 && (prm->flags & GPV_SOLVE_RIGID_TEXTURE)) ? 8 : 4) * ((npx_max + 31) / 32 * 32);
     const size_t need = (size_t)workers * stride * elem;
     if (int rc = ctx->scratch.ensure(need)) return rc;
     if (int rc = ctx->queue.ensure(64)) return rc;

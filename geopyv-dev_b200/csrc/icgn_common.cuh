@@ -37,6 +37,7 @@ struct KArgs {
     int64_t scratch_stride;  // elements (float for mixed, double for fp64) per worker
     int *queue;
     const float *grain = nullptr;        // rigid texture: f's grain maps (3 x h x w)
+    const double *grain64 = nullptr;     // the same in FP64, or null
     const double *grain_scal = nullptr;  // [mean, correlation length, s2, corr, built]
 };
 

@@ -125,6 +125,7 @@ struct gpv_image {
     // rigid-texture speckle statistics (grain.cu): fxx, fyy, fxy maps (3 h w
     // FP32) and [mean, correlation length, s2, corr, built] on the device
     float *grain = nullptr;
+    double *grain64 = nullptr;  // the same maps in FP64 (images that keep FP64 coefficients)
     double *grain_scal = nullptr;
     double *grain_ac = nullptr;  // autocorrelation lag sums (2 x 256)
 };

@@ -68,8 +68,9 @@ typedef enum {
                                 template f + G(E(p)) rebuilt every iteration
                                 from the reference image's grain maps (f needs
                                 them: GPV_IMAGE_GRAIN or gpv_image_build_grain);
-                                orders 1 and 2; mixed-precision ICGN and FAGN
-                                (not the FP64 ICGN form).  An
+                                orders 1 and 2; ICGN in both precisions and
+                                FAGN (an image with FP64 coefficients keeps
+                                the maps in FP64 too).  An
                                 image without measurable speckle keeps the
                                 deformable template (result texture = 0), as the
                                 reference falls back.  The branch for known

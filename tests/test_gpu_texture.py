@@ -7,9 +7,9 @@
   (src/texture.rs:424-437): displacement within 1e-3 px and gradient terms
   within 1e-5 of the FP64 oracle's rigid solve, identical flags, texture = 1;
   better than the deformable template at order 1 (src/texture.rs:481-500);
-  FAGN with the rigid template against the oracle's; the deformable template
-  for order 0 and for an image without measurable speckle; refused for the
-  FP64 ICGN form.
+  FAGN and the FP64 ICGN form with the rigid template against the oracle's
+  (FP64 maps: the FP64 bars); the deformable template for order 0 and for an
+  image without measurable speckle; maps refused for device-created images.
 """
 import numpy as np
 import pytest
@@ -78,8 +78,8 @@ def test_rigid_solve_matches_the_oracle(gpv_mod, oracle, order, gamma):
 @pytest.mark.parametrize("order", [1, 2])
 def test_rigid_fagn_matches_the_oracle(gpv_mod, oracle, order):
     """FAGN with the rigid template (src/subset.rs:1228-1334), FP64 arithmetic:
-    on FP64 coefficients within 1e-6 px of the oracle (the maps are held in
-    FP32, the oracle's in FP64), on FP32 coefficients within the mixed bar."""
+    on FP64 coefficients (and FP64 grain maps) within 1e-8 px of the oracle,
+    on FP32 coefficients and maps within the mixed bar."""
     gamma = 0.05
     f, g = TC.shear_pair(gamma)
     d = TC.grid_desc(gpv_mod, gamma, order)
@@ -89,7 +89,7 @@ def test_rigid_fagn_matches_the_oracle(gpv_mod, oracle, order):
     ref = oracle.solve_batch(cf, cg, f.shape, 8, d, grain=(maps, s2), eta=True,
                              **{k: v for k, v in kw.items() if k != "texture"})
     assert np.all(ref["texture"] == 1)
-    for keep, prec, tol in ((True, gpv_mod.PREC_FP64, 1e-6), (False, gpv_mod.PREC_MIXED, 1e-3)):
+    for keep, prec, tol in ((True, gpv_mod.PREC_FP64, 1e-8), (False, gpv_mod.PREC_MIXED, 1e-3)):
         F = gpv_mod.Image(image_gs=f, border=8, keep_f64=keep)
         G = gpv_mod.Image(image_gs=g, border=8, keep_f64=keep)
         r = gpv_mod.solve_batch(F, G, d, precision=prec, eta=True, **kw)
@@ -97,6 +97,29 @@ def test_rigid_fagn_matches_the_oracle(gpv_mod, oracle, order):
         assert np.array_equal(r["converged"], ref["converged"]) and np.array_equal(r["status"], ref["status"])
         assert np.abs(r["p"][:, :2] - ref["p"][:, :2]).max() <= tol
         assert np.abs(r["p"][:, 2:6] - ref["p"][:, 2:6]).max() <= tol * 1e-2
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_rigid_fp64_icgn_matches_the_oracle(gpv_mod, oracle, order):
+    """The plain FP64 ICGN form with the rigid template: FP64 coefficients and
+    FP64 grain maps (equal to the oracle's), displacement within 1e-9 px,
+    gradients within 1e-11, identical iterations and flags -- the FP64 form's
+    bar."""
+    gamma = 0.05
+    f, g = TC.shear_pair(gamma)
+    d = TC.grid_desc(gpv_mod, gamma, order)
+    kw = dict(max_norm=1e-6, max_iterations=100, tolerance=0.75)
+    maps, s2 = oracle.grain(f)
+    cf, cg = oracle.get_c(f, 8), oracle.get_c(g, 8)
+    ref = oracle.solve_batch(cf, cg, f.shape, 8, d, grain=(maps, s2), eta=True, **kw)
+    F = gpv_mod.Image(image_gs=f, border=8, keep_f64=True)
+    G = gpv_mod.Image(image_gs=g, border=8, keep_f64=True)
+    r = gpv_mod.solve_batch(F, G, d, precision=gpv_mod.PREC_FP64, texture="rigid", eta=True, **kw)
+    assert np.all(r["texture"] == 1) and np.all(ref["texture"] == 1)
+    assert np.array_equal(r["converged"], ref["converged"]) and np.array_equal(r["iterations"], ref["iterations"])
+    assert np.abs(r["p"][:, :2] - ref["p"][:, :2]).max() < 1e-9
+    assert np.abs(r["p"][:, 2:] - ref["p"][:, 2:]).max() < 1e-11
+    assert np.abs(r["eta_u"] - ref["eta_u"]).max() < 1e-9
 
 
 def test_rigid_falls_back_and_is_refused_where_unsupported(gpv_mod):
@@ -108,8 +131,17 @@ def test_rigid_falls_back_and_is_refused_where_unsupported(gpv_mod):
     r = gpv_mod.solve_batch(F, G, d, texture="rigid")  # order 0: deformable
     assert np.all(r["texture"] == 0) and np.mean(r["converged"]) > 0.9
     d1 = gpv_mod.make_desc(W["coords"][:40], 25, 1, W["p0"][:40])
-    with pytest.raises(gpv_mod.GpvError):
-        gpv_mod.solve_batch(F, G, d1, texture="rigid", precision=gpv_mod.PREC_FP64)
+    with pytest.raises(gpv_mod.GpvError):  # a device-created image has no staged pixels for the maps
+        import torch
+        dev = torch.from_numpy(np.ascontiguousarray(W["f"])).cuda()
+        Fd = gpv_mod.Image.__new__(gpv_mod.Image)
+        Fd.ctx, Fd.shape, Fd.dtype, Fd.border, Fd.keep_f64 = F.ctx, W["f"].shape, W["f"].dtype, 20, False
+        h = gpv_mod.ct.c_void_p()
+        gpv_mod.check(gpv_mod.lib().gpv_image_create_device(F.ctx.handle, gpv_mod.ct.c_void_p(dev.data_ptr()),
+                                                             gpv_mod._lib.DTYPES[W["f"].dtype], W["f"].shape[0],
+                                                             W["f"].shape[1], 20, 0, gpv_mod.ct.byref(h)), "create")
+        Fd._h = h
+        Fd.build_grain()
     with pytest.raises(ValueError):
         gpv_mod.solve_batch(F, G, d1, texture="grainy")
     # textured but too small to measure a correlation length (src/texture.rs:555-566):
