@@ -148,6 +148,10 @@ int default_execute(gpv_server *S, Worker &W, Request &q, gpv_subset_result *out
         }
         F = pair.first;
     }
+    // the rigid texture reads the reference's grain maps: built on the first
+    // such request (an allocation), then kept up to date with every upload
+    if ((r.params.flags & GPV_SOLVE_RIGID_TEXTURE) && !F->grain)
+        if (int rc = gpv_image_build_grain(F)) return rc;
     // seeds from the session's previous converged warps
     if (sess && (r.flags & GPV_REQUEST_SEED_FROM_PREVIOUS) && (int64_t)sess->last.size() == r.n) {
         for (int64_t i = 0; i < r.n; i++) {

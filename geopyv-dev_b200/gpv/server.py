@@ -67,7 +67,8 @@ class Server:
                                        _lib.DTYPES[np.dtype(dtype)], timeout_ms), "gpv_server_prepare")
 
     def submit(self, f_px, g_px, desc, border: int = 20, max_norm=1e-5, max_iterations=50, tolerance=0.75,
-               session: int = 0, reuse_reference: bool = False, seed_from_previous: bool = False) -> Ticket:
+               session: int = 0, reuse_reference: bool = False, seed_from_previous: bool = False,
+               texture: str = "deformable") -> Ticket:
         g = np.ascontiguousarray(g_px)
         if g.dtype not in _lib.DTYPES:
             raise TypeError(f"unsupported pixel dtype {g.dtype}")
@@ -84,7 +85,10 @@ class Server:
         r.h, r.w = g.shape
         r.desc = d.ctypes.data
         r.n = d.size
-        r.params = SolveParams(max_norm=max_norm, tolerance=tolerance, max_iterations=max_iterations, flags=0,
+        if texture not in ("deformable", "rigid"):
+            raise ValueError(f"texture must be 'deformable' or 'rigid', got {texture!r}")
+        r.params = SolveParams(max_norm=max_norm, tolerance=tolerance, max_iterations=max_iterations,
+                               flags=_lib.SOLVE_RIGID_TEXTURE if texture == "rigid" else 0,
                                precision=PREC_MIXED, reserved=0, mask=None, history=None)
         r.session = session
         r.flags = (_lib.REQUEST_REUSE_REFERENCE if reuse_reference else 0) | \

@@ -95,6 +95,22 @@ def test_priority_lane_results_equal_results_alone(gpv_mod):
         assert alone.tobytes() == got.tobytes()
 
 
+def test_rigid_texture_requests_equal_solves_alone(gpv_mod):
+    """A served request with the rigid texture (the worker builds the
+    reference's grain maps) returns the bytes of the same solve alone."""
+    rng = np.random.default_rng(31)
+    reqs = [_request(rng, 512, np.uint8, 300, 810), _request(rng, 256, np.uint16, 120, 811)]
+    srv = gpv_mod.Server(workers=2)
+    got = [srv.wait(srv.submit(f, g, d, texture="rigid"), 120000).copy() for f, g, d in reqs]
+    srv.close()
+    for (f, g, d), r in zip(reqs, got):
+        ctx = gpv_mod.Context(0)
+        alone = gpv_mod.solve_batch(gpv_mod.Image(image_gs=f, ctx=ctx), gpv_mod.Image(image_gs=g, ctx=ctx), d,
+                                    texture="rigid")
+        assert alone.tobytes() == r.tobytes()
+        assert np.all(r["texture"] == 1)
+
+
 def test_session_frames_match_the_frame_tracker(gpv_mod):
     from gpv import synth
     Ws = [synth.workload(4, scale_down=4, seed_frame=k) for k in (0, 6, 12, 18, 24)]
