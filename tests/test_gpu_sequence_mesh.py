@@ -74,3 +74,54 @@ def test_reference_update_fallback(gpv_mod, oracle, override):
         assert got["reference_updates"] == [False, True] and got["override_log"] == [2]
     else:
         assert [(p["f_index"], p["g_index"]) for p in got["pairs"]] == [(0, 1)] and got["unsolvable"]
+
+
+@pytest.mark.parametrize("sequential", [False, True])
+def test_rigid_texture_sequence_matches_oracle(gpv_mod, oracle, sequential):
+    """Sequence.solve(texture="rigid") on rigid blobs under growing shear: each
+    pair fits the rigid template of its reference frame (grain maps follow
+    the images through in-place updates and the sequential swap), against the
+    oracle's loop over its rigid solve."""
+    import sequence_oracle as SO
+    import texture_cases as TC
+    frames = [TC.shear_pair(0.0)[0]] + [TC.shear_pair(g)[1] for g in (0.02, 0.04)]
+    xs = np.linspace(60.0, 140.0, 5)
+    nodes = np.array([[x, y] for y in xs for x in xs])
+    el = []
+    for j in range(4):
+        for i in range(4):
+            a, b, c, e = j * 5 + i, j * 5 + i + 1, (j + 1) * 5 + i, (j + 1) * 5 + i + 1
+            el += [[a, b, e], [a, e, c]]
+    el = np.array(el)
+    Cs = [oracle.get_c(f, 15) for f in frames]
+    grains = [oracle.grain(f) for f in frames]
+
+    def solver_for(Cf, Cg):
+        k = next(i for i, c in enumerate(Cs) if c is Cf)
+        def s(desc, tol):
+            return oracle.solve_batch(Cf, Cg, frames[0].shape, 15, desc, max_norm=1e-5, tolerance=tol,
+                                      grain=grains[k])
+        return s
+    kw = dict(radius=15, seed_coord=(100.0, 100.0), seed_tolerance=0.5, tolerance=0.5, guide=True,
+              sequential=sequential)
+    ref = SO.solve_sequence(Cs, frames[0].shape, 15, nodes, el, solver_for, desc_dtype=oracle.DESC_DTYPE, **kw)
+    seq = gpv_mod.sequence.Sequence(frames, nodes, el, border=15)
+    got = seq.solve(15, seed_coord=(100.0, 100.0), seed_tolerance=0.5, tolerance=0.5, guide=True,
+                    sequential=sequential, texture="rigid")
+    _compare(got, ref)
+    assert got["all_converged"]
+    for pr in got["pairs"]:
+        assert np.all(pr["results"]["texture"] == 1)
+
+
+def test_rigid_texture_from_colour_pixels(gpv_mod, oracle):
+    """Grain maps of a colour-ingested reference come from its device-made
+    grey image: the same maps as from those grey pixels directly."""
+    import texture_cases as TC
+    f, _ = TC.shear_pair(0.0)
+    grey = np.clip(np.round(f), 0, 255).astype(np.uint8)
+    rgb = np.repeat(grey[:, :, None], 3, axis=2)
+    Fc = gpv_mod.Image(image_rgb=rgb, border=8, grain=True)
+    Fg = gpv_mod.Image(image_gs=gpv_mod.Image(image_rgb=rgb, border=8).image_gs, border=8, grain=True)
+    a, b = Fc.grain(maps=True), Fg.grain(maps=True)
+    assert a["built"] and np.array_equal(a["maps"], b["maps"]) and a["s2"] == b["s2"]
