@@ -595,6 +595,22 @@ int gpv_image_eval(const gpv_image *img, const double *xy, int64_t n, int32_t pr
     return GPV_SUCCESS;
 }
 
+int gpv_image_grain_sample(gpv_image *img, const double *xy, int64_t n, double *out) {
+    if (!img || (n && (!xy || !out)) || n < 0) { set_error("invalid arguments"); return GPV_ERR_INVALID; }
+    if (!img->grain) { set_error("the image keeps no grain maps"); return GPV_ERR_INVALID; }
+    if (n == 0) return GPV_SUCCESS;
+    gpv_context *ctx = img->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    if (int rc = ctx->eval_dev.ensure(sizeof(double) * 5 * n)) return rc;
+    double *dxy = static_cast<double *>(ctx->eval_dev.ptr), *dout = dxy + 2 * n;
+    GPV_CUDA_TRY(cudaMemcpyAsync(dxy, xy, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, ctx->stream));
+    if (int rc = grain_points_launch(img, dxy, n, dout, ctx->stream)) return rc;
+    GPV_CUDA_TRY(cudaMemcpyAsync(out, dout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+    GPV_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GPV_SUCCESS;
+}
+
 int gpv_mask_create(gpv_context *ctx, const uint8_t *mask, int64_t h, int64_t w, gpv_mask **out) {
     if (!ctx || !mask || !out || h < 1 || w < 1) { set_error("invalid mask arguments"); return GPV_ERR_INVALID; }
     DeviceGuard dg(ctx->device);

@@ -158,6 +158,28 @@ __global__ void grain_maps(const void *px, int dtype, int h, int w, GrainTaps t,
     }
 }
 
+// The three maps at n points (x = column, y = row): bilinear in FP64 from
+// the FP64 maps when the image keeps them, else the FP32 ones, clamped
+// (GrainMaps::sample, src/texture.rs:125-143); out: 3 values per point.
+__global__ void grain_points(const float *maps, const double *maps64, int rows, int cols, const double *xy, int64_t n,
+                             double *out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = fmin(fmax(xy[2 * i], 0.0), (double)(cols - 1));
+    const double y = fmin(fmax(xy[2 * i + 1], 0.0), (double)(rows - 1));
+    const int x0 = min((int)floor(x), max(cols - 2, 0)), y0 = min((int)floor(y), max(rows - 2, 0));
+    const int x1 = min(x0 + 1, cols - 1), y1 = min(y0 + 1, rows - 1);
+    const double tx = x - (double)x0, ty = y - (double)y0;
+    const int64_t np = (int64_t)rows * cols;
+    for (int m = 0; m < 3; m++) {
+        const int64_t a = m * np + (int64_t)y0 * cols + x0, b = m * np + (int64_t)y0 * cols + x1;
+        const int64_t c = m * np + (int64_t)y1 * cols + x0, e = m * np + (int64_t)y1 * cols + x1;
+        const double v00 = maps64 ? maps64[a] : (double)maps[a], v01 = maps64 ? maps64[b] : (double)maps[b];
+        const double v10 = maps64 ? maps64[c] : (double)maps[c], v11 = maps64 ? maps64[e] : (double)maps[e];
+        out[3 * i + m] = (1.0 - ty) * ((1.0 - tx) * v00 + tx * v01) + ty * ((1.0 - tx) * v10 + tx * v11);
+    }
+}
+
 // kernel_with(order, 1.0) (src/texture.rs:49-68), on the host (libm exp).
 GrainTaps grain_taps() {
     GrainTaps t;
@@ -174,6 +196,13 @@ GrainTaps grain_taps() {
 }
 
 }  // namespace
+
+int grain_points_launch(const gpv_image *img, const double *xy_dev, int64_t n, double *out_dev, cudaStream_t s) {
+    grain_points<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(img->grain, img->grain64, (int)img->h, (int)img->w, xy_dev,
+                                                              n, out_dev);
+    GPV_CUDA_TRY(cudaGetLastError());
+    return GPV_SUCCESS;
+}
 
 int grain_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s) {
     const int64_t h = img->h, w = img->w;

@@ -144,6 +144,8 @@ int prefilter_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t
 int image_pixels_in(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s, bool staged);
 // grain.cu: correlation length, s2, corr and the three maps of img from its pixels
 int grain_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s);
+// the maps at n device points (x, y) -> 3 values per point
+int grain_points_launch(const gpv_image *img, const double *xy_dev, int64_t n, double *out_dev, cudaStream_t s);
 // icgn.cu
 struct SolveLaunch {
     const gpv_image *f, *g;

@@ -176,6 +176,14 @@ class Image:
             r["maps"] = m
         return r
 
+    def grain_sample(self, xy) -> np.ndarray:
+        """(n, 3) fxx, fyy, fxy of the grain maps at points (x = column, y = row),
+        sampled on the device as the solves sample them."""
+        xy = np.ascontiguousarray(np.atleast_2d(xy), dtype=np.float64)
+        out = np.empty((xy.shape[0], 3))
+        check(lib().gpv_image_grain_sample(self._h, ptr(xy), xy.shape[0], ptr(out)), "gpv_image_grain_sample")
+        return out
+
     def update_rgb(self, image_rgb) -> None:
         """Ingest and prefilter new colour pixels of the same shape in place."""
         rgb = np.ascontiguousarray(image_rgb, dtype=np.uint8)
@@ -356,6 +364,7 @@ class Subset:
         self.subset_order = subset_order
         self._result = None
         self._history = None
+        self._precision = PREC_MIXED
         self.solved = False
 
     def solve(self, p_0=None, solver=None, max_norm=1e-3, max_iterations=50, tolerance=0.75, precision=PREC_MIXED,
@@ -394,6 +403,7 @@ class Subset:
             what = "FAGN Hessian singular" if method == "fagn" else "ICGN Hessian singular"
             raise RuntimeError(what if st == 3 else "W_delta singular")
         self._result = r
+        self._precision = precision
         k = int(r["iterations"])
         self._history = [(i + 1, *hist[0, i]) for i in range(k)]
         self.solved = True
@@ -422,6 +432,65 @@ class Subset:
     sigma_intensity = property(lambda s: float(s._get("sigma")))
     n_px = property(lambda s: int(s._get("n_px")))
     history = property(lambda s: s._history)
+
+    @property
+    def f_coords(self) -> np.ndarray:
+        """(n, 2) subset pixel coordinates: the circle's offsets in its scan
+        order (LocalMask::circle, src/masks.rs:69-109) about the centre, less
+        the pixels the global mask removes (mask_update, :199-263)."""
+        r = self.local_mask.size
+        y, x = np.mgrid[-r:r + 1, -r:r + 1]
+        keep = x * x + y * y <= r * r
+        off = np.column_stack([x[keep], y[keep]]).astype(np.float64)
+        if self.global_mask is not None:
+            b = self.global_mask.binary
+            X = int(self.coord[0]) + off[:, 0].astype(np.int64)
+            Y = int(self.coord[1]) + off[:, 1].astype(np.int64)
+            ok = (X >= 0) & (Y >= 0) & (X <= b.shape[1] - 2) & (Y <= b.shape[0] - 2)
+            ok[ok] = b[Y[ok], X[ok]] != 0
+            off = off[ok]
+        return off + np.array(self.coord)
+
+    def _f_eval(self):
+        prec = PREC_FP64 if self.f_img.keep_f64 else PREC_MIXED
+        return self.f_img.eval(self.f_coords, grad=True, precision=prec)
+
+    f = property(lambda s: s._f_eval()[0], doc="reference subset values (Subset::f)")
+    grad_f = property(lambda s: s._f_eval()[1], doc="reference subset gradients (n, 2)")
+
+    def residual_map(self) -> np.ndarray:
+        """Per-pixel zero-normalised residual zn(f) - zn(g) at the solved warp,
+        against the rigid-texture template when the solve fitted it
+        (Subset::residual_map, src/subset.rs:1350-1392); the images are
+        evaluated on the device."""
+        if self._result is None:
+            raise RuntimeError("invalid input: residual_map: subset has not been solved")
+        fc = self.f_coords
+        prec = self._precision if (self._precision == PREC_MIXED or
+                                   (self.f_img.keep_f64 and self.g_img.keep_f64)) else PREC_MIXED
+        f = self.f_img.eval(fc, precision=prec)
+        m = {0: 2, 1: 6, 2: 12}[self.subset_order]
+        p = np.zeros(12)
+        p[:m] = self._get("p")[:m]
+        dx, dy = fc[:, 0] - self.coord[0], fc[:, 1] - self.coord[1]
+        xw = fc[:, 0] + p[0] + p[2] * dx + p[4] * dy + 0.5 * p[6] * dx * dx + p[8] * dx * dy + 0.5 * p[10] * dy * dy
+        yw = fc[:, 1] + p[1] + p[3] * dx + p[5] * dy + 0.5 * p[7] * dx * dx + p[9] * dx * dy + 0.5 * p[11] * dy * dy
+        g = self.g_img.eval(np.column_stack([xw, yw]), precision=prec)
+        t = f
+        if self.texture == "rigid":  # grain_template (src/texture.rs:213-244), base = the subset mean
+            h = self.f_img.grain_sample(fc)
+            if m <= 7:
+                ux, vx, uy, vy = p[2], p[3], p[4], p[5]
+            else:
+                ux, vx = p[2] + p[6] * dx + p[8] * dy, p[3] + p[7] * dx + p[9] * dy
+                uy, vy = p[4] + p[8] * dx + p[10] * dy, p[5] + p[9] * dx + p[11] * dy
+            e0 = ux + 0.5 * (ux * ux + vx * vx)
+            e1 = vy + 0.5 * (uy * uy + vy * vy)
+            e2 = 0.5 * (uy + vx) + 0.5 * (ux * uy + vx * vy)
+            s2 = self.f_img.grain()["s2"]
+            t = f + (-0.5 * s2 * (e0 * h[:, 0] + e1 * h[:, 1] + 2.0 * e2 * h[:, 2]) - (e0 + e1) * (f - f.mean()))
+        tm, gm = t.mean(), g.mean()
+        return (t - tm) / np.sqrt(np.sum((t - tm) ** 2)) - (g - gm) / np.sqrt(np.sum((g - gm) ** 2))
 
     @property
     def eta_omitted(self):

@@ -109,6 +109,7 @@ SIGNATURES = {
     "gpv_image_update": (ct.c_int, [P, P, I32]),
     "gpv_image_build_grain": (ct.c_int, [P]),
     "gpv_image_grain": (ct.c_int, [P, P, P, P]),
+    "gpv_image_grain_sample": (ct.c_int, [P, P, I64, P]),
     "gpv_image_destroy": (ct.c_int, [P]),
     "gpv_image_shape": (ct.c_int, [P, P, P, P]),
     "gpv_image_coefficients_f32": (ct.c_int, [P, P]),

@@ -177,6 +177,10 @@ int gpv_image_build_grain(gpv_image *img);
  * length, s2, smoothing correction; *built = 0 when the image has no
  * measurable speckle; maps (host, 3 x h x w FP32: fxx, fyy, fxy) or NULL. */
 int gpv_image_grain(gpv_image *img, double *out3, int32_t *built, float *maps);
+/* The maps at n points (host xy, x = column, y = row): fxx, fyy, fxy per
+ * point into out (host, 3n), bilinear and clamped as the solves sample them
+ * (GrainMaps::sample, src/texture.rs:125-143).  Synchronous. */
+int gpv_image_grain_sample(gpv_image *img, const double *xy, int64_t n, double *out);
 int gpv_image_shape(const gpv_image *img, int64_t *h, int64_t *w, int32_t *border);
 /* Download coefficients C (h+2b, w+2b) row-major: FP32 always, FP64 if kept. */
 int gpv_image_coefficients_f32(const gpv_image *img, float *out);

@@ -173,3 +173,23 @@ def test_rigid_mesh_solve(gpv_mod, oracle):
     res = mesh.results
     assert np.all(res["texture"] == 1) and np.all(res["converged"] == 1)
     assert np.abs(res["p"][:, 4] - 0.05).max() < 0.02
+
+
+def test_rigid_residual_map_and_record(gpv_mod):
+    """src/texture.rs:533-552: after a rigid solve the residual map uses the
+    rigid template (well under half the deformable solve's rms) and the
+    result records the texture."""
+    f, g = TC.shear_pair(0.05)
+    F = gpv_mod.Image(image_gs=f, border=8)
+    G = gpv_mod.Image(image_gs=g, border=8)
+    rms = []
+    for tex in ("deformable", "rigid"):
+        sub = gpv_mod.Subset([100.3, 100.6], gpv_mod.Mask("local", shape="circle", size=15), F, G, 1)
+        sub.solve_icgn(max_norm=1e-5, max_iterations=100, tolerance=0.75, texture=tex)
+        assert sub.texture == tex
+        e = sub.residual_map()
+        assert e.shape == (sub.n_px,) and sub.f_coords.shape == (sub.n_px, 2)
+        rms.append(float(np.sqrt(np.mean(e * e))))
+    assert rms[1] < 0.5 * rms[0]
+    # the subset's reference values are the image's spline at its pixels
+    assert np.abs(sub.f - F.eval(sub.f_coords)).max() == 0.0
