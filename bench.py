@@ -63,6 +63,7 @@ def parse():
     ap.add_argument("--no-sequence", action="store_true", help="skip the frame-tracking leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch (graph) leg")
+    ap.add_argument("--no-rigid", action="store_true", help="skip the rigid-texture leg")
     ap.add_argument("--serving-seconds", type=float, default=10.0)
     return ap.parse_args()
 
@@ -420,6 +421,63 @@ def uneven_leg(device, steps=10):
 
 
 # ---------------------------------------------------------------------------
+def rigid_leg(W, device, steps=5):
+    """The headline batch with the rigid-texture template (src/texture.rs): the
+    reference's grain maps built on the device from its pixels, then the
+    same subsets solved with the per-iteration template, beside the
+    deformable solve on the same images; CUDA events on the library stream,
+    inputs resident."""
+    import ctypes as ct
+
+    import torch
+
+    import gpv
+    from gpv import _lib
+    ctx = gpv.Context(device)
+    F = gpv.Image(image_gs=W["f"], border=20, ctx=ctx, grain=True)
+    G = gpv.Image(image_gs=W["g"], border=20, ctx=ctx)
+    desc = gpv.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
+    n = len(desc)
+    ctx.reserve(n, int(desc["radius"].max()), 50)
+    order = np.argsort(-(3 * desc["radius"].astype(np.int64) + desc["order"]), kind="stable").astype(np.int32)
+    d_dev = torch.from_numpy(desc.view(np.uint8).copy()).cuda(device)
+    o_dev = torch.from_numpy(order).cuda(device)
+    out_dev = torch.zeros(n * _lib.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{device}")
+    L = _lib.lib()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    out = {}
+    for tex in ("deformable", "rigid"):
+        prm = gpv._params(1e-5, 50, 0.75, False, gpv.PREC_MIXED, None, None, "icgn", tex)
+        args = (ctx.handle, F.handle, G.handle, ct.c_void_p(d_dev.data_ptr()), ct.c_void_p(o_dev.data_ptr()), n,
+                ct.byref(prm), ct.c_void_p(out_dev.data_ptr()), None)
+        for _ in range(2):
+            _lib.check(L.gpv_solve_batch_device(*args), "solve")
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            _lib.check(L.gpv_solve_batch_device(*args), "solve")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res = np.frombuffer(out_dev.cpu().numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
+        out[tex] = dict(ms=ms, subsets_per_s=n / (ms * 1e-3), iterations_mean=float(res["iterations"].mean()),
+                        converged_frac=float(res["converged"].mean()), texture_frac=float(res["texture"].mean()))
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    F.update(W["f"])  # prefilter + grain statistics and maps of a 4096^2 reference
+    t1.record(stream)
+    torch.cuda.synchronize()
+    gr = F.grain()
+    return {"workload": W["name"], "subsets": n, "correlation_length_px": gr["correlation_length"],
+            "update_with_grain_ms": t0.elapsed_time(t1),
+            "update_with_grain": "host pixels of the reference: upload + prefilter + correlation length + maps", **out,
+            "timing": "CUDA events on the library stream; the rigid template's extra work is one template pass "
+                      "and its sums per iteration"}
+
+
+# ---------------------------------------------------------------------------
 def sequence_leg(ctx, n_frames=20, frame_step=10):
     """Frame-to-frame tracking (gpv_sequence_*) on the incremental-sequence
     workload: 2048^2 u8 frames under simple shear rising by 0.25% per frame,
@@ -751,6 +809,9 @@ def run_ours(args, world, rank, local):
     uneven = None
     if not args.no_uneven and args.config == 2 and args.scale_down == 1:
         uneven = uneven_leg(local)
+    rigid = None
+    if not args.no_rigid and args.config == 2 and args.scale_down == 1 and prec == gpv.PREC_MIXED:
+        rigid = rigid_leg(W, local)
     serving = None
     if not args.no_serving and args.config == 2 and args.scale_down == 1:
         serving = serving_leg(seconds=args.serving_seconds)
@@ -810,6 +871,8 @@ def run_ours(args, world, rank, local):
         line["sequence"] = seq
     if uneven is not None:
         line["uneven_batch"] = uneven
+    if rigid is not None:
+        line["rigid_texture"] = rigid
     if serving is not None:
         line["serving"] = serving
         line["p50_ms"] = serving["p50_ms"]
