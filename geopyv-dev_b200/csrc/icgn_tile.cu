@@ -531,11 +531,10 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                     ta[4 + 2 * mu] = fmaf(gyt, mv, ta[4 + 2 * mu]);
                 }
             }
+            double tv[NT_];
 #pragma unroll
-            for (int q = 0; q < NT_; q++) {
-                const double tq = warp_sum((double)ta[q]);
-                if (lane == 0) sm.redt[wid][q] = tq;
-            }
+            for (int q = 0; q < NT_; q++) tv[q] = (double)ta[q];
+            warp_sum_many<NT_>(tv, sm.redt[wid], lane);
         }
         double s1 = 0.0, s2 = 0.0, sfg = 0.0;
         float pb[M];
@@ -607,11 +606,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             v[0] = s1; v[1] = s2; v[2] = sfg;
 #pragma unroll
             for (int j = 0; j < M; j++) v[3 + j] = (double)pb[j];
-#pragma unroll
-            for (int k = 0; k < 3 + M; k++) {
-                const double t = warp_sum(v[k]);
-                if (lane == 0) sm.red[wid][k] = t;
-            }
+            warp_sum_many<3 + M>(v, sm.red[wid], lane);
         }
         __syncthreads();
         if (wid == 0) {

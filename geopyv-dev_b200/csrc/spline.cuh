@@ -120,6 +120,38 @@ __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+// Warp sums of K <= 16 values at once, a transposed butterfly: the values
+// are padded to P (4, 8 or 16); the offsets from 16 down to P add all P
+// values pairwise, then each of the offsets P/2 .. 1 halves the set a lane
+// keeps and sends the other half to its partner, so lane l ends with the
+// total of value l mod P.  P log2(32/P) + P - 1 shuffles instead of 5 K
+// (31 instead of 75 for K = 15).  Lanes l < K write their total to dst[l].
+// Every total is a fixed tree over the 32 lanes (deterministic).
+template <int K>
+__device__ __forceinline__ void warp_sum_many(const double (&in)[K], double *dst, int lane) {
+    static_assert(K >= 1 && K <= 16, "up to 16 values");
+    constexpr int P = K <= 4 ? 4 : (K <= 8 ? 8 : 16);
+    double v[P];
+#pragma unroll
+    for (int j = 0; j < P; j++) v[j] = j < K ? in[j] : 0.0;
+#pragma unroll
+    for (int off = 16; off >= P; off >>= 1) {
+#pragma unroll
+        for (int j = 0; j < P; j++) v[j] += __shfl_xor_sync(0xffffffffu, v[j], off);
+    }
+#pragma unroll
+    for (int off = P / 2; off >= 1; off >>= 1) {
+        const bool up = (lane & off) != 0;
+#pragma unroll
+        for (int j = 0; j < off; j++) {
+            const double send = up ? v[j] : v[j + off];
+            const double keep = up ? v[j + off] : v[j];
+            v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+        }
+    }
+    if (lane < K) dst[lane] = v[0];
+}
+
 __device__ __forceinline__ int warp_sum_int(int v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
