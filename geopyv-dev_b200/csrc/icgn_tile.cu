@@ -130,6 +130,20 @@ __device__ __forceinline__ bool window_covers(const TileSmem &sm, int xlo, int x
            yhi + border + 3 < sm.win_r0 + sm.win_h;
 }
 
+// Warp sums of K FP32 per-thread values (FP64 totals) into dst[0..K), in
+// transposed reductions of up to 16 values.
+template <int K, int C = 0>
+__device__ __forceinline__ void warp_sums_chunked(const float (&a)[K], double *dst, int lane) {
+    if constexpr (C < K) {
+        constexpr int N = (K - C) < 16 ? (K - C) : 16;
+        double v[N];
+#pragma unroll
+        for (int j = 0; j < N; j++) v[j] = (double)a[C + j];
+        warp_sum_many<N>(v, dst + C, lane);
+        warp_sums_chunked<K, C + N>(a, dst, lane);
+    }
+}
+
 // Sum K per-thread values over the block into sm.tot[0..K) (FP64).
 template <int NT, int K>
 __device__ __forceinline__ void block_reduce(const double (&v)[K], TileSmem &sm) {
@@ -350,12 +364,9 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             }
         }
     }
-    // warp partials of pass 1 straight into red2 (frees the accumulators)
-#pragma unroll
-    for (int q = 0; q < NVA; q++) {
-        const double t = warp_sum((double)acc[q]);
-        if (lane == 0) sm.red2[wid][q] = t;
-    }
+    // warp partials of pass 1 straight into red2 (frees the accumulators),
+    // up to 16 values per transposed reduction
+    warp_sums_chunked<NVA>(acc, sm.red2[wid], lane);
     {
         float mom[3 * NMOM];
 #pragma unroll
@@ -381,11 +392,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                         mom[p * NMOM + mom_idx(dgr - bb, bb)] = fmaf(gg[p], mono, mom[p * NMOM + mom_idx(dgr - bb, bb)]);
                 }
         }
-#pragma unroll
-        for (int q = 0; q < 3 * NMOM; q++) {
-            const double t = warp_sum((double)mom[q]);
-            if (lane == 0) sm.red2[wid][NVA + q] = t;
-        }
+        warp_sums_chunked<3 * NMOM>(mom, sm.red2[wid] + NVA, lane);
     }
     __syncthreads();
     if (wid == 0) {
