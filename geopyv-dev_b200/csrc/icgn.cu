@@ -91,6 +91,16 @@ __device__ void block_sum(double (&v)[K], BlockSmem &sm) {
     }
 }
 
+// Block sums of K values in place, 15 at a time.
+template <int K, int C = 0>
+__device__ __forceinline__ void block_sums_inplace(double (&v)[K], BlockSmem &sm) {
+    if constexpr (C < K) {
+        constexpr int N = (K - C) < 15 ? (K - C) : 15;
+        block_sum<N>(*reinterpret_cast<double(*)[N]>(&v[C]), sm);
+        block_sums_inplace<K, C + N>(v, sm);
+    }
+}
+
 __device__ double block_sum1(double x, BlockSmem &sm) {
     double v[1] = {x};
     block_sum<1>(v, sm);
@@ -660,10 +670,13 @@ __device__ void fagn_subset(const KArgs &A, int idx, const gpv_subset_desc &d, d
             }
         }
         block_sum<M + 1>(acc, sm);
+        // the moments in place, in block sums of up to 15 values (each
+        // value's sum is the same tree as one at a time, with far fewer
+        // barriers)
+        block_sums_inplace<3 * NMOM>(mom, sm);
+        if (tid == 0) {
 #pragma unroll
-        for (int q = 0; q < 3 * NMOM; q++) {
-            const double v = block_sum1(mom[q], sm);
-            if (tid == 0) sm.mom[q] = v;
+            for (int q = 0; q < 3 * NMOM; q++) sm.mom[q] = mom[q];
         }
         __syncthreads();
         if (tid < 32) assemble_hessian<ORDER>(sm.mom, sm.H, tid);
