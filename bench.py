@@ -437,32 +437,38 @@ def rigid_leg(W, device, steps=5):
     F = gpv.Image(image_gs=W["f"], border=20, ctx=ctx, grain=True)
     G = gpv.Image(image_gs=W["g"], border=20, ctx=ctx)
     desc = gpv.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
+    desc1 = desc.copy()  # the same subsets at first order
+    desc1["order"] = 1
+    desc1["p0"][:, 6:] = 0.0
     n = len(desc)
     ctx.reserve(n, int(desc["radius"].max()), 50)
     order = np.argsort(-(3 * desc["radius"].astype(np.int64) + desc["order"]), kind="stable").astype(np.int32)
-    d_dev = torch.from_numpy(desc.view(np.uint8).copy()).cuda(device)
     o_dev = torch.from_numpy(order).cuda(device)
     out_dev = torch.zeros(n * _lib.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{device}")
     L = _lib.lib()
     stream = torch.cuda.ExternalStream(ctx.stream)
     out = {}
-    for tex in ("deformable", "rigid"):
-        prm = gpv._params(1e-5, 50, 0.75, False, gpv.PREC_MIXED, None, None, "icgn", tex)
-        args = (ctx.handle, F.handle, G.handle, ct.c_void_p(d_dev.data_ptr()), ct.c_void_p(o_dev.data_ptr()), n,
-                ct.byref(prm), ct.c_void_p(out_dev.data_ptr()), None)
-        for _ in range(2):
-            _lib.check(L.gpv_solve_batch_device(*args), "solve")
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            _lib.check(L.gpv_solve_batch_device(*args), "solve")
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        res = np.frombuffer(out_dev.cpu().numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
-        out[tex] = dict(ms=ms, subsets_per_s=n / (ms * 1e-3), iterations_mean=float(res["iterations"].mean()),
-                        converged_frac=float(res["converged"].mean()), texture_frac=float(res["texture"].mean()))
+    for label, dsc in (("", desc), ("_order1", desc1)):
+        d_dev = torch.from_numpy(dsc.view(np.uint8).copy()).cuda(device)
+        for tex in ("deformable", "rigid"):
+            prm = gpv._params(1e-5, 50, 0.75, False, gpv.PREC_MIXED, None, None, "icgn", tex)
+            args = (ctx.handle, F.handle, G.handle, ct.c_void_p(d_dev.data_ptr()), ct.c_void_p(o_dev.data_ptr()), n,
+                    ct.byref(prm), ct.c_void_p(out_dev.data_ptr()), None)
+            for _ in range(2):
+                _lib.check(L.gpv_solve_batch_device(*args), "solve")
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                _lib.check(L.gpv_solve_batch_device(*args), "solve")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            res = np.frombuffer(out_dev.cpu().numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
+            out[tex + label] = dict(ms=ms, subsets_per_s=n / (ms * 1e-3),
+                                    iterations_mean=float(res["iterations"].mean()),
+                                    converged_frac=float(res["converged"].mean()),
+                                    texture_frac=float(res["texture"].mean()))
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
@@ -474,7 +480,8 @@ def rigid_leg(W, device, steps=5):
             "update_with_grain_ms": t0.elapsed_time(t1),
             "update_with_grain": "host pixels of the reference: upload + prefilter + correlation length + maps", **out,
             "timing": "CUDA events on the library stream; the rigid template's extra work is one template pass "
-                      "and its sums per iteration"}
+                      "and its sums per iteration at second order, closed-form sums from fixed grain moments "
+                      "at first order (*_order1: the same subsets solved at first order)"}
 
 
 # ---------------------------------------------------------------------------

@@ -41,7 +41,8 @@ struct TileSmem {
     double A[12], S[12];
     double p[12], pprev[12], dp[12], grad[12];
     double red[kMaxTileWarps][16];
-    double redt[kMaxTileWarps][16];  // rigid texture: the template pass's warp sums
+    double redt[kMaxTileWarps][16];  // rigid texture: the template pass's warp sums (order 2), or the
+                                     // fixed grain moments (redt[0..1]) and G's coefficients (redt[2]) (order 1)
     double red2[kMaxTileWarps][80];  // setup: one combined reduction
     double tot[16];
     double tt[16];  // rigid texture: the template pass's block sums
@@ -244,6 +245,10 @@ __device__ __forceinline__ void green_lagrange(float ux, float vx, float uy, flo
 // plus per-iteration sums of the small G (sum G, sum G^2, sum (f - f_m) G,
 // sum SDI_j G), so the FP32 rounding of the per-iteration pass scales with
 // the strain and vanishes at zero strain, as the deformable sums do.
+// Order 1 has a uniform strain, so G = c . (h0, h1, h2, f - f_m) with four
+// coefficients per iteration, and those sums follow in closed form from
+// fixed setup moments of the grain samples (sum h_k, h_k h_l, (f - f_m) h_k,
+// SDI_j h_k): no template pass, only sum h_k (g - f_m) in the sample loop.
 template <int ORDER, int NT, bool RIGID>
 __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d, float4 *S4, float *Sg, float *win,
                             TileSmem &sm, float *Sh, float *St, int64_t nmax) {
@@ -264,6 +269,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
     const int B = A.border, ch = A.h + 2 * B;
     const bool rigid_on = RIGID && A.grain_scal[4] != 0.0;  // uniform: maps built
     const float s2f = RIGID ? (float)A.grain_scal[2] : 0.f;
+    double *const gq = &sm.redt[0][0], *const gcoef = &sm.redt[2][0];  // order-1 rigid
 
     // ---- stage f's window ------------------------------------------------
     {
@@ -394,10 +400,43 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         }
         warp_sums_chunked<3 * NMOM>(mom, sm.red2[wid] + NVA, lane);
     }
+    if (RIGID && ORDER == 1 && rigid_on) {
+        // grain moments: [0,3) h_k, [3,9) h_k h_l (00 01 02 11 12 22),
+        // [9,12) (f - s) h_k, [12,30) SDI_j h_k at 12 + 3 j + k
+        float gm[30];
+#pragma unroll
+        for (int q = 0; q < 30; q++) gm[q] = 0.f;
+        for (int i = tid; i < npx_t; i += NT) {
+            const float4 rec = S4[i];
+            if (rec.x != rec.x) continue;
+            float dx, dy;
+            unpack_off(rec.w, dx, dy);
+            const float h[3] = {Sh[i], Sh[nmax + i], Sh[2 * nmax + i]};
+            const float fs = rec.x - shift;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                gm[k] += h[k];
+                gm[9 + k] = fmaf(fs, h[k], gm[9 + k]);
+            }
+            gm[3] = fmaf(h[0], h[0], gm[3]); gm[4] = fmaf(h[0], h[1], gm[4]); gm[5] = fmaf(h[0], h[2], gm[5]);
+            gm[6] = fmaf(h[1], h[1], gm[6]); gm[7] = fmaf(h[1], h[2], gm[7]); gm[8] = fmaf(h[2], h[2], gm[8]);
+#pragma unroll
+            for (int mu = 0; mu < NMU; mu++) {
+                const float mv = mu_val<float>(mu, dx, dy), sx = rec.y * mv, sy = rec.z * mv;
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    gm[12 + 3 * (2 * mu) + k] = fmaf(sx, h[k], gm[12 + 3 * (2 * mu) + k]);
+                    gm[12 + 3 * (2 * mu + 1) + k] = fmaf(sy, h[k], gm[12 + 3 * (2 * mu + 1) + k]);
+                }
+            }
+        }
+        warp_sums_chunked<30>(gm, sm.red2[wid] + NV, lane);
+    }
     __syncthreads();
     if (wid == 0) {
-        // sum the warp partials: aug[0..NV)
-        for (int q = lane; q < NV; q += 32) {
+        // sum the warp partials: aug[0..NV) (+ 30 grain moments, order-1 rigid)
+        const int nv = NV + ((RIGID && ORDER == 1 && rigid_on) ? 30 : 0);
+        for (int q = lane; q < nv; q += 32) {
             double t = 0.0;
 #pragma unroll
             for (int w = 0; w < NT / 32; w++) t += sm.red2[w][q];
@@ -418,6 +457,8 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             }
             if (lane < 3 * NMOM) sm.mom[lane] = sm.aug[NVA + lane];
             if (lane + 32 < 3 * NMOM) sm.mom[lane + 32] = sm.aug[NVA + lane + 32];
+            if (RIGID && ORDER == 1 && rigid_on && lane < 30)  // (f - s) h_k -> (f - f_m) h_k
+                gq[lane] = (lane >= 9 && lane < 12) ? sm.aug[NV + lane] - ms * sm.aug[NV + lane - 9] : sm.aug[NV + lane];
             __syncwarp();
             assemble_hessian<ORDER>(sm.mom, sm.H, lane);
             if (!spd_inverse_warp<M>(sm.H, sm.aug + 96, sm.Hinv, lane)) st = GPV_SINGULAR_H;
@@ -502,7 +543,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         }
         // window-relative base: sample (ix, iy) reads win[(iy + B-2 - r0) * ww + (ix + B-2 - c0)]
         const int offx = B - 2 - gc0, offy = B - 2 - gr0;
-        if (RIGID && rigid_on) {
+        if (RIGID && rigid_on && ORDER == 2) {
             // template pass: G per pixel, sums of G, G^2, (f - f_m) G and
             // SDI_j G (their warp sums meet the iteration's reduction)
             constexpr int NT_ = 3 + M;
@@ -548,8 +589,10 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
 #pragma unroll
         for (int j = 0; j < M; j++) pb[j] = 0.f;
         float4 rec_next = tid < npx_t ? S4[tid] : make_float4(0.f, 0.f, 0.f, 0.f);
+        constexpr bool kClosed = RIGID && ORDER == 1;  // order-1 rigid: sums of h_k (g - f_m)
+        double sh0 = 0.0, sh1 = 0.0, sh2 = 0.0;
         for (int base = 0; base < npx_t; base += NT * kChunk) {
-            float p1 = 0.f, p2 = 0.f, pfg = 0.f;
+            float p1 = 0.f, p2 = 0.f, pfg = 0.f, ph0 = 0.f, ph1 = 0.f, ph2 = 0.f;
 #pragma unroll 2
             for (int c = 0; c < kChunk; c++) {
                 const int i = base + c * NT + tid;
@@ -585,7 +628,12 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                         const float gc = g - fmf;
                         p1 += gc;
                         p2 = fmaf(gc, gc, p2);
-                        pfg = fmaf((RIGID && rigid_on ? (fv - fmf) + St[i] : fv - fmf), gc, pfg);
+                        pfg = fmaf((RIGID && ORDER == 2 && rigid_on ? (fv - fmf) + St[i] : fv - fmf), gc, pfg);
+                        if (kClosed && rigid_on) {
+                            ph0 = fmaf(Sh[i], gc, ph0);
+                            ph1 = fmaf(Sh[nmax + i], gc, ph1);
+                            ph2 = fmaf(Sh[2 * nmax + i], gc, ph2);
+                        }
                         const float gxg = rec.y * gc, gyg = rec.z * gc;
                         pb[0] += gxg;
                         pb[1] += gyg;
@@ -605,25 +653,36 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             s1 += (double)p1;
             s2 += (double)p2;
             sfg += (double)pfg;
+            if (kClosed) {
+                sh0 += (double)ph0;
+                sh1 += (double)ph1;
+                sh2 += (double)ph2;
+            }
         }
         // block sums: warp partials to shared memory, one barrier, then warp 0
         // adds them up and updates the warp; a second barrier publishes p
+        constexpr int KR = 3 + M + (kClosed ? 3 : 0);
         {
-            double v[3 + M];
+            double v[KR];
             v[0] = s1; v[1] = s2; v[2] = sfg;
 #pragma unroll
             for (int j = 0; j < M; j++) v[3 + j] = (double)pb[j];
-            warp_sum_many<3 + M>(v, sm.red[wid], lane);
+            if (kClosed) {
+                v[(3 + M) % KR] = sh0;
+                v[(4 + M) % KR] = sh1;
+                v[(5 + M) % KR] = sh2;
+            }
+            warp_sum_many<KR>(v, sm.red[wid], lane);
         }
         __syncthreads();
         if (wid == 0) {
-            if (lane < 3 + M) {
+            if (lane < KR) {
                 double t = 0.0;
 #pragma unroll
                 for (int w = 0; w < NT / 32; w++) t += sm.red[w][lane];
                 sm.tot[lane] = t;
             }
-            if (RIGID && rigid_on && lane < 3 + M) {
+            if (RIGID && ORDER == 2 && rigid_on && lane < 3 + M) {
                 double t = 0.0;
 #pragma unroll
                 for (int w = 0; w < NT / 32; w++) t += sm.redt[w][lane];
@@ -638,23 +697,58 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             const double dg2 = sm.tot[1] - sm.tot[0] * gmt;
             dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
             double sab, dref = df, tmf = 0.0;
+            // the template's sums sum G, G^2, (f - f_m) G, SDI_j G (tg[0..3+M))
+            // and sum G (g - f_m) (tgc): the template pass's (order 2), or
+            // in closed form from the fixed grain moments (order 1)
+            double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0, tg0 = 0.0, tg1 = 0.0, tg2 = 0.0, tgc = 0.0;
+            if (kClosed && rigid_on) {
+                double e0, e1, e2;
+                const double ux = sm.p[2 % M], vx = sm.p[3 % M], uy = sm.p[4 % M], vy = sm.p[5 % M];
+                e0 = ux + 0.5 * (ux * ux + vx * vx);
+                e1 = vy + 0.5 * (uy * uy + vy * vy);
+                e2 = 0.5 * (uy + vx) + 0.5 * (ux * uy + vx * vy);
+                const double s2d = A.grain_scal[2];
+                c0 = -0.5 * s2d * e0; c1 = -0.5 * s2d * e1; c2 = -s2d * e2; c3 = -(e0 + e1);
+                const double *q = gq;
+                tg0 = c0 * q[0] + c1 * q[1] + c2 * q[2];
+                const double cfh = c0 * q[9] + c1 * q[10] + c2 * q[11];
+                tg1 = c0 * c0 * q[3] + c1 * c1 * q[6] + c2 * c2 * q[8] +
+                      2.0 * (c0 * c1 * q[4] + c0 * c2 * q[5] + c1 * c2 * q[7]) + 2.0 * c3 * cfh + c3 * c3 * saa;
+                tg2 = cfh + c3 * saa;
+                tgc = c0 * sm.tot[(3 + M) % KR] + c1 * sm.tot[(4 + M) % KR] + c2 * sm.tot[(5 + M) % KR] +
+                      c3 * sm.tot[2];
+            }
             if (RIGID && rigid_on) {  // the template t = f + G: t_m = f_m + tmf, spread dref
-                tmf = sm.tt[0] / dn;
-                const double dt2 = saa + 2.0 * sm.tt[2] + sm.tt[1] - sm.tt[0] * tmf;
+                if (ORDER == 2) {
+                    tg0 = sm.tt[0];
+                    tg1 = sm.tt[1];
+                    tg2 = sm.tt[2];
+                }
+                tmf = tg0 / dn;
+                const double dt2 = saa + 2.0 * tg2 + tg1 - tg0 * tmf;
                 dref = sqrt(dt2 > 0.0 ? dt2 : 0.0);
-                sab = sm.tot[2] - tmf * sm.tot[0];
+                sab = sm.tot[2] + tgc - tmf * sm.tot[0];
             } else {
                 sab = sm.tot[2] - gmt * sa;
             }
             znssd = 2.0 - 2.0 * sab / (dref * dg);
             const double ratio = dref / dg;
             if (lane < M) {
-                const double aj = (RIGID && rigid_on) ? sm.A[lane] + sm.tt[3 + lane] - tmf * sm.S[lane] : sm.A[lane];
+                double sg = 0.0;  // sum SDI_j G
+                if (RIGID && rigid_on)
+                    sg = ORDER == 2 ? sm.tt[3 + lane]
+                                    : c0 * gq[12 + 3 * lane] + c1 * gq[13 + 3 * lane] + c2 * gq[14 + 3 * lane] +
+                                          c3 * sm.A[lane];
+                const double aj = (RIGID && rigid_on) ? sm.A[lane] + sg - tmf * sm.S[lane] : sm.A[lane];
                 sm.grad[lane] = aj - ratio * (sm.tot[3 + lane] - gmt * sm.S[lane]);
             }
             if (lane == 0) {
                 sm.misc[8] = tmf;
                 sm.misc[9] = dref;
+                gcoef[0] = c0;  // the order-1 template's coefficients (eta)
+                gcoef[1] = c1;
+                gcoef[2] = c2;
+                gcoef[3] = c3;
             }
             __syncwarp();
             if (lane < M) {
@@ -751,7 +845,12 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             if (rec.x != rec.x) return false;
             float dxf, dyf;
             unpack_off(rec.w, dxf, dyf);
-            f = (RIGID && rigid_on) ? (double)rec.x + (double)St[i] : rec.x;  // the template fitted at the last iteration
+            f = rec.x;
+            if (RIGID && rigid_on) {  // the template fitted at the last iteration
+                if (ORDER == 2) f += (double)St[i];
+                else f += gcoef[0] * Sh[i] + gcoef[1] * Sh[nmax + i] + gcoef[2] * Sh[2 * nmax + i] +
+                          gcoef[3] * ((double)rec.x - fm);
+            }
             gx = rec.y; gy = rec.z; g = Sg[i]; dx = dxf; dy = dyf;
             return true;
         };
