@@ -24,6 +24,7 @@
 #include <mutex>
 #include <set>
 #include <utility>
+#include <type_traits>
 
 #include "icgn_common.cuh"
 
@@ -175,7 +176,7 @@ __device__ __forceinline__ double block_sum1(double v, TileSmem &sm) {
 // subset centred at (cx, cy), conservatively.
 template <int ORDER>
 __device__ void warp_extent(const double *p, double cx, double cy, int r, int w, int h, int &xlo, int &xhi, int &ylo,
-                            int &yhi) {
+                            int &yhi, bool *inside = nullptr) {
     double ex = r, ey = r;
     if (ORDER >= 1) {
         ex = r * (fabs(1.0 + p[2]) + fabs(p[4]));
@@ -190,8 +191,12 @@ __device__ void warp_extent(const double *p, double cx, double cy, int r, int w,
     double a = floor(X0 - ex) - 1.0, b = floor(X0 + ex) + 1.0, c = floor(Y0 - ey) - 1.0, d = floor(Y0 + ey) + 1.0;
     if (!(isfinite(a) && isfinite(b) && isfinite(c) && isfinite(d))) {
         xlo = 0; xhi = w - 1; ylo = 0; yhi = h - 1;  // plans a window that cannot fit: global path
+        if (inside) *inside = false;
         return;
     }
+    // inside: the extent (with its one-pixel margin) lies in the image, so no
+    // sample position meets the edge clamp
+    if (inside) *inside = a >= 0.0 && b <= (double)(w - 1) && c >= 0.0 && d <= (double)(h - 1);
     xlo = (int)fmax(0.0, fmin(a, (double)(w - 1)));
     xhi = (int)fmax(0.0, fmin(b, (double)(w - 1)));
     ylo = (int)fmax(0.0, fmin(c, (double)(h - 1)));
@@ -514,9 +519,10 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
     double c_zncc = 0.0, c_znssd = 4.0, last_norm = 0.0, gm_last = 0.0, dg_last = 0.0;
     for (int it = 1; it <= A.max_iter; it++) {
         // (re)stage g's window when the warped subset has left it
+        bool inside;
         {
             int xlo, xhi, ylo, yhi;
-            warp_extent<ORDER>(sm.p, cx, cy, r, A.w, A.h, xlo, xhi, ylo, yhi);
+            warp_extent<ORDER>(sm.p, cx, cy, r, A.w, A.h, xlo, xhi, ylo, yhi, &inside);
             if (!window_covers(sm, xlo, xhi, ylo, yhi, B)) {
                 int r0, c0, wh, ww;
                 const bool ok = plan_window(xlo, xhi, ylo, yhi, B, T.win_cap, T.layout, r0, c0, wh, ww);
@@ -591,74 +597,92 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         float4 rec_next = tid < npx_t ? S4[tid] : make_float4(0.f, 0.f, 0.f, 0.f);
         constexpr bool kClosed = RIGID && ORDER == 1;  // order-1 rigid: sums of h_k (g - f_m)
         double sh0 = 0.0, sh1 = 0.0, sh2 = 0.0;
-        for (int base = 0; base < npx_t; base += NT * kChunk) {
-            float p1 = 0.f, p2 = 0.f, pfg = 0.f, ph0 = 0.f, ph1 = 0.f, ph2 = 0.f;
-#pragma unroll 2
-            for (int c = 0; c < kChunk; c++) {
-                const int i = base + c * NT + tid;
-                if (i < npx_t) {
-                    const float4 rec = rec_next;  // loaded one sample ahead
-                    if (i + NT < npx_t) rec_next = S4[i + NT];
-                    const float fv = rec.x;
-                    if (fv == fv) {
-                        float dx, dy;
-                        unpack_off(rec.w, dx, dy);
-                        float lx = fmaf(uy, dy, fmaf(ux, dx, ox)) + dx;
-                        float ly = fmaf(vy, dy, fmaf(vx, dx, oy)) + dy;
-                        float dxx = 0.f, dxy = 0.f, dyy = 0.f;
-                        if (ORDER == 2) {
-                            dxx = dx * dx; dxy = dx * dy; dyy = dy * dy;
-                            lx += fmaf(uxx, dxx, fmaf(uxy, dxy, uyy * dyy));
-                            ly += fmaf(vxx, dxx, fmaf(vxy, dxy, vyy * dyy));
-                        }
-                        int ix, iy;
-                        float tx, ty;
-                        split_clamped(wbx, lx, A.w, ix, tx);
-                        split_clamped(wby, ly, A.h, iy, ty);
-                        float a[6], b[6];
-                        basis(ty, a);
-                        basis(tx, b);
-                        float g;
-                        if (staged) {
-                            const int wx = min(max(ix + offx, 0), gww - 6), wy = min(max(iy + offy, 0), gwh - 6);
-                            g = contract<float>(win + wy * gww + wx, gww, a, b);
-                        } else {
-                            g = contract<float>(A.g32 + (int64_t)(iy + B - 2) * A.pitch32 + (ix + B - 2), A.pitch32, a, b);
-                        }
-                        const float gc = g - fmf;
-                        p1 += gc;
-                        p2 = fmaf(gc, gc, p2);
-                        pfg = fmaf((RIGID && ORDER == 2 && rigid_on ? (fv - fmf) + St[i] : fv - fmf), gc, pfg);
-                        if (kClosed && rigid_on) {
-                            ph0 = fmaf(Sh[i], gc, ph0);
-                            ph1 = fmaf(Sh[nmax + i], gc, ph1);
-                            ph2 = fmaf(Sh[2 * nmax + i], gc, ph2);
-                        }
-                        const float gxg = rec.y * gc, gyg = rec.z * gc;
-                        pb[0] += gxg;
-                        pb[1] += gyg;
-                        if (ORDER >= 1) {
-                            pb[2 % M] = fmaf(gxg, dx, pb[2 % M]); pb[3 % M] = fmaf(gyg, dx, pb[3 % M]);
-                            pb[4 % M] = fmaf(gxg, dy, pb[4 % M]); pb[5 % M] = fmaf(gyg, dy, pb[5 % M]);
-                        }
-                        if (ORDER == 2) {
-                            const float hxx = 0.5f * dxx, hyy = 0.5f * dyy;
-                            pb[6 % M] = fmaf(gxg, hxx, pb[6 % M]); pb[7 % M] = fmaf(gyg, hxx, pb[7 % M]);
-                            pb[8 % M] = fmaf(gxg, dxy, pb[8 % M]); pb[9 % M] = fmaf(gyg, dxy, pb[9 % M]);
-                            pb[10 % M] = fmaf(gxg, hyy, pb[10 % M]); pb[11 % M] = fmaf(gyg, hyy, pb[11 % M]);
+        // the sample loop, specialised for subsets whose warped extent lies
+        // inside the image and the staged window (no clamps per sample)
+        const bool fast = staged && inside;
+        const int wx0 = wbx + offx, wy0 = wby + offy;
+        auto sweep = [&](auto fast_tag) {
+            constexpr bool FAST = decltype(fast_tag)::value;
+            for (int base = 0; base < npx_t; base += NT * kChunk) {
+                float p1 = 0.f, p2 = 0.f, pfg = 0.f, ph0 = 0.f, ph1 = 0.f, ph2 = 0.f;
+    #pragma unroll 2
+                for (int c = 0; c < kChunk; c++) {
+                    const int i = base + c * NT + tid;
+                    if (i < npx_t) {
+                        const float4 rec = rec_next;  // loaded one sample ahead
+                        if (i + NT < npx_t) rec_next = S4[i + NT];
+                        const float fv = rec.x;
+                        if (fv == fv) {
+                            float dx, dy;
+                            unpack_off(rec.w, dx, dy);
+                            float lx = fmaf(uy, dy, fmaf(ux, dx, ox)) + dx;
+                            float ly = fmaf(vy, dy, fmaf(vx, dx, oy)) + dy;
+                            float dxx = 0.f, dxy = 0.f, dyy = 0.f;
+                            if (ORDER == 2) {
+                                dxx = dx * dx; dxy = dx * dy; dyy = dy * dy;
+                                lx += fmaf(uxx, dxx, fmaf(uxy, dxy, uyy * dyy));
+                                ly += fmaf(vxx, dxx, fmaf(vxy, dxy, vyy * dyy));
+                            }
+                            float g;
+                            if (FAST) {  // no edge clamp can apply and the window covers every tap
+                                const float flx = floorf(lx), fly = floorf(ly);
+                                float a[6], b[6];
+                                basis(ly - fly, a);
+                                basis(lx - flx, b);
+                                g = contract_rows2(win + ((int)fly + wy0) * gww + ((int)flx + wx0), gww, a, b);
+                            } else {
+                                int ix, iy;
+                                float tx, ty;
+                                split_clamped(wbx, lx, A.w, ix, tx);
+                                split_clamped(wby, ly, A.h, iy, ty);
+                                float a[6], b[6];
+                                basis(ty, a);
+                                basis(tx, b);
+                                if (staged) {
+                                    const int wx = min(max(ix + offx, 0), gww - 6), wy = min(max(iy + offy, 0), gwh - 6);
+                                    g = contract<float>(win + wy * gww + wx, gww, a, b);
+                                } else {
+                                    g = contract<float>(A.g32 + (int64_t)(iy + B - 2) * A.pitch32 + (ix + B - 2), A.pitch32,
+                                                        a, b);
+                                }
+                            }
+                            const float gc = g - fmf;
+                            p1 += gc;
+                            p2 = fmaf(gc, gc, p2);
+                            pfg = fmaf((RIGID && ORDER == 2 && rigid_on ? (fv - fmf) + St[i] : fv - fmf), gc, pfg);
+                            if (kClosed && rigid_on) {
+                                ph0 = fmaf(Sh[i], gc, ph0);
+                                ph1 = fmaf(Sh[nmax + i], gc, ph1);
+                                ph2 = fmaf(Sh[2 * nmax + i], gc, ph2);
+                            }
+                            const float gxg = rec.y * gc, gyg = rec.z * gc;
+                            pb[0] += gxg;
+                            pb[1] += gyg;
+                            if (ORDER >= 1) {
+                                pb[2 % M] = fmaf(gxg, dx, pb[2 % M]); pb[3 % M] = fmaf(gyg, dx, pb[3 % M]);
+                                pb[4 % M] = fmaf(gxg, dy, pb[4 % M]); pb[5 % M] = fmaf(gyg, dy, pb[5 % M]);
+                            }
+                            if (ORDER == 2) {
+                                const float hxx = 0.5f * dxx, hyy = 0.5f * dyy;
+                                pb[6 % M] = fmaf(gxg, hxx, pb[6 % M]); pb[7 % M] = fmaf(gyg, hxx, pb[7 % M]);
+                                pb[8 % M] = fmaf(gxg, dxy, pb[8 % M]); pb[9 % M] = fmaf(gyg, dxy, pb[9 % M]);
+                                pb[10 % M] = fmaf(gxg, hyy, pb[10 % M]); pb[11 % M] = fmaf(gyg, hyy, pb[11 % M]);
+                            }
                         }
                     }
                 }
+                s1 += (double)p1;
+                s2 += (double)p2;
+                sfg += (double)pfg;
+                if (kClosed) {
+                    sh0 += (double)ph0;
+                    sh1 += (double)ph1;
+                    sh2 += (double)ph2;
+                }
             }
-            s1 += (double)p1;
-            s2 += (double)p2;
-            sfg += (double)pfg;
-            if (kClosed) {
-                sh0 += (double)ph0;
-                sh1 += (double)ph1;
-                sh2 += (double)ph2;
-            }
-        }
+        };
+        if (fast) sweep(std::true_type{});
+        else sweep(std::false_type{});
         // block sums: warp partials to shared memory, one barrier, then warp 0
         // adds them up and updates the warp; a second barrier publishes p
         constexpr int KR = 3 + M + (kClosed ? 3 : 0);

@@ -90,6 +90,32 @@ __device__ __forceinline__ T contract(const C *__restrict__ p, int64_t pitch, co
     return val;
 }
 
+// contract() for an FP32 block with rows taken in pairs: the two rows'
+// partial sums share one paired FMA per tap (sm_100 FFMA2); each row sum and
+// the final combine keep contract()'s operation order and rounding.
+__device__ __forceinline__ float contract_rows2(const float *__restrict__ p, int pitch, const float a[6],
+                                                const float b[6]) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    float2 s[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const float *r0 = p + 2 * q * pitch, *r1 = r0 + pitch;
+        s[q] = __fmul2_rn(make_float2(r0[0], r1[0]), make_float2(b[0], b[0]));
+#pragma unroll
+        for (int k = 1; k < 6; k++) s[q] = __ffma2_rn(make_float2(r0[k], r1[k]), make_float2(b[k], b[k]), s[q]);
+    }
+    float val = 0.f;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        val = fmaf(a[2 * q], s[q].x, val);
+        val = fmaf(a[2 * q + 1], s[q].y, val);
+    }
+    return val;
+#else
+    return contract<float>(p, pitch, a, b);
+#endif
+}
+
 // Value and gradient (Image::eval_grad, src/image.rs:115-124, :155-178).
 template <typename T, typename C>
 __device__ __forceinline__ T contract_grad(const C *__restrict__ p, int64_t pitch, const T a[6], const T da[6],
