@@ -724,18 +724,25 @@ int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, co
     // sizes of the tiled launch come from the histogram.
     constexpr int kMaxR = 4000;
     constexpr int nk = 3 * (kMaxR + 1);
+    static_assert(nk <= 65536, "work-order keys are 16-bit");
     std::vector<int64_t> start(nk + 1, 0);
     auto key = [](const gpv_subset_desc &d) -> int {
         const int r = d.radius, o = d.order;
         if (r < 1 || r > kMaxR || o < 0 || o > 2) return 0;
         return nk - 1 - (3 * r + o);
     };
+    // the descriptors are read once: keys kept compact for the scatter
+    ctx->h_keys.resize((size_t)n);
+    uint16_t *keys = ctx->h_keys.data();
     int max_r = 1;
     for (int64_t i = 0; i < n; i++) {
         const gpv_subset_desc &d = desc[i];
-        start[key(d) + 1]++;
+        const int k = key(d);
+        keys[i] = (uint16_t)k;
+        start[k + 1]++;
         if (d.radius > max_r && d.radius <= kMaxR) max_r = d.radius;
     }
+    const bool one_key = start[keys[0] + 1] == n;  // every subset in one bucket: the order is 0..n-1
     if (int rc = ensure_tables(ctx, max_r)) return rc;
     uint32_t seg_mask = 0;
     for (int q = 0; q < kTileSegs; q++) ctx->seg_count[q] = 0;
@@ -747,8 +754,12 @@ int gpv_solve_batch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, co
             ctx->seg_count[q] += c;
             seg_mask |= 1u << q;
         }
-    for (int k = 0; k < nk; k++) start[k + 1] += start[k];
-    for (int64_t i = 0; i < n; i++) order[start[key(desc[i])]++] = (int32_t)i;
+    if (one_key) {
+        for (int64_t i = 0; i < n; i++) order[i] = (int32_t)i;
+    } else {
+        for (int k = 0; k < nk; k++) start[k + 1] += start[k];
+        for (int64_t i = 0; i < n; i++) order[start[keys[i]]++] = (int32_t)i;
+    }
     GPV_CUDA_TRY(cudaMemcpyAsync(ctx->order_dev.ptr, order, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
     SolveLaunch L;
     L.f = f;

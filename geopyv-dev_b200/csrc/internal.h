@@ -78,6 +78,7 @@ struct gpv_context {
     gpv::DevBuf tab_off;  // int32 [table_radius + 1]
     gpv::DevBuf tab_n;    // int32 [table_radius + 1]
     std::vector<int32_t> h_tab_off, h_tab_n, h_slot_n;
+    std::vector<uint16_t> h_keys;  // work-order keys of a host batch (one pass over its descriptors)
     // solve workspace
     gpv::DevBuf scratch;   // per-warp / per-block pixel arrays
     gpv::DevBuf queue;     // work-queue counters
