@@ -627,8 +627,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                             if (FAST) {  // no edge clamp can apply and the window covers every tap
                                 const float flx = floorf(lx), fly = floorf(ly);
                                 float a[6], b[6];
-                                basis(ly - fly, a);
-                                basis(lx - flx, b);
+                                basis_pair(ly - fly, lx - flx, a, b);
                                 g = contract_rows2(win + ((int)fly + wy0) * gww + ((int)flx + wx0), gww, a, b);
                             } else {
                                 int ix, iy;

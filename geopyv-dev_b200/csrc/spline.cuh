@@ -35,6 +35,33 @@ __device__ __forceinline__ void basis(T t, T w[6]) {
     w[3] = e2 - o2;
 }
 
+// basis() for two fractions at once (a from ty in .x, b from tx in .y): the
+// same operations per lane as basis(), issued as sm_100 paired FP32 ops.
+__device__ __forceinline__ void basis_pair(float ty, float tx, float a[6], float b[6]) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    const float2 u = __fadd2_rn(make_float2(ty, tx), make_float2(-0.5f, -0.5f));
+    const float2 v = __fmul2_rn(u, u);
+    const float2 nu = make_float2(-u.x, -u.y);
+    auto poly = [&](float p2, float p1, float p0) {
+        return __ffma2_rn(__ffma2_rn(v, make_float2(p2, p2), make_float2(p1, p1)), v, make_float2(p0, p0));
+    };
+    const float2 e0 = poly(1.0f / 48.0f, 1.0f / 96.0f, 1.0f / 3840.0f);
+    const float2 e1 = poly(-1.0f / 16.0f, 7.0f / 32.0f, 79.0f / 1280.0f);
+    const float2 e2 = poly(1.0f / 24.0f, -11.0f / 48.0f, 841.0f / 1920.0f);
+    const float2 o0 = __fmul2_rn(nu, poly(1.0f / 120.0f, 1.0f / 48.0f, 1.0f / 384.0f));
+    const float2 o1 = __fmul2_rn(nu, poly(-1.0f / 24.0f, 1.0f / 16.0f, 25.0f / 128.0f));
+    const float2 o2 = __fmul2_rn(nu, poly(1.0f / 12.0f, -7.0f / 24.0f, 77.0f / 192.0f));
+    const float2 w0 = __fadd2_rn(e0, o0), w5 = __fadd2_rn(e0, make_float2(-o0.x, -o0.y));
+    const float2 w1 = __fadd2_rn(e1, o1), w4 = __fadd2_rn(e1, make_float2(-o1.x, -o1.y));
+    const float2 w2 = __fadd2_rn(e2, o2), w3 = __fadd2_rn(e2, make_float2(-o2.x, -o2.y));
+    a[0] = w0.x; a[1] = w1.x; a[2] = w2.x; a[3] = w3.x; a[4] = w4.x; a[5] = w5.x;
+    b[0] = w0.y; b[1] = w1.y; b[2] = w2.y; b[3] = w3.y; b[4] = w4.y; b[5] = w5.y;
+#else
+    basis(ty, a);
+    basis(tx, b);
+#endif
+}
+
 // d/dt of the weights (Image::rows uses the derivative at the fractional
 // position itself, src/image.rs:210-230).
 template <typename T>
