@@ -324,6 +324,12 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         float a0[6], da0[6], b0[6], db0[6];
         basis(fy, a0); dbasis(fy, da0);
         basis(fx, b0); dbasis(fx, db0);
+        float2 bb0[6], dbb0[6];  // the column weights as duplicated pairs (paired taps)
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            bb0[k] = make_float2(b0[k], b0[k]);
+            dbb0[k] = make_float2(db0[k], db0[k]);
+        }
         for (int i = tid; i < npx_t; i += NT) {
             const short2 o = po[i];
             if (o.x == -32768 || !mask_ok(A, cxi, cyi, o.x, o.y)) {
@@ -333,7 +339,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             float gx, gy, f;
             if (interior) {
                 const int wx = bx + o.x + B - 2 - fc0, wy = by + o.y + B - 2 - fr0;
-                f = contract_grad<float>(win + wy * fww + wx, fww, a0, da0, b0, db0, gx, gy);
+                f = contract_grad_rows2(win + wy * fww + wx, fww, a0, da0, bb0, dbb0, gx, gy);
             } else {
                 int ix, iy;
                 float tx, ty;

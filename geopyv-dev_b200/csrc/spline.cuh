@@ -167,6 +167,44 @@ __device__ __forceinline__ T contract_grad(const C *__restrict__ p, int64_t pitc
     return val;
 }
 
+// contract_grad() for an FP32 block with rows taken in pairs: each pair's
+// value and x-derivative row sums advance by one paired FMA per tap (sm_100
+// FFMA2) against the column weights given as duplicated pairs
+// bb[k] = (b_k, b_k), dbb[k] = (db_k, db_k).  The row sums and the combine
+// keep contract_grad()'s operation order.
+__device__ __forceinline__ float contract_grad_rows2(const float *__restrict__ p, int pitch, const float a[6],
+                                                     const float da[6], const float2 bb[6], const float2 dbb[6],
+                                                     float &gx, float &gy) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    float val = 0.f, vx = 0.f, vy = 0.f;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const float *r0 = p + 2 * q * pitch, *r1 = r0 + pitch;
+        float2 c = make_float2(r0[0], r1[0]);
+        float2 s = __fmul2_rn(c, bb[0]), d = __fmul2_rn(c, dbb[0]);
+#pragma unroll
+        for (int k = 1; k < 6; k++) {
+            c = make_float2(r0[k], r1[k]);
+            s = __ffma2_rn(c, bb[k], s);
+            d = __ffma2_rn(c, dbb[k], d);
+        }
+        val = fmaf(a[2 * q], s.x, val);
+        vx = fmaf(a[2 * q], d.x, vx);
+        vy = fmaf(da[2 * q], s.x, vy);
+        val = fmaf(a[2 * q + 1], s.y, val);
+        vx = fmaf(a[2 * q + 1], d.y, vx);
+        vy = fmaf(da[2 * q + 1], s.y, vy);
+    }
+    gx = vx;
+    gy = vy;
+    return val;
+#else
+    float b[6], db[6];
+    for (int k = 0; k < 6; k++) { b[k] = bb[k].x; db[k] = dbb[k].x; }
+    return contract_grad<float>(p, pitch, a, da, b, db, gx, gy);
+#endif
+}
+
 // ---- warp reductions --------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
