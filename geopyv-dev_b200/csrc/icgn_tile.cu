@@ -609,6 +609,14 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         const int wx0 = wbx + offx, wy0 = wby + offy;
         auto sweep = [&](auto fast_tag) {
             constexpr bool FAST = decltype(fast_tag)::value;
+            // second order without clamps: the warp and the gradient sums as
+            // (x, y) pairs of paired FP32 ops (the same operations per lane)
+            constexpr bool kPair = FAST && ORDER == 2;
+            const float2 U1 = make_float2(ux, vx), U2 = make_float2(uy, vy), O2 = make_float2(ox, oy);
+            const float2 Q1 = make_float2(uxx, vxx), Q2 = make_float2(uxy, vxy), Q3 = make_float2(uyy, vyy);
+            float2 pbp[6];
+#pragma unroll
+            for (int j = 0; j < 6; j++) pbp[j] = make_float2(0.f, 0.f);
             for (int base = 0; base < npx_t; base += NT * kChunk) {
                 float p1 = 0.f, p2 = 0.f, pfg = 0.f, ph0 = 0.f, ph1 = 0.f, ph2 = 0.f;
     #pragma unroll 2
@@ -621,13 +629,27 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                         if (fv == fv) {
                             float dx, dy;
                             unpack_off(rec.w, dx, dy);
-                            float lx = fmaf(uy, dy, fmaf(ux, dx, ox)) + dx;
-                            float ly = fmaf(vy, dy, fmaf(vx, dx, oy)) + dy;
+                            float lx, ly;
                             float dxx = 0.f, dxy = 0.f, dyy = 0.f;
-                            if (ORDER == 2) {
-                                dxx = dx * dx; dxy = dx * dy; dyy = dy * dy;
-                                lx += fmaf(uxx, dxx, fmaf(uxy, dxy, uyy * dyy));
-                                ly += fmaf(vxx, dxx, fmaf(vxy, dxy, vyy * dyy));
+                            float2 D2, E2, DXX, DXY, DYY;
+                            if (kPair) {
+                                D2 = make_float2(dx, dx);
+                                E2 = make_float2(dy, dy);
+                                float2 L = __fadd2_rn(__ffma2_rn(U2, E2, __ffma2_rn(U1, D2, O2)), make_float2(dx, dy));
+                                DXX = __fmul2_rn(D2, D2);
+                                DXY = __fmul2_rn(D2, E2);
+                                DYY = __fmul2_rn(E2, E2);
+                                L = __fadd2_rn(L, __ffma2_rn(Q1, DXX, __ffma2_rn(Q2, DXY, __fmul2_rn(Q3, DYY))));
+                                lx = L.x;
+                                ly = L.y;
+                            } else {
+                                lx = fmaf(uy, dy, fmaf(ux, dx, ox)) + dx;
+                                ly = fmaf(vy, dy, fmaf(vx, dx, oy)) + dy;
+                                if (ORDER == 2) {
+                                    dxx = dx * dx; dxy = dx * dy; dyy = dy * dy;
+                                    lx += fmaf(uxx, dxx, fmaf(uxy, dxy, uyy * dyy));
+                                    ly += fmaf(vxx, dxx, fmaf(vxy, dxy, vyy * dyy));
+                                }
                             }
                             float g;
                             if (FAST) {  // no edge clamp can apply and the window covers every tap
@@ -660,6 +682,17 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                                 ph1 = fmaf(Sh[nmax + i], gc, ph1);
                                 ph2 = fmaf(Sh[2 * nmax + i], gc, ph2);
                             }
+                            if (kPair) {
+                                const float2 G2 = __fmul2_rn(make_float2(rec.y, rec.z), make_float2(gc, gc));
+                                const float2 half = make_float2(0.5f, 0.5f);
+                                pbp[0] = __fadd2_rn(pbp[0], G2);
+                                pbp[1] = __ffma2_rn(G2, D2, pbp[1]);
+                                pbp[2] = __ffma2_rn(G2, E2, pbp[2]);
+                                pbp[3] = __ffma2_rn(G2, __fmul2_rn(half, DXX), pbp[3]);
+                                pbp[4] = __ffma2_rn(G2, DXY, pbp[4]);
+                                pbp[5] = __ffma2_rn(G2, __fmul2_rn(half, DYY), pbp[5]);
+                                continue;
+                            }
                             const float gxg = rec.y * gc, gyg = rec.z * gc;
                             pb[0] += gxg;
                             pb[1] += gyg;
@@ -683,6 +716,13 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                     sh0 += (double)ph0;
                     sh1 += (double)ph1;
                     sh2 += (double)ph2;
+                }
+            }
+            if (kPair) {
+#pragma unroll
+                for (int j = 0; j < 6; j++) {
+                    pb[(2 * j) % M] = pbp[j].x;
+                    pb[(2 * j + 1) % M] = pbp[j].y;
                 }
             }
         };
