@@ -609,9 +609,9 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         const int wx0 = wbx + offx, wy0 = wby + offy;
         auto sweep = [&](auto fast_tag) {
             constexpr bool FAST = decltype(fast_tag)::value;
-            // second order without clamps: the warp and the gradient sums as
+            // orders 1-2 without clamps: the warp and the gradient sums as
             // (x, y) pairs of paired FP32 ops (the same operations per lane)
-            constexpr bool kPair = FAST && ORDER == 2;
+            constexpr bool kPair = FAST && (ORDER == 2 || (ORDER == 1 && !RIGID));  // (slower for the closed-form rigid loop)
             const float2 U1 = make_float2(ux, vx), U2 = make_float2(uy, vy), O2 = make_float2(ox, oy);
             const float2 Q1 = make_float2(uxx, vxx), Q2 = make_float2(uxy, vxy), Q3 = make_float2(uyy, vyy);
             float2 pbp[6];
@@ -636,10 +636,12 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                                 D2 = make_float2(dx, dx);
                                 E2 = make_float2(dy, dy);
                                 float2 L = __fadd2_rn(__ffma2_rn(U2, E2, __ffma2_rn(U1, D2, O2)), make_float2(dx, dy));
-                                DXX = __fmul2_rn(D2, D2);
-                                DXY = __fmul2_rn(D2, E2);
-                                DYY = __fmul2_rn(E2, E2);
-                                L = __fadd2_rn(L, __ffma2_rn(Q1, DXX, __ffma2_rn(Q2, DXY, __fmul2_rn(Q3, DYY))));
+                                if (ORDER == 2) {
+                                    DXX = __fmul2_rn(D2, D2);
+                                    DXY = __fmul2_rn(D2, E2);
+                                    DYY = __fmul2_rn(E2, E2);
+                                    L = __fadd2_rn(L, __ffma2_rn(Q1, DXX, __ffma2_rn(Q2, DXY, __fmul2_rn(Q3, DYY))));
+                                }
                                 lx = L.x;
                                 ly = L.y;
                             } else {
@@ -688,9 +690,11 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                                 pbp[0] = __fadd2_rn(pbp[0], G2);
                                 pbp[1] = __ffma2_rn(G2, D2, pbp[1]);
                                 pbp[2] = __ffma2_rn(G2, E2, pbp[2]);
-                                pbp[3] = __ffma2_rn(G2, __fmul2_rn(half, DXX), pbp[3]);
-                                pbp[4] = __ffma2_rn(G2, DXY, pbp[4]);
-                                pbp[5] = __ffma2_rn(G2, __fmul2_rn(half, DYY), pbp[5]);
+                                if (ORDER == 2) {
+                                    pbp[3] = __ffma2_rn(G2, __fmul2_rn(half, DXX), pbp[3]);
+                                    pbp[4] = __ffma2_rn(G2, DXY, pbp[4]);
+                                    pbp[5] = __ffma2_rn(G2, __fmul2_rn(half, DYY), pbp[5]);
+                                }
                                 continue;
                             }
                             const float gxg = rec.y * gc, gyg = rec.z * gc;
@@ -720,9 +724,9 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             }
             if (kPair) {
 #pragma unroll
-                for (int j = 0; j < 6; j++) {
-                    pb[(2 * j) % M] = pbp[j].x;
-                    pb[(2 * j + 1) % M] = pbp[j].y;
+                for (int j = 0; j < M / 2; j++) {
+                    pb[2 * j] = pbp[j].x;
+                    pb[2 * j + 1] = pbp[j].y;
                 }
             }
         };
