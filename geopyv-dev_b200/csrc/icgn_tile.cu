@@ -388,26 +388,81 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         float mom[3 * NMOM];
 #pragma unroll
         for (int q = 0; q < 3 * NMOM; q++) mom[q] = 0.f;
-        for (int i = tid; i < npx_t; i += NT) {
-            const float4 rec = S4[i];
-            if (rec.x != rec.x) continue;
-            float dx, dy;
-            unpack_off(rec.w, dx, dy);
-            const float gx = rec.y, gy = rec.z;
-            float pxp[5], pyp[5];
-            pxp[0] = 1.f; pyp[0] = 1.f;
+        if constexpr (ORDER == 0) {
+            for (int i = tid; i < npx_t; i += NT) {
+                const float4 rec = S4[i];
+                if (rec.x != rec.x) continue;
+                mom[0] += rec.y * rec.y;
+                mom[1] += rec.y * rec.z;
+                mom[2] += rec.z * rec.z;
+            }
+        } else {
+            // the monomials in (x, y) pairs: (dx^e, dy^e) for e = 1..2 DEG,
+            // (dx^2 dy, dx dy^2) and (dx^3 dy, dx dy^3); dx dy and dx^2 dy^2
+            // alone; each moment takes one FMA per pixel, as a paired or a
+            // plain FP32 op, in pixel order
+            constexpr int E = 2 * O::DEG;
+            float2 mp[3][E], m21[3], m31[3];
+            float m00[3], m11[3], m22[3];
 #pragma unroll
-            for (int e = 1; e <= 2 * O::DEG; e++) { pxp[e] = pxp[e - 1] * dx; pyp[e] = pyp[e - 1] * dy; }
-            const float gg[3] = {gx * gx, gx * gy, gy * gy};
+            for (int p = 0; p < 3; p++) {
 #pragma unroll
-            for (int dgr = 0; dgr <= 2 * O::DEG; dgr++)
+                for (int e = 0; e < E; e++) mp[p][e] = make_float2(0.f, 0.f);
+                m21[p] = m31[p] = make_float2(0.f, 0.f);
+                m00[p] = m11[p] = m22[p] = 0.f;
+            }
+            for (int i = tid; i < npx_t; i += NT) {
+                const float4 rec = S4[i];
+                if (rec.x != rec.x) continue;
+                float dx, dy;
+                unpack_off(rec.w, dx, dy);
+                const float gx = rec.y, gy = rec.z;
+                float2 P[E];
+                P[0] = make_float2(dx, dy);
 #pragma unroll
-                for (int bb = 0; bb <= dgr; bb++) {
-                    const float mono = pxp[dgr - bb] * pyp[bb];
-#pragma unroll
-                    for (int p = 0; p < 3; p++)
-                        mom[p * NMOM + mom_idx(dgr - bb, bb)] = fmaf(gg[p], mono, mom[p * NMOM + mom_idx(dgr - bb, bb)]);
+                for (int e = 1; e < E; e++) P[e] = __fmul2_rn(P[e - 1], P[0]);
+                const float d11 = dx * dy;
+                const float gg[3] = {gx * gx, gx * gy, gy * gy};
+                float2 X21, X31;
+                float d22 = 0.f;
+                if (ORDER == 2) {
+                    const float2 sw = make_float2(dy, dx);
+                    X21 = __fmul2_rn(P[1], sw);
+                    X31 = __fmul2_rn(P[2], sw);
+                    d22 = P[1].x * P[1].y;
                 }
+#pragma unroll
+                for (int p = 0; p < 3; p++) {
+                    const float2 G2 = make_float2(gg[p], gg[p]);
+                    m00[p] += gg[p];
+#pragma unroll
+                    for (int e = 0; e < E; e++) mp[p][e] = __ffma2_rn(G2, P[e], mp[p][e]);
+                    m11[p] = fmaf(gg[p], d11, m11[p]);
+                    if (ORDER == 2) {
+                        m21[p] = __ffma2_rn(G2, X21, m21[p]);
+                        m31[p] = __ffma2_rn(G2, X31, m31[p]);
+                        m22[p] = fmaf(gg[p], d22, m22[p]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                float *m = mom + p * NMOM;
+                m[mom_idx(0, 0)] = m00[p];
+                m[mom_idx(1, 1)] = m11[p];
+#pragma unroll
+                for (int e = 1; e <= E; e++) {
+                    m[mom_idx(e, 0)] = mp[p][e - 1].x;
+                    m[mom_idx(0, e)] = mp[p][e - 1].y;
+                }
+                if (ORDER == 2) {
+                    m[mom_idx(2, 1)] = m21[p].x;
+                    m[mom_idx(1, 2)] = m21[p].y;
+                    m[mom_idx(3, 1)] = m31[p].x;
+                    m[mom_idx(1, 3)] = m31[p].y;
+                    m[mom_idx(2, 2)] = m22[p];
+                }
+            }
         }
         warp_sums_chunked<3 * NMOM>(mom, sm.red2[wid] + NVA, lane);
     }
