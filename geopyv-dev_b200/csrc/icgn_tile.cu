@@ -666,7 +666,8 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             constexpr bool FAST = decltype(fast_tag)::value;
             // orders 1-2 without clamps: the warp and the gradient sums as
             // (x, y) pairs of paired FP32 ops (the same operations per lane)
-            constexpr bool kPair = FAST && (ORDER == 2 || (ORDER == 1 && !RIGID));  // (slower for the closed-form rigid loop)
+            // (not for the closed-form first-order rigid loop, where it measured slower)
+            constexpr bool kPair = FAST && (ORDER == 2 || (ORDER == 1 && !RIGID));
             const float2 U1 = make_float2(ux, vx), U2 = make_float2(uy, vy), O2 = make_float2(ox, oy);
             const float2 Q1 = make_float2(uxx, vxx), Q2 = make_float2(uxy, vxy), Q3 = make_float2(uyy, vyy);
             float2 pbp[6];
@@ -674,7 +675,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             for (int j = 0; j < 6; j++) pbp[j] = make_float2(0.f, 0.f);
             for (int base = 0; base < npx_t; base += NT * kChunk) {
                 float p1 = 0.f, p2 = 0.f, pfg = 0.f, ph0 = 0.f, ph1 = 0.f, ph2 = 0.f;
-    #pragma unroll 2
+#pragma unroll 2
                 for (int c = 0; c < kChunk; c++) {
                     const int i = base + c * NT + tid;
                     if (i < npx_t) {
