@@ -662,8 +662,9 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
         // inside the image and the staged window (no clamps per sample)
         const bool fast = staged && inside;
         const int wx0 = wbx + offx, wy0 = wby + offy;
-        auto sweep = [&](auto fast_tag) {
+        auto sweep = [&](auto fast_tag, auto dense_tag) {
             constexpr bool FAST = decltype(fast_tag)::value;
+            constexpr bool DENSE = decltype(dense_tag)::value;  // no masked pixel: every record is valid
             // orders 1-2 without clamps: the warp and the gradient sums as
             // (x, y) pairs of paired FP32 ops (the same operations per lane)
             // (not for the closed-form first-order rigid loop, where it measured slower)
@@ -682,7 +683,7 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                         const float4 rec = rec_next;  // loaded one sample ahead
                         if (i + NT < npx_t) rec_next = S4[i + NT];
                         const float fv = rec.x;
-                        if (fv == fv) {
+                        if (DENSE || fv == fv) {
                             float dx, dy;
                             unpack_off(rec.w, dx, dy);
                             float lx, ly;
@@ -786,8 +787,9 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                 }
             }
         };
-        if (fast) sweep(std::true_type{});
-        else sweep(std::false_type{});
+        if (fast && n == npx_t) sweep(std::true_type{}, std::true_type{});
+        else if (fast) sweep(std::true_type{}, std::false_type{});
+        else sweep(std::false_type{}, std::false_type{});
         // block sums: warp partials to shared memory, one barrier, then warp 0
         // adds them up and updates the warp; a second barrier publishes p
         constexpr int KR = 3 + M + (kClosed ? 3 : 0);
