@@ -669,8 +669,9 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
             // (x, y) pairs of paired FP32 ops (the same operations per lane)
             // (not for the closed-form first-order rigid loop, where it measured slower)
             constexpr bool kPair = FAST && (ORDER == 2 || (ORDER == 1 && !RIGID));
-            const float2 U1 = make_float2(ux, vx), U2 = make_float2(uy, vy), O2 = make_float2(ox, oy);
-            const float2 Q1 = make_float2(uxx, vxx), Q2 = make_float2(uxy, vxy), Q3 = make_float2(uyy, vyy);
+            // the warp's pairs in (y, x) order, as the weights take them
+            const float2 U1 = make_float2(vx, ux), U2 = make_float2(vy, uy), O2 = make_float2(oy, ox);
+            const float2 Q1 = make_float2(vxx, uxx), Q2 = make_float2(vxy, uxy), Q3 = make_float2(vyy, uyy);
             float2 pbp[6];
 #pragma unroll
             for (int j = 0; j < 6; j++) pbp[j] = make_float2(0.f, 0.f);
@@ -688,19 +689,19 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                             unpack_off(rec.w, dx, dy);
                             float lx, ly;
                             float dxx = 0.f, dxy = 0.f, dyy = 0.f;
-                            float2 D2, E2, DXX, DXY, DYY;
+                            float2 D2, E2, DXX, DXY, DYY, L;  // L = (ly, lx)
                             if (kPair) {
                                 D2 = make_float2(dx, dx);
                                 E2 = make_float2(dy, dy);
-                                float2 L = __fadd2_rn(__ffma2_rn(U2, E2, __ffma2_rn(U1, D2, O2)), make_float2(dx, dy));
+                                L = __fadd2_rn(__ffma2_rn(U2, E2, __ffma2_rn(U1, D2, O2)), make_float2(dy, dx));
                                 if (ORDER == 2) {
                                     DXX = __fmul2_rn(D2, D2);
                                     DXY = __fmul2_rn(D2, E2);
                                     DYY = __fmul2_rn(E2, E2);
                                     L = __fadd2_rn(L, __ffma2_rn(Q1, DXX, __ffma2_rn(Q2, DXY, __fmul2_rn(Q3, DYY))));
                                 }
-                                lx = L.x;
-                                ly = L.y;
+                                lx = L.y;
+                                ly = L.x;
                             } else {
                                 lx = fmaf(uy, dy, fmaf(ux, dx, ox)) + dx;
                                 ly = fmaf(vy, dy, fmaf(vx, dx, oy)) + dy;
@@ -714,7 +715,8 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                             if (FAST) {  // no edge clamp can apply and the window covers every tap
                                 const float flx = floorf(lx), fly = floorf(ly);
                                 float a[6], b[6];
-                                basis_pair(ly - fly, lx - flx, a, b);
+                                if (kPair) basis_pair_yx(__fadd2_rn(L, make_float2(-fly, -flx)), a, b);
+                                else basis_pair(ly - fly, lx - flx, a, b);
                                 g = contract_rows2(win + ((int)fly + wy0) * gww + ((int)flx + wx0), gww, a, b);
                             } else {
                                 int ix, iy;
@@ -733,8 +735,14 @@ __device__ void tile_subset(const TileArgs &T, int idx, const gpv_subset_desc &d
                                 }
                             }
                             const float gc = g - fmf;
-                            p1 += gc;
-                            p2 = fmaf(gc, gc, p2);
+                            if (kPair) {  // (p1, p2) += (gc * 1, gc * gc)
+                                float2 q = __ffma2_rn(make_float2(gc, gc), make_float2(1.f, gc), make_float2(p1, p2));
+                                p1 = q.x;
+                                p2 = q.y;
+                            } else {
+                                p1 += gc;
+                                p2 = fmaf(gc, gc, p2);
+                            }
                             pfg = fmaf((RIGID && ORDER == 2 && rigid_on ? (fv - fmf) + St[i] : fv - fmf), gc, pfg);
                             if (kClosed && rigid_on) {
                                 ph0 = fmaf(Sh[i], gc, ph0);

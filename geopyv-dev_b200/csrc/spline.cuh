@@ -35,11 +35,11 @@ __device__ __forceinline__ void basis(T t, T w[6]) {
     w[3] = e2 - o2;
 }
 
-// basis() for two fractions at once (a from ty in .x, b from tx in .y): the
+// basis() for two fractions at once, t = (ty, tx): a from .x, b from .y, the
 // same operations per lane as basis(), issued as sm_100 paired FP32 ops.
-__device__ __forceinline__ void basis_pair(float ty, float tx, float a[6], float b[6]) {
+__device__ __forceinline__ void basis_pair_yx(float2 t, float a[6], float b[6]) {
 #if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
-    const float2 u = __fadd2_rn(make_float2(ty, tx), make_float2(-0.5f, -0.5f));
+    const float2 u = __fadd2_rn(t, make_float2(-0.5f, -0.5f));
     const float2 v = __fmul2_rn(u, u);
     const float2 nu = make_float2(-u.x, -u.y);
     auto poly = [&](float p2, float p1, float p0) {
@@ -56,6 +56,15 @@ __device__ __forceinline__ void basis_pair(float ty, float tx, float a[6], float
     const float2 w2 = __fadd2_rn(e2, o2), w3 = __fadd2_rn(e2, make_float2(-o2.x, -o2.y));
     a[0] = w0.x; a[1] = w1.x; a[2] = w2.x; a[3] = w3.x; a[4] = w4.x; a[5] = w5.x;
     b[0] = w0.y; b[1] = w1.y; b[2] = w2.y; b[3] = w3.y; b[4] = w4.y; b[5] = w5.y;
+#else
+    basis(t.x, a);
+    basis(t.y, b);
+#endif
+}
+
+__device__ __forceinline__ void basis_pair(float ty, float tx, float a[6], float b[6]) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    basis_pair_yx(make_float2(ty, tx), a, b);
 #else
     basis(ty, a);
     basis(tx, b);
