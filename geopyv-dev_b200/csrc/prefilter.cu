@@ -12,9 +12,11 @@
 // whose spectrum is evaluated here in closed form once per line length N
 // (the kernel's FFT in the reference).  |h_N[m]| decays as 0.4306^|m|, so
 // |m| <= 44 reproduces the FFT result to FP64 rounding (1e-14 relative; see
-// tests/test_prefilter_*).  Each pass is one kernel: a tile of 32 lines is
-// staged in shared memory with its circular halo and every thread slides an
-// 89-tap FP64 window along 16 outputs of one line (taps are kernel
+// tests/test_prefilter_*).  An image whose coefficients are kept in FP32
+// only uses |m| <= 28: the dropped taps sum to 2.7e-10 of the largest input
+// per pass, below FP32 rounding.  Each pass is one kernel: a tile of 32 lines
+// is staged in shared memory with its circular halo and every thread slides
+// a (2 MT + 1)-tap FP64 window along 16 outputs of one line (taps are kernel
 // parameters, i.e. constant-bank operands).  Row pass: pixels -> FP64
 // (h, w + 2b) (rows of the border are copies of rows 0 / h-1, so only the h
 // image rows are filtered); column pass: -> FP32 (and optionally FP64)
@@ -27,9 +29,9 @@
 namespace gpv {
 
 namespace {
-constexpr int kM = 44;             // taps on each side of the centre
+constexpr int kM = 44;             // taps on each side of the centre (FP64 coefficients)
+constexpr int kM32 = 28;           // the same when the coefficients are kept in FP32 only
 constexpr int kT = 2 * kM + 1;     // 89
-constexpr int kHalo = kT - 1;      // 88
 constexpr int kLines = 32;         // lines per tile (one per lane)
 constexpr int kGroups = 8;         // warps per block
 constexpr int kQ = 16;             // outputs per thread
@@ -47,10 +49,12 @@ __device__ __forceinline__ double px_load(const P *p, int64_t i) {
     return (double)p[i];
 }
 
-// Row pass: out[r][j] = sum_k taps[k] * X[r][(j - mr + k) mod cw], X = replicate-padded row r.
-template <typename P>
-__global__ void __launch_bounds__(kGroups * 32) rowpass89(const P *__restrict__ px, int64_t h, int64_t w, int64_t border,
-                                                          int64_t cw, int mr, TapArg taps, double *__restrict__ out) {
+// Row pass: out[r][j] = sum_k taps[k] * X[r][(j - MT + k) mod cw], X = replicate-padded row r,
+// k = 0 .. 2 MT.
+template <typename P, int MT>
+__global__ void __launch_bounds__(kGroups * 32) rowpass_fir(const P *__restrict__ px, int64_t h, int64_t w, int64_t border,
+                                                            int64_t cw, int mr, TapArg taps, double *__restrict__ out) {
+    constexpr int kTaps = 2 * MT + 1, kHalo = kTaps - 1;
     extern __shared__ double tile[];  // [kLines][kSpan + kHalo + 1]
     constexpr int stride = kSpan + kHalo + 1;
     const int64_t r0 = (int64_t)blockIdx.y * kLines;
@@ -77,7 +81,7 @@ __global__ void __launch_bounds__(kGroups * 32) rowpass89(const P *__restrict__ 
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
             const int k = s - q;
-            if (k >= 0 && k < kT) acc[q] = fma(taps.h[k], xv, acc[q]);
+            if (k >= 0 && k < kTaps) acc[q] = fma(taps.h[k], xv, acc[q]);
         }
     }
     const int64_t r = r0 + rr;
@@ -92,9 +96,12 @@ __global__ void __launch_bounds__(kGroups * 32) rowpass89(const P *__restrict__ 
 
 // Column pass over padded rows i: C[i][j] = sum_k taps[k] * R[(i - mr + k) mod ch][j],
 // R[ii] = rowpass[clamp(ii - border, 0, h - 1)].
-__global__ void __launch_bounds__(kGroups * 32) colpass89(const double *__restrict__ rp, int64_t h, int64_t cw, int64_t ch,
-                                                          int64_t border, int mr, TapArg taps, float *__restrict__ c32,
-                                                          int64_t pitch32, double *__restrict__ c64, int64_t pitch64) {
+template <int MT>
+__global__ void __launch_bounds__(kGroups * 32) colpass_fir(const double *__restrict__ rp, int64_t h, int64_t cw,
+                                                            int64_t ch, int64_t border, int mr, TapArg taps,
+                                                            float *__restrict__ c32, int64_t pitch32,
+                                                            double *__restrict__ c64, int64_t pitch64) {
+    constexpr int kTaps = 2 * MT + 1, kHalo = kTaps - 1;
     extern __shared__ double tile[];  // [kSpan + kHalo][kLines]
     const int64_t i0 = (int64_t)blockIdx.y * kSpan;
     const int64_t j0 = (int64_t)blockIdx.x * kLines;
@@ -120,7 +127,7 @@ __global__ void __launch_bounds__(kGroups * 32) colpass89(const double *__restri
 #pragma unroll
         for (int q = 0; q < kQ; q++) {
             const int k = s - q;
-            if (k >= 0 && k < kT) acc[q] = fma(taps.h[k], xv, acc[q]);
+            if (k >= 0 && k < kTaps) acc[q] = fma(taps.h[k], xv, acc[q]);
         }
     }
     const int64_t j = j0 + c;
@@ -178,19 +185,46 @@ void fill_taparg(const Taps &t, TapArg &a) {
     for (int k = 0; k < nt; k++) a.h[k] = t.h[t.mr - k + t.ml];
 }
 
+// The central 2 mt + 1 taps of a long line's filter (|m| <= mt), reversed.
+void fill_taparg_central(const Taps &t, int mt, TapArg &a) {
+    for (int k = 0; k <= 2 * mt; k++) a.h[k] = t.h[t.ml + mt - k];
+}
+
+// One FIR pass pair for lines of at least kT samples, MT taps on each side.
+template <typename P, int MT>
+int launch_fir_rows(gpv_image *img, const P *px, const Taps &tr, cudaStream_t s) {
+    constexpr int kHalo = 2 * MT;
+    const size_t smem_row = sizeof(double) * kLines * (kSpan + kHalo + 1);
+    TapArg a;
+    fill_taparg_central(tr, MT, a);
+    GPV_CUDA_TRY(cudaFuncSetAttribute(rowpass_fir<P, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row));
+    dim3 grid((unsigned)((img->cw + kSpan - 1) / kSpan), (unsigned)((img->h + kLines - 1) / kLines));
+    rowpass_fir<P, MT><<<grid, kGroups * 32, smem_row, s>>>(px, img->h, img->w, img->border, img->cw, MT, a,
+                                                             img->rowpass);
+    return GPV_SUCCESS;
+}
+
+template <int MT>
+int launch_fir_cols(gpv_image *img, const Taps &tc, cudaStream_t s) {
+    constexpr int kHalo = 2 * MT;
+    const size_t smem_col = sizeof(double) * (kSpan + kHalo) * kLines;
+    TapArg a;
+    fill_taparg_central(tc, MT, a);
+    GPV_CUDA_TRY(cudaFuncSetAttribute(colpass_fir<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_col));
+    dim3 grid((unsigned)((img->cw + kLines - 1) / kLines), (unsigned)((img->ch + kSpan - 1) / kSpan));
+    colpass_fir<MT><<<grid, kGroups * 32, smem_col, s>>>(img->rowpass, img->h, img->cw, img->ch, img->border, MT, a,
+                                                         img->c32, img->pitch32, img->c64, img->pitch64);
+    return GPV_SUCCESS;
+}
+
 template <typename P>
 int run_prefilter(gpv_image *img, const P *px, cudaStream_t s) {
     const Taps &tr = taps_for(img->cw);
     const Taps &tc = taps_for(img->ch);
-    const size_t smem_row = sizeof(double) * kLines * (kSpan + kHalo + 1);
-    const size_t smem_col = sizeof(double) * (kSpan + kHalo) * kLines;
+    const bool f32_only = img->c64 == nullptr;  // coefficients kept in FP32 only: |m| <= kM32
     if (tr.ml + tr.mr + 1 == kT) {
-        TapArg a;
-        fill_taparg(tr, a);
-        GPV_CUDA_TRY(cudaFuncSetAttribute(rowpass89<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row));
-        dim3 grid((unsigned)((img->cw + kSpan - 1) / kSpan), (unsigned)((img->h + kLines - 1) / kLines));
-        rowpass89<P><<<grid, kGroups * 32, smem_row, s>>>(px, img->h, img->w, img->border, img->cw, tr.mr, a,
-                                                          img->rowpass);
+        if (int rc = f32_only ? launch_fir_rows<P, kM32>(img, px, tr, s) : launch_fir_rows<P, kM>(img, px, tr, s))
+            return rc;
     } else {
         const int nt = tr.ml + tr.mr + 1;
         TapArg a;
@@ -204,12 +238,7 @@ int run_prefilter(gpv_image *img, const P *px, cudaStream_t s) {
     }
     GPV_CUDA_TRY(cudaGetLastError());
     if (tc.ml + tc.mr + 1 == kT) {
-        TapArg a;
-        fill_taparg(tc, a);
-        GPV_CUDA_TRY(cudaFuncSetAttribute(colpass89, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_col));
-        dim3 grid((unsigned)((img->cw + kLines - 1) / kLines), (unsigned)((img->ch + kSpan - 1) / kSpan));
-        colpass89<<<grid, kGroups * 32, smem_col, s>>>(img->rowpass, img->h, img->cw, img->ch, img->border, tc.mr, a,
-                                                       img->c32, img->pitch32, img->c64, img->pitch64);
+        if (int rc = f32_only ? launch_fir_cols<kM32>(img, tc, s) : launch_fir_cols<kM>(img, tc, s)) return rc;
     } else {
         const int nt = tc.ml + tc.mr + 1;
         TapArg a;
