@@ -33,6 +33,22 @@ def test_coefficients_match_oracle(oracle, gpv_mod, shape, border, dtype):
     assert np.abs(c32.astype(np.float64) - ref).max() <= 2e-7 * scale
 
 
+@pytest.mark.parametrize("shape,dtype", [((200, 300), np.uint8), ((257, 129), np.uint16), ((1024, 1024), np.uint8)])
+def test_fp32_only_coefficients_match_oracle(oracle, gpv_mod, shape, dtype):
+    """Images that keep FP32 coefficients only take the 57-tap filter
+    (|m| <= 28): still within the FP32 bound of the oracle, and within a few
+    FP32 roundings of the 89-tap coefficients of the same image."""
+    rng = np.random.default_rng(shape[0] * 11 + shape[1])
+    hi = 255 if dtype != np.uint16 else 4095
+    img = rng.integers(0, hi + 1, shape).astype(dtype)
+    ref = oracle.get_c(img.astype(np.float64), 20)
+    c32 = gpv_mod.Image(image_gs=img, border=20).coef().astype(np.float64)
+    c89 = gpv_mod.Image(image_gs=img, border=20, keep_f64=True).coef().astype(np.float64)
+    scale = np.abs(ref).max()
+    assert np.abs(c32 - ref).max() <= 2e-7 * scale
+    assert np.abs(c32 - c89).max() <= 1e-7 * scale
+
+
 def test_constant_image_gives_constant_coefficients(gpv_mod):
     # test_get_c_constant (src/image.rs:539-550): 20x25, border 5, value 77
     im = gpv_mod.Image(image_gs=np.full((20, 25), 77.0), border=5, keep_f64=True)
