@@ -400,8 +400,22 @@ int gpv_image_update(gpv_image *img, const void *px, int32_t dtype) {
         GPV_CUDA_TRY(cudaMalloc(&img->px_dev, bytes));
         img->px_bytes = bytes;
     }
-    GPV_CUDA_TRY(cudaMemcpyAsync(img->px_dev, px, bytes, cudaMemcpyHostToDevice, ctx->stream));
-    if (int rc = image_pixels_in(img, img->px_dev, dtype, ctx->stream, true)) return rc;
+    if (host_pinned(px, bytes)) {
+        // pinned pixels: the upload runs in row chunks beside the row passes
+        if (!img->up_stream) {
+            GPV_CUDA_TRY(cudaStreamCreateWithFlags(&img->up_stream, cudaStreamNonBlocking));
+            for (cudaEvent_t &e : img->up_ev) GPV_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        if (int rc = prefilter_from_host(img, px, dtype, ctx->stream, img->up_stream, img->up_ev, 5)) return rc;
+        img->px_current = true;
+        img->px_dtype = dtype;
+        if (img->grain) {
+            if (int rc = grain_launch(img, img->px_dev, dtype, ctx->stream)) return rc;
+        }
+    } else {
+        GPV_CUDA_TRY(cudaMemcpyAsync(img->px_dev, px, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        if (int rc = image_pixels_in(img, img->px_dev, dtype, ctx->stream, true)) return rc;
+    }
     GPV_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return GPV_SUCCESS;
 }
@@ -492,6 +506,12 @@ int gpv_image_destroy(gpv_image *img) {
     cudaFree(img->grain64);
     cudaFree(img->grain_scal);
     cudaFree(img->grain_ac);
+    if (img->up_stream) {
+        cudaStreamSynchronize(img->up_stream);
+        cudaStreamDestroy(img->up_stream);
+    }
+    for (cudaEvent_t e : img->up_ev)
+        if (e) cudaEventDestroy(e);
     gpv_context *ctx = img->ctx;
     delete img;
     context_release(ctx);

@@ -129,6 +129,9 @@ struct gpv_image {
     double *grain64 = nullptr;  // the same maps in FP64 (images that keep FP64 coefficients)
     double *grain_scal = nullptr;
     double *grain_ac = nullptr;  // autocorrelation lag sums (2 x 256)
+    // chunked uploads of pinned host pixels (created on first use)
+    cudaStream_t up_stream = nullptr;
+    cudaEvent_t up_ev[5] = {};
 };
 
 struct gpv_mask {
@@ -140,6 +143,10 @@ struct gpv_mask {
 namespace gpv {
 // prefilter.cu
 int prefilter_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s);
+// host pixels (pinned) -> img->px_dev in row chunks on cs, each chunk's row
+// pass on s once it has landed, then the column pass on s; ev: nev >= 2 events
+int prefilter_from_host(gpv_image *img, const void *px_host, int dtype, cudaStream_t s, cudaStream_t cs,
+                        cudaEvent_t *ev, int nev);
 // New pixels into an image: prefilter, and the grain maps when it keeps them.
 // staged: px_dev is the image's own staging (it then holds the pixels).
 int image_pixels_in(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s, bool staged);

@@ -21,6 +21,7 @@
 // (h, w + 2b) (rows of the border are copies of rows 0 / h-1, so only the h
 // image rows are filtered); column pass: -> FP32 (and optionally FP64)
 // coefficients (h + 2b, w + 2b).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -191,16 +192,18 @@ void fill_taparg_central(const Taps &t, int mt, TapArg &a) {
 }
 
 // One FIR pass pair for lines of at least kT samples, MT taps on each side.
+// Rows [r0, r0 + nr) of the image (rows are filtered independently).
 template <typename P, int MT>
-int launch_fir_rows(gpv_image *img, const P *px, const Taps &tr, cudaStream_t s) {
+int launch_fir_rows(gpv_image *img, const P *px, const Taps &tr, cudaStream_t s, int64_t r0 = 0, int64_t nr = -1) {
     constexpr int kHalo = 2 * MT;
+    if (nr < 0) nr = img->h - r0;
     const size_t smem_row = sizeof(double) * kLines * (kSpan + kHalo + 1);
     TapArg a;
     fill_taparg_central(tr, MT, a);
     GPV_CUDA_TRY(cudaFuncSetAttribute(rowpass_fir<P, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row));
-    dim3 grid((unsigned)((img->cw + kSpan - 1) / kSpan), (unsigned)((img->h + kLines - 1) / kLines));
-    rowpass_fir<P, MT><<<grid, kGroups * 32, smem_row, s>>>(px, img->h, img->w, img->border, img->cw, MT, a,
-                                                             img->rowpass);
+    dim3 grid((unsigned)((img->cw + kSpan - 1) / kSpan), (unsigned)((nr + kLines - 1) / kLines));
+    rowpass_fir<P, MT><<<grid, kGroups * 32, smem_row, s>>>(px + r0 * img->w, nr, img->w, img->border, img->cw, MT, a,
+                                                             img->rowpass + r0 * img->cw);
     return GPV_SUCCESS;
 }
 
@@ -286,6 +289,58 @@ const Taps &taps_for(int64_t n) {
         t.h[m + t.ml] = acc / (double)n;
     }
     return g_taps.emplace(n, std::move(t)).first->second;
+}
+
+namespace {
+// Host pixels in row chunks into img->px_dev on the copy stream cs; the row
+// pass of each chunk starts on s as soon as its copy has landed, so the
+// copies overlap the row passes; then the column pass on s.  Lines too short
+// for the FIR kernels take the whole copy, then the ordinary prefilter.
+template <typename P>
+int prefilter_host(gpv_image *img, const P *px_host, cudaStream_t s, cudaStream_t cs, cudaEvent_t *ev, int nev) {
+    P *dst = static_cast<P *>(img->px_dev);
+    const size_t row_bytes = sizeof(P) * (size_t)img->w;
+    const Taps &tr = taps_for(img->cw);
+    const Taps &tc = taps_for(img->ch);
+    const bool fir = tr.ml + tr.mr + 1 == kT && tc.ml + tc.mr + 1 == kT;
+    const int64_t chunk = (img->h / (nev - 1) + kLines - 1) / kLines * kLines;  // rows per copy
+    // the copies wait for earlier work on s that may still read px_dev
+    GPV_CUDA_TRY(cudaEventRecord(ev[0], s));
+    GPV_CUDA_TRY(cudaStreamWaitEvent(cs, ev[0], 0));
+    if (!fir || img->h < 2 * kLines * (nev - 1)) {
+        GPV_CUDA_TRY(cudaMemcpyAsync(dst, px_host, row_bytes * (size_t)img->h, cudaMemcpyHostToDevice, cs));
+        GPV_CUDA_TRY(cudaEventRecord(ev[1], cs));
+        GPV_CUDA_TRY(cudaStreamWaitEvent(s, ev[1], 0));
+        return run_prefilter(img, static_cast<const P *>(dst), s);
+    }
+    const bool f32_only = img->c64 == nullptr;
+    int k = 1;
+    for (int64_t r0 = 0; r0 < img->h; r0 += chunk, k++) {
+        const int64_t nr = std::min(chunk, img->h - r0);
+        GPV_CUDA_TRY(cudaMemcpyAsync(dst + r0 * img->w, px_host + r0 * img->w, row_bytes * (size_t)nr,
+                                     cudaMemcpyHostToDevice, cs));
+        GPV_CUDA_TRY(cudaEventRecord(ev[k], cs));
+        GPV_CUDA_TRY(cudaStreamWaitEvent(s, ev[k], 0));
+        if (int rc = f32_only ? launch_fir_rows<P, kM32>(img, dst, tr, s, r0, nr)
+                              : launch_fir_rows<P, kM>(img, dst, tr, s, r0, nr))
+            return rc;
+    }
+    GPV_CUDA_TRY(cudaGetLastError());
+    if (int rc = f32_only ? launch_fir_cols<kM32>(img, tc, s) : launch_fir_cols<kM>(img, tc, s)) return rc;
+    GPV_CUDA_TRY(cudaGetLastError());
+    return GPV_SUCCESS;
+}
+}  // namespace
+
+int prefilter_from_host(gpv_image *img, const void *px_host, int dtype, cudaStream_t s, cudaStream_t cs,
+                        cudaEvent_t *ev, int nev) {
+    switch (dtype) {
+        case GPV_U8: return prefilter_host(img, static_cast<const uint8_t *>(px_host), s, cs, ev, nev);
+        case GPV_U16: return prefilter_host(img, static_cast<const uint16_t *>(px_host), s, cs, ev, nev);
+        case GPV_F32: return prefilter_host(img, static_cast<const float *>(px_host), s, cs, ev, nev);
+        case GPV_F64: return prefilter_host(img, static_cast<const double *>(px_host), s, cs, ev, nev);
+        default: set_error("unknown pixel dtype"); return GPV_ERR_INVALID;
+    }
 }
 
 int prefilter_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s) {
