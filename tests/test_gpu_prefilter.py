@@ -100,3 +100,32 @@ def test_far_out_of_range_query_saturates(gpv_mod):
         assert abs(far - edge) < 1e-3
         _, g = im.eval([[1_000_000.0, -1_000_000.0]], grad=True, precision=prec)
         assert np.all(np.isfinite(g)) and np.all(np.abs(g) < 200.0)
+
+
+@pytest.mark.parametrize("dtype,keep_f64", [(np.uint16, False), (np.uint8, True), (np.float64, False)])
+def test_pinned_chunked_update_equals_pageable_update(gpv_mod, dtype, keep_f64):
+    """gpv_image_update from page-locked pixels uploads them in row chunks
+    beside the row passes: the coefficients (and the pixel staging the grain
+    statistics read) equal those of an update from pageable memory."""
+    import ctypes as ct
+
+    import torch
+    from gpv import _lib
+    rng = np.random.default_rng(17)
+    shape = (1000, 777)
+    hi = 4095 if dtype == np.uint16 else 255
+    img = rng.integers(0, hi + 1, shape).astype(dtype)
+    a = gpv_mod.Image(image_gs=np.zeros(shape, dtype), border=20, keep_f64=keep_f64)
+    b = gpv_mod.Image(image_gs=np.zeros(shape, dtype), border=20, keep_f64=keep_f64)
+    a.update(img)  # pageable
+    pinned = torch.from_numpy(img.view(np.uint8).reshape(-1).copy()).pin_memory()
+    _lib.check(_lib.lib().gpv_image_update(b.handle, ct.c_void_p(pinned.data_ptr()), _lib.DTYPES[np.dtype(dtype)]),
+               "gpv_image_update (pinned)")
+    assert np.array_equal(a.coef(), b.coef())
+    if keep_f64:
+        assert np.array_equal(a.coef(f64=True), b.coef(f64=True))
+    a.build_grain()
+    b.build_grain()
+    ga, gb = a.grain(maps=True), b.grain(maps=True)
+    assert ga["correlation_length"] == gb["correlation_length"]
+    assert np.array_equal(ga["maps"], gb["maps"])
