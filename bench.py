@@ -731,9 +731,9 @@ def run_ours(args, world, rank, local):
     if prec == gpv.PREC_MIXED and not os.environ.get("GPV_TILE_THREADS"):
         tuned = gpv.autotune(F, G, desc, sample_per_class=2048)
     layouts = [lay for _, lay in ctx.tuning()]
-    peak_buf = ct.c_double(0.0)
-    _lib.check(L.gpv_probe_fp32_peak(ctx.handle, ct.byref(peak_buf)), "probe")
-    fp32_peak = peak_buf.value
+    peaks = _lib.Peaks()
+    _lib.check(L.gpv_probe_peaks(ctx.handle, ct.byref(peaks)), "probe")
+    fp32_peak = max(peaks.fp32_scalar_tflops, peaks.fp32_paired_tflops)
     for _ in range(args.warmup):
         full_step()
     torch.cuda.synchronize()
@@ -859,7 +859,10 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "fp32" if t_fma >= t_bytes else "hbm", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
                      "kernel": "icgn_tile<2,128>" if prec == gpv.PREC_MIXED else "icgn_fp64",
-                     "peak_source": "measured live: register-only FP32 FMA kernel (gpv_probe_fp32_peak)",
+                     "peak_scalar": peaks.fp32_scalar_tflops, "peak_paired": peaks.fp32_paired_tflops,
+                     "peak_source": "measured live (gpv_probe_peaks): the larger of register-only FFMA and paired "
+                                    "FFMA2 chains (of measured)",
+                     "fp64_peak_tflops": peaks.fp64_tflops, "smem_peak_gbs": peaks.smem_gbs,
                      "work": "2 x (42 FMA per target sample x iterations + 90 FMA per reference sample)",
                      "t_fma_ms": 1e3 * t_fma, "t_bytes_ms": 1e3 * t_bytes,
                      "roofline_frac": max(t_fma, t_bytes) / (solve_avg_ms * 1e-3),

@@ -1113,4 +1113,11 @@ int gpv_probe_fp32_peak(gpv_context *ctx, double *tflops) {
     return probe_fp32_peak(ctx, tflops);
 }
 
+int gpv_probe_peaks(gpv_context *ctx, gpv_peaks *out) {
+    if (!ctx || !out) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    return probe_peaks(ctx, out);
+}
+
 }  // extern "C"

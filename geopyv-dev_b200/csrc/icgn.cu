@@ -959,52 +959,3 @@ int solve_launch(gpv_context *ctx, const SolveLaunch &L, cudaStream_t s) {
 }
 
 }  // namespace gpv
-
-// ---------------------------------------------------------------------------
-// FP32 FMA throughput probe: independent FMA chains in registers only.
-// ---------------------------------------------------------------------------
-namespace gpv {
-namespace {
-constexpr int kProbeChains = 8;
-constexpr int kProbeIters = 4096;
-__global__ void __launch_bounds__(256) fma_probe(float *out, float a, float b) {
-    float x[kProbeChains];
-#pragma unroll
-    for (int c = 0; c < kProbeChains; c++) x[c] = (float)(threadIdx.x + c);
-    for (int it = 0; it < kProbeIters; it++) {
-#pragma unroll
-        for (int c = 0; c < kProbeChains; c++) x[c] = fmaf(x[c], a, b);
-    }
-    float s = 0.f;
-#pragma unroll
-    for (int c = 0; c < kProbeChains; c++) s += x[c];
-    if (s == 1234.5f) out[threadIdx.x] = s;  // keeps the chains live
-}
-}  // namespace
-
-int probe_fp32_peak(gpv_context *ctx, double *tflops) {
-    const int blocks = ctx->num_sms * 8;
-    float *out = nullptr;
-    GPV_CUDA_TRY(cudaMalloc(&out, 256 * sizeof(float)));
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    double best = 0.0;
-    for (int rep = 0; rep < 5; rep++) {
-        cudaEventRecord(e0, ctx->stream);
-        fma_probe<<<blocks, 256, 0, ctx->stream>>>(out, 0.9999f, 1e-4f);
-        cudaEventRecord(e1, ctx->stream);
-        cudaEventSynchronize(e1);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        const double flop = 2.0 * blocks * 256.0 * kProbeChains * kProbeIters;
-        if (rep > 0 && ms > 0.f) best = fmax(best, flop / (ms * 1e-3) / 1e12);
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaFree(out);
-    GPV_CUDA_TRY(cudaGetLastError());
-    *tflops = best;
-    return GPV_SUCCESS;
-}
-}  // namespace gpv

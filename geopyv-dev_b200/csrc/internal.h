@@ -172,6 +172,7 @@ int eval_launch(const gpv_image *img, const double *xy_dev, int64_t n, int preci
                 cudaStream_t s);
 int ensure_tables(gpv_context *ctx, int max_radius);
 int probe_fp32_peak(gpv_context *ctx, double *tflops);
+int probe_peaks(gpv_context *ctx, gpv_peaks *out);  // probe.cu
 int mesh_drive(const double *nodes, int64_t n_nodes, const int64_t *elements, int64_t n_elements,
                int32_t nodes_per_element, const gpv_mesh_params *mp, gpv_batch_solver_fn solver, void *solver_user,
                gpv_subset_result *out, int32_t *rounds, gpv_mesh_stats *stats);

@@ -303,7 +303,9 @@ int prefilter_host(gpv_image *img, const P *px_host, cudaStream_t s, cudaStream_
     const Taps &tr = taps_for(img->cw);
     const Taps &tc = taps_for(img->ch);
     const bool fir = tr.ml + tr.mr + 1 == kT && tc.ml + tc.mr + 1 == kT;
-    const int64_t chunk = (img->h / (nev - 1) + kLines - 1) / kLines * kLines;  // rows per copy
+    // rows per copy: ceil(h / (nev - 1)) rounded up to whole row tiles, so at
+    // most nev - 1 chunks (events ev[1 .. nev-1]) cover the image
+    const int64_t chunk = ((img->h + nev - 2) / (nev - 1) + kLines - 1) / kLines * kLines;
     // the copies wait for earlier work on s that may still read px_dev
     GPV_CUDA_TRY(cudaEventRecord(ev[0], s));
     GPV_CUDA_TRY(cudaStreamWaitEvent(cs, ev[0], 0));
@@ -316,7 +318,8 @@ int prefilter_host(gpv_image *img, const P *px_host, cudaStream_t s, cudaStream_
     const bool f32_only = img->c64 == nullptr;
     int k = 1;
     for (int64_t r0 = 0; r0 < img->h; r0 += chunk, k++) {
-        const int64_t nr = std::min(chunk, img->h - r0);
+        // the last event takes whatever rows remain (never an event past ev[nev - 1])
+        const int64_t nr = k == nev - 1 ? img->h - r0 : std::min(chunk, img->h - r0);
         GPV_CUDA_TRY(cudaMemcpyAsync(dst + r0 * img->w, px_host + r0 * img->w, row_bytes * (size_t)nr,
                                      cudaMemcpyHostToDevice, cs));
         GPV_CUDA_TRY(cudaEventRecord(ev[k], cs));

@@ -79,6 +79,14 @@ class ServerStats(ct.Structure):
                 ("bytes_in_flight", ct.c_size_t), ("peak_bytes", ct.c_size_t), ("hbm_budget", ct.c_size_t)]
 
 
+class Peaks(ct.Structure):
+    _fields_ = [("fp32_scalar_tflops", ct.c_double), ("fp32_paired_tflops", ct.c_double),
+                ("fp64_tflops", ct.c_double), ("smem_gbs", ct.c_double), ("sm_count", ct.c_int32),
+                ("reserved", ct.c_int32)]
+
+
+assert ct.sizeof(Peaks) == 40
+
 REQUEST_REUSE_REFERENCE, REQUEST_SEED_FROM_PREVIOUS = 1, 2
 CONTEXT_HIGH_PRIORITY, CONTEXT_PER_SUBSET_BLOCKS = 1, 2
 
@@ -124,6 +132,7 @@ SIGNATURES = {
     "gpv_solve_batch": (ct.c_int, [P, P, P, P, I64, P, P]),
     "gpv_solve_batch_device": (ct.c_int, [P, P, P, P, P, I64, P, P, P]),
     "gpv_probe_fp32_peak": (ct.c_int, [P, P]),
+    "gpv_probe_peaks": (ct.c_int, [P, P]),
     "gpv_autotune": (ct.c_int, [P, P, P, P, I64, P, I32, P]),
     "gpv_context_tuning": (ct.c_int, [P, P, P]),
     "gpv_batch_graph_create": (ct.c_int, [P, P, P, P, P, I64, P, P, P]),

@@ -52,7 +52,8 @@ typedef enum { GPV_U8 = 1, GPV_U16 = 2, GPV_F32 = 3, GPV_F64 = 4 } gpv_dtype;
 /* ---- precision of the solve -------------------------------------------- */
 typedef enum {
     GPV_PREC_MIXED = 0, /* FP32 interpolation/warp/residual, FP64 reductions,
-                           Hessian inverse and warp composition; warp per subset */
+                           Hessian solve and warp composition; one thread block
+                           per subset at a time                               */
     GPV_PREC_FP64 = 1   /* FP64 throughout, one subset per thread block      */
 } gpv_precision;
 
@@ -466,6 +467,22 @@ int gpv_context_tuning(gpv_context *ctx, int32_t *threads, int32_t *layouts);
  * Measured FP32 FMA throughput of this device (TFLOP/s, 2 FLOP per FMA) from
  * a register-only FMA kernel: the denominator of the interpolation roofline. */
 int gpv_probe_fp32_peak(gpv_context *ctx, double *tflops);
+
+/* Measured throughputs of this device (no reference counterpart: the
+ * denominators of the solve's rooflines).  FP32 FMA as scalar FFMA chains
+ * and as sm_100 paired FFMA2 chains (gpv_probe_fp32_peak reports the larger),
+ * FP64 DFMA, and shared-memory read bandwidth over all SMs (conflict-free
+ * 16-byte loads).  TFLOP/s count 2 FLOP per FMA. */
+typedef struct {
+    double fp32_scalar_tflops;
+    double fp32_paired_tflops;
+    double fp64_tflops;
+    double smem_gbs;
+    int32_t sm_count;
+    int32_t reserved;
+} gpv_peaks;
+
+int gpv_probe_peaks(gpv_context *ctx, gpv_peaks *out);
 
 #ifdef __cplusplus
 }

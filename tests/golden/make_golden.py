@@ -2,15 +2,15 @@
 
 reference_kats.json -- the known-answer values of the reference crate's own
 unit tests for this path, transcribed with their file:line (within the
-geopyv-dev repository).  When the reference checkout is available (path in
-$GPV_REFERENCE, default /root/reference) every transcribed literal is looked
-up at its cited line, so a mis-transcription fails loudly here.
+geopyv-dev repository).  When $GPV_REFERENCE names a checkout of the
+reference, every transcribed literal is looked up at its cited line, so a
+mis-transcription fails loudly here; without it that check is skipped.
 
 oracle_small.npz -- a small seeded synthetic pair (workload 1 at 1/8 scale)
 with the FP64 oracle's coefficients and batch results, so tests can detect
 an oracle change independently of the oracle itself.
 
-    python tests/golden/make_golden.py
+    GPV_REFERENCE=<geopyv-dev checkout> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -21,7 +21,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("GPV_REFERENCE", "/root/reference")
+REF = os.environ.get("GPV_REFERENCE", "")
 
 S2 = math.sqrt(2.0) / 4.0
 KATS = [
@@ -152,8 +152,8 @@ KATS = [
 
 
 def verify_provenance():
-    if not os.path.isdir(REF):
-        print("reference checkout not found; provenance not re-checked")
+    if not REF or not os.path.isdir(REF):
+        print("GPV_REFERENCE does not name a reference checkout; provenance not re-checked")
         return
     for k in KATS:
         path, lines = k["src"].split(":")

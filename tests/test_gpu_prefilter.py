@@ -102,8 +102,12 @@ def test_far_out_of_range_query_saturates(gpv_mod):
         assert np.all(np.isfinite(g)) and np.all(np.abs(g) < 200.0)
 
 
-@pytest.mark.parametrize("dtype,keep_f64", [(np.uint16, False), (np.uint8, True), (np.float64, False)])
-def test_pinned_chunked_update_equals_pageable_update(gpv_mod, dtype, keep_f64):
+@pytest.mark.parametrize("dtype,keep_f64,shape", [
+    (np.uint16, False, (1000, 777)), (np.uint8, True, (1000, 777)), (np.float64, False, (1000, 777)),
+    # heights whose quarter is a whole number of 32-row tiles but which do not
+    # split into four equal parts (the chunk count must stay within the events)
+    (np.uint8, False, (1025, 300)), (np.uint16, True, (257, 640)), (np.uint8, False, (2049, 200))])
+def test_pinned_chunked_update_equals_pageable_update(gpv_mod, dtype, keep_f64, shape):
     """gpv_image_update from page-locked pixels uploads them in row chunks
     beside the row passes: the coefficients (and the pixel staging the grain
     statistics read) equal those of an update from pageable memory."""
@@ -112,7 +116,6 @@ def test_pinned_chunked_update_equals_pageable_update(gpv_mod, dtype, keep_f64):
     import torch
     from gpv import _lib
     rng = np.random.default_rng(17)
-    shape = (1000, 777)
     hi = 4095 if dtype == np.uint16 else 255
     img = rng.integers(0, hi + 1, shape).astype(dtype)
     a = gpv_mod.Image(image_gs=np.zeros(shape, dtype), border=20, keep_f64=keep_f64)

@@ -32,7 +32,7 @@ def _request(rng, size, dtype, n, seed):
     return f, g, gpv.make_desc(xy, radius, order, p0)
 
 
-def test_results_alone_equal_results_in_the_mix(gpv_mod):
+def test_results_alone_equal_results_in_the_mix(gpv_mod, oracle):
     rng = np.random.default_rng(5)
     reqs = []
     for k, (size, dt) in enumerate([(256, np.uint8), (512, np.uint16), (1024, np.uint8), (256, np.uint16),
@@ -45,11 +45,24 @@ def test_results_alone_equal_results_in_the_mix(gpv_mod):
     st = srv.stats()
     assert st["completed"] == len(reqs) and st["failed"] == 0 and st["p99_ms"] > 0
     srv.close()
-    for (f, g, d), got in zip(reqs, mixed):
+    for k, ((f, g, d), got) in enumerate(zip(reqs, mixed)):
         ctx = gpv_mod.Context(0)
         alone = gpv_mod.solve_batch(gpv_mod.Image(image_gs=f, ctx=ctx), gpv_mod.Image(image_gs=g, ctx=ctx), d)
         assert alone.tobytes() == got.tobytes()
         assert np.mean(got["converged"]) > 0.95
+        # served results against the FP64 oracle on a sample of each request
+        # (the mixed-precision bar: 1e-3 px, 1e-5 strain, identical flags)
+        pick = np.random.default_rng(k).choice(len(d), min(len(d), 60), replace=False)
+        Cf = oracle.get_c(f.astype(np.float64), 20)
+        Cg = oracle.get_c(g.astype(np.float64), 20)
+        ref = oracle.solve_batch(Cf, Cg, f.shape, 20, d[pick], max_norm=1e-5, max_iterations=50, tolerance=0.75)
+        sub = got[pick]
+        assert np.array_equal(sub["status"], ref["status"])
+        assert np.array_equal(sub["converged"], ref["converged"])
+        assert np.array_equal(sub["quality_ok"], ref["quality_ok"])
+        ok = ref["status"] == 0
+        assert np.abs(sub["p"][ok, :2] - ref["p"][ok, :2]).max() <= 1e-3
+        assert np.abs(sub["p"][ok, 2:6] - ref["p"][ok, 2:6]).max() <= 1e-5
 
 
 def test_per_subset_blocks_give_the_persistent_bytes(gpv_mod):
