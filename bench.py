@@ -41,9 +41,9 @@ sys.path.insert(0, os.path.join(ROOT, "geopyv-dev_b200"))
 # hardware work queues for the serving leg's concurrent worker streams
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of the icgn_tile<2,128>
-# launch of one full-size second-order step (564.47 + 413.38 MB)
-ICGN_C2_DRAM_BYTES = 977.85e6
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size
+# second-order solve launch, by kernel (captured separately, not in this run)
+ICGN_C2_DRAM_BYTES = {"icgn_tile<2,128>": 977.85e6}
 
 METRIC = "ICGN subsets/s at <=1e-3 px vs FP64 oracle; p50/p99 served solve latency"
 
@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch (graph) leg")
     ap.add_argument("--no-rigid", action="store_true", help="skip the rigid-texture leg")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form on the full batch")
+    ap.add_argument("--no-c1", action="store_true", help="skip the first-order 1024^2 workload at full size")
+    ap.add_argument("--sequence-frames", type=int, default=200, help="frames of the sequence leg")
     ap.add_argument("--serving-seconds", type=float, default=10.0)
     return ap.parse_args()
 
@@ -229,6 +232,22 @@ def load_workload(args):
     W = synth.workload(args.config, scale_down=args.scale_down)
     W["gen_s"] = time.time() - t
     return W
+
+
+def common_config(W, args, world):
+    """The workload's `config` object, the same in both arms."""
+    h, w = W["f"].shape
+    l2_bytes = 2 * 4 * (h + 40) * (w + 40) + 2 * 8 * h * (w + 40)
+    orders = np.unique(W["order"])
+    return {"workload": W["name"], "subsets": int(len(W["coords"])), "image": [int(h), int(w)],
+            "pixel_dtype": str(W["f"].dtype), "radius": int(np.max(W["radius"])),
+            "order": int(orders[0]) if len(orders) == 1 else "mixed", "max_norm": 1e-5,
+            "max_iterations": 15 if args.config == 1 else 50,
+            "step": "prefilter(f)+prefilter(g)+batched ICGN solve of every subset",
+            "l2": (("inputs larger than L2" if l2_bytes > 126e6 else "inputs SMALLER than L2 (profiling case)") +
+                   f": 2 x {h + 40}x{w + 40} FP32 coefficients + FP64 row passes ({l2_bytes / 1e6:.0f} MB)"
+                   " rewritten each step"),
+            "parallelism": f"replicas x{world}"}
 
 
 def measured_hbm_gbs():
@@ -421,6 +440,110 @@ def uneven_leg(device, steps=10):
 
 
 # ---------------------------------------------------------------------------
+def fp64_leg(W, device, mixed_solve_ms, steps=3):
+    """The plain one-subset-per-block FP64 form (icgn_fp64: FP64 coefficients,
+    interpolation, sums and solve) on the headline batch, device-resident,
+    CUDA events around `steps` solves; beside it the mixed form's solve time
+    of the same batch from the headline timing."""
+    import ctypes as ct
+
+    import torch
+
+    import gpv
+    from gpv import _lib
+    ctx = gpv.Context(device)
+    F = gpv.Image(image_gs=W["f"], border=20, ctx=ctx, keep_f64=True)
+    G = gpv.Image(image_gs=W["g"], border=20, ctx=ctx, keep_f64=True)
+    desc = gpv.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
+    n = len(desc)
+    ctx.reserve(n, int(desc["radius"].max()), 50)
+    d_dev = torch.from_numpy(desc.view(np.uint8).copy()).cuda(device)
+    out_dev = torch.zeros(n * _lib.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{device}")
+    prm = gpv._params(1e-5, 50, 0.75, False, gpv.PREC_FP64, None, None)
+    L = _lib.lib()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    args = (ctx.handle, F.handle, G.handle, ct.c_void_p(d_dev.data_ptr()), None, n, ct.byref(prm),
+            ct.c_void_p(out_dev.data_ptr()), None)
+    _lib.check(L.gpv_solve_batch_device(*args), "fp64 solve")
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        _lib.check(L.gpv_solve_batch_device(*args), "fp64 solve")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    res = np.frombuffer(out_dev.cpu().numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
+    return {"kernel": "icgn_fp64 (one block of 256 threads per subset, FP64 throughout)", "subsets": n,
+            "solve_ms": ms, "fp64_plain_subsets_per_s": n / (ms * 1e-3),
+            "mixed_solve_ms": mixed_solve_ms, "mixed_over_fp64": ms / mixed_solve_ms,
+            "iterations_mean": float(res["iterations"].mean()), "converged_frac": float(res["converged"].mean()),
+            "timing": "CUDA events on the library stream, device-resident inputs, solve only (both forms)"}
+
+
+def c1_leg(device, steps=10):
+    """The first-order workload at full size (1024^2 u8, rigid (0.35, -0.20)
+    px, r = 25 on a 20 px grid, 15 iterations): steps of prefilter(f) +
+    prefilter(g) + solve through the device C ABI (CUDA events), and every
+    subset compared with the FP64 oracle."""
+    import ctypes as ct
+
+    import torch
+
+    import gpv
+    from gpv import _lib, synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    W = synth.workload(1)
+    ctx = gpv.Context(device)
+    F = gpv.Image(image_gs=W["f"], border=20, ctx=ctx)
+    G = gpv.Image(image_gs=W["g"], border=20, ctx=ctx)
+    desc = gpv.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
+    n = len(desc)
+    ctx.reserve(n, 25, 15)
+    f_dev = torch.from_numpy(W["f"].copy()).cuda(device)
+    g_dev = torch.from_numpy(W["g"].copy()).cuda(device)
+    d_dev = torch.from_numpy(desc.view(np.uint8).copy()).cuda(device)
+    out_dev = torch.zeros(n * _lib.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{device}")
+    prm = gpv._params(1e-5, 15, 0.75, False, gpv.PREC_MIXED, None, None)
+    L = _lib.lib()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def step():
+        _lib.check(L.gpv_image_update_device(F.handle, ct.c_void_p(f_dev.data_ptr()), _lib.GPV_U8), "update f")
+        _lib.check(L.gpv_image_update_device(G.handle, ct.c_void_p(g_dev.data_ptr()), _lib.GPV_U8), "update g")
+        _lib.check(L.gpv_solve_batch_device(ctx.handle, F.handle, G.handle, ct.c_void_p(d_dev.data_ptr()), None, n,
+                                            ct.byref(prm), ct.c_void_p(out_dev.data_ptr()), None), "solve")
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    res = np.frombuffer(out_dev.cpu().numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
+    O.build()
+    t0 = time.perf_counter()
+    Cf, Cg = O.get_c(W["f"].astype(np.float64), 20), O.get_c(W["g"].astype(np.float64), 20)
+    ref = O.solve_batch(Cf, Cg, W["f"].shape, 20, desc, max_norm=1e-5, max_iterations=15)
+    tc = time.perf_counter() - t0
+    ok = (ref["status"] == 0) & (ref["converged"] == 1)
+    return {"workload": W["name"], "subsets": n, "steps": steps, "ms_per_step": ms, "subsets_per_s": n / (ms * 1e-3),
+            "iterations_mean": float(res["iterations"].mean()),
+            "accuracy": {"oracle_subsets": n, "max_disp_err_px": float(np.abs(res["p"][ok, :2] - ref["p"][ok, :2]).max()),
+                         "max_strain_err": float(np.abs(res["p"][ok, 2:6] - ref["p"][ok, 2:6]).max()),
+                         "flag_agreement": float(np.mean((res["converged"] == ref["converged"]) &
+                                                         (res["quality_ok"] == ref["quality_ok"]))),
+                         "iteration_agreement": float(np.mean(res["iterations"] == ref["iterations"])),
+                         "max_err_vs_imposed_px": float(np.abs(res["p"][ok, :2] - W["truth_uv"][ok]).max())},
+            "cpu_oracle_step_s": tc, "cpu_oracle_cores": int(O.lib().gpvo_max_threads()),
+            "timing": "CUDA events on the library stream; step = prefilter(f) + prefilter(g) + solve, device pixels"}
+
+
+# ---------------------------------------------------------------------------
 def rigid_leg(W, device, steps=5):
     """The headline batch with the rigid-texture template (src/texture.rs): the
     reference's grain maps built on the device from its pixels, then the
@@ -485,25 +608,27 @@ def rigid_leg(W, device, steps=5):
 
 
 # ---------------------------------------------------------------------------
-def sequence_leg(ctx, n_frames=20, frame_step=10):
+def sequence_leg(ctx, n_frames=200, frame_step=1):
     """Frame-to-frame tracking (gpv_sequence_*) on the incremental-sequence
-    workload: 2048^2 u8 frames under simple shear rising by 0.25% per frame,
-    20,000 subsets of radius 25, reference fixed at frame 0.  Per frame:
-    pinned host pixels -> device, in-place prefilter, seeding from the last
-    converged warps, batched solve; results stay on the device.  Timed with
-    CUDA events on the library stream over frames 1..n-1, once as CUDA-graph
-    replay and once as eager launches."""
+    workload: 2048^2 u8 frames under simple shear rising linearly to 5% at
+    frame 200 (every frame by default), 20,000 subsets of radius 25,
+    reference fixed at frame 0.  Per frame: pinned host pixels -> device,
+    in-place prefilter, seeding from the last converged warps, batched solve;
+    results stay on the device.  Timed with CUDA events on the library stream
+    over frames 1..n-1, once as CUDA-graph replay and once as eager launches."""
     import torch
 
     import gpv
     from gpv import synth
-    Ws = [synth.workload(4, 1, seed_frame=frame_step * k) for k in range(n_frames)]
-    W0 = Ws[0]
-    pins = [torch.from_numpy(W["g"].copy()).pin_memory() for W in Ws]
+    t0 = time.perf_counter()
+    W0, frames = synth.sequence_frames(n_frames, 1, frame_step)
+    gen_s = time.perf_counter() - t0
+    n_frames = len(frames)
+    pins = [torch.from_numpy(g).pin_memory() for g in frames]
     desc = gpv.make_desc(W0["coords"], W0["radius"], W0["order"], W0["p0"])
     stream = torch.cuda.ExternalStream(ctx.stream)
-    out = {"workload": W0["name"].replace("frame 0 ", "") + f", {n_frames} frames, shear +{0.05 * frame_step / 200:.4f}/frame",
-           "subsets": int(len(desc)), "frames_timed": n_frames - 1}
+    out = {"workload": W0["name"].replace("frame 0 ", "") + f", {n_frames} frames, shear +{0.05 * frame_step / 200:.5f}/frame",
+           "subsets": int(len(desc)), "frames_timed": n_frames - 1, "frame_generation_s": gen_s}
     for graph in (True, False):
         F = gpv.Image(image_gs=W0["f"], border=20, ctx=ctx)
         G = gpv.Image(image_gs=W0["f"], border=20, ctx=ctx)
@@ -528,7 +653,9 @@ def sequence_leg(ctx, n_frames=20, frame_step=10):
             import ctypes as ct
             _lib.check(_lib.lib().gpv_sequence_frame(seq._h, ct.c_void_p(pins[-1].data_ptr()), 0,
                                                      res.ctypes.data_as(ct.c_void_p)), "frame")
-            truth = synth.displacement(Ws[-1]["field"], W0["coords"])
+            c = (W0["f"].shape[0] - 1) / 2.0
+            last = synth.make_field(xc=c, yc=c, a=(0.0, 0.05 * frame_step * (n_frames - 1) / 200.0, 0.0, 0.0))
+            truth = synth.displacement(last, W0["coords"])
             good = res["converged"] == 1
             out["converged_frac_last_frame"] = float(good.mean())
             out["max_err_vs_field_px_last_frame"] = float(np.abs(res["p"][good, :2] - truth[good]).max())
@@ -642,26 +769,64 @@ def serving_leg(seconds=10.0, rate=200.0, seed=55, configs=None):
 
 # ---------------------------------------------------------------------------
 def run_reference(args, world, rank):
-    """--impl reference: the oracle restatement of the reference's CPU solver."""
+    """--impl reference: the FP64 C restatement of the reference's CPU solver
+    (the Rust crate cannot be built here) on the box's host cores.  Every
+    timed step is a full step of the workload -- the oracle's prefilter of
+    both images and the solve of every subset, all host threads -- timed by
+    the host clock; warm-up steps solve a bounded sample.  A single-core rate
+    on a bounded sample follows the timed steps."""
     if rank != 0:
         return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    import gpv
+    O.build()
     W = load_workload(args)
-    steps = []
-    for i in range(args.warmup + args.steps):
-        b = cpu_baseline(W, args, seconds=max(2.0, args.cpu_seconds / 3), rng_seed=100 + i)
-        if i >= args.warmup:
-            steps.append(b)
-    vals = [b["value"] for b in steps]
-    v = float(np.mean(vals))
-    b = steps[-1]
+    nthreads = O.lib().gpvo_max_threads()
+    d = gpv.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
+    n = len(d)
+    max_it = 15 if args.config == 1 else 50
+    f64, g64 = W["f"].astype(np.float64), W["g"].astype(np.float64)
+    rng = np.random.default_rng(100)
+
+    def solve(Cf, Cg, dd, threads):
+        return O.solve_batch(Cf, Cg, W["f"].shape, 20, dd, max_norm=1e-5, max_iterations=max_it, nthreads=threads)
+
+    for _ in range(args.warmup):  # bounded: prefilter + 2% of the subsets
+        Cf, Cg = O.get_c(f64, 20, nthreads), O.get_c(g64, 20, nthreads)
+        solve(Cf, Cg, d[rng.choice(n, max(64, n // 50), replace=False)], nthreads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        Cf, Cg = O.get_c(f64, 20, nthreads), O.get_c(g64, 20, nthreads)
+        ref = solve(Cf, Cg, d, nthreads)
+        times.append(time.perf_counter() - t0)
+    v = n * args.steps / float(np.sum(times))
+    # one host thread on a bounded sample (~seconds), solve only
+    k = min(n, 64)
+    t0 = time.perf_counter()
+    solve(Cf, Cg, d[:k], 1)
+    per = (time.perf_counter() - t0) / k
+    ks = int(min(n, max(k, args.cpu_seconds / 3.0 / max(per, 1e-9))))
+    pick = rng.choice(n, ks, replace=False)
+    t0 = time.perf_counter()
+    solve(Cf, Cg, d[pick], 1)
+    t1 = time.perf_counter() - t0
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "subsets/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * W["coords"].shape[0] / v,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": W["name"], "subsets": int(W["coords"].shape[0])},
-        "cpu_baseline": {"value": v, "unit": "subsets/s", "cores": b["cores"], "kind": "port",
-                         "sample": f"{len(b['sample_idx'])} random subsets per step + prefilter of both images "
-                                   f"(FP64 C restatement of src/subset.rs / src/image.rs, OpenMP)"},
+        "config": common_config(W, args, world),
+        "cpu_baseline": {"value": v, "unit": "subsets/s", "cores": int(nthreads), "kind": "port",
+                         "sample": f"every step whole: oracle prefilter of both images + all {n} subsets (FP64 C "
+                                   "restatement of src/image.rs / src/subset.rs, OpenMP); warm-up steps: prefilter "
+                                   "+ 2% of the subsets"},
+        "single_core": {"subsets_per_s": ks / t1, "cores": 1, "sample": f"{ks} random subsets, solve only, "
+                                                                          f"{t1:.1f} s"},
+        "step_ms": [1e3 * t for t in times],
+        "converged_frac": float(np.mean(ref["converged"])),
+        "timing": "host clock (time.perf_counter) around each full step",
         "e2e": {"value": v, "unit": "subsets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -730,7 +895,16 @@ def run_ours(args, world, rank, local):
     tuned = [0, 0, 0]
     if prec == gpv.PREC_MIXED and not os.environ.get("GPV_TILE_THREADS"):
         tuned = gpv.autotune(F, G, desc, sample_per_class=2048)
-    layouts = [lay for _, lay in ctx.tuning()]
+    layouts = [t["layout"] for t in ctx.tuning()]
+    runk = [t["run_length"] for t in ctx.tuning()]
+    runs = os.environ.get("GPV_SOLVE_KERNEL", "runs")[:1] != "t"
+    cls = 0 if max_r <= 20 else (1 if max_r <= 40 else 2)
+    if prec != gpv.PREC_MIXED:
+        kernel_name = "icgn_fp64"
+    elif runs:
+        kernel_name = f"icgn_runs<{2 if args.config == 2 else 'mixed'},{tuned[cls] or 128},{runk[cls] or 8}>"
+    else:
+        kernel_name = f"icgn_tile<{2 if args.config == 2 else 'mixed'},{tuned[cls] or 128}>"
     peaks = _lib.Peaks()
     _lib.check(L.gpv_probe_peaks(ctx.handle, ct.byref(peaks)), "probe")
     fp32_peak = max(peaks.fp32_scalar_tflops, peaks.fp32_paired_tflops)
@@ -812,22 +986,30 @@ def run_ours(args, world, rank, local):
         mesh = mesh_leg(W, F, G, args, cpu=not args.no_cpu_baseline)
     seq = None
     if not args.no_sequence and args.config == 2 and args.scale_down == 1:
-        seq = sequence_leg(ctx)
+        seq = sequence_leg(ctx, n_frames=args.sequence_frames)
     uneven = None
     if not args.no_uneven and args.config == 2 and args.scale_down == 1:
         uneven = uneven_leg(local)
     rigid = None
     if not args.no_rigid and args.config == 2 and args.scale_down == 1 and prec == gpv.PREC_MIXED:
         rigid = rigid_leg(W, local)
+    fp64 = None
+    if not args.no_fp64 and args.config == 2 and prec == gpv.PREC_MIXED:
+        fp64 = fp64_leg(W, local, float(np.mean(solve_ms)))
+    c1 = None
+    if not args.no_c1 and args.config == 2 and args.scale_down == 1:
+        c1 = c1_leg(local)
     serving = None
     if not args.no_serving and args.config == 2 and args.scale_down == 1:
         serving = serving_leg(seconds=args.serving_seconds)
     flop = algorithmic_flop(res)
     solve_avg_ms = float(np.mean(solve_ms))
     achieved = flop / (solve_avg_ms * 1e-3) / 1e12
-    # DRAM bytes (read + write) of one solve launch, from ncu at full size
-    # (profiles/icgn_tile_c2.md): known for the second-order workload only
-    traffic = ICGN_C2_DRAM_BYTES if (args.config == 2 and args.scale_down == 1 and prec == gpv.PREC_MIXED) else None
+    # DRAM bytes (read + write) of one solve launch from an ncu capture of the
+    # same command at full size (not measured in this run; null elsewhere)
+    traffic = None
+    if args.config == 2 and args.scale_down == 1 and prec == gpv.PREC_MIXED:
+        traffic = ICGN_C2_DRAM_BYTES.get(kernel_name)
     samples = float(np.sum(res["n_px"].astype(np.float64) * (res["iterations"] + 1)))
     # roofline time = the slower of the tap FMAs at the FP32 peak and the
     # coefficient-window bytes at the measured HBM bandwidth
@@ -841,16 +1023,12 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": "subsets/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if prec == gpv.PREC_MIXED else "f64", "data": "synthetic",
-        "config": {"workload": W["name"], "subsets": n, "image": [h, w], "pixel_dtype": str(px_dtype),
-                   "radius": max_r, "order": 2 if args.config == 2 else "mixed", "max_norm": 1e-5,
-                   "max_iterations": 50, "precision": args.precision,
-                   "step": "prefilter(f)+prefilter(g)+batched ICGN solve",
-                   "l2": (("inputs larger than L2" if l2_bytes > 126e6 else "inputs SMALLER than L2 (profiling case)") +
-                          f": 2 x {h + 40}x{w + 40} FP32 coefficients + FP64 row passes ({l2_bytes / 1e6:.0f} MB)"
-                          " rewritten each step"),
-                   "parallelism": f"replicas x{world}",
-                   "tuned_threads_per_subset": {"r<=20": tuned[0], "r21-40": tuned[1], "r>40": tuned[2]},
-                   "tuned_layout": {"r<=20": layouts[0], "r21-40": layouts[1], "r>40": layouts[2]}},
+        "config": common_config(W, args, world),
+        "precision": args.precision,
+        "tuning": {"threads_per_block": {"r<=20": tuned[0], "r21-40": tuned[1], "r>40": tuned[2]},
+                   "tile_layout": {"r<=20": layouts[0], "r21-40": layouts[1], "r>40": layouts[2]},
+                   "run_length": {"r<=20": runk[0], "r21-40": runk[1], "r>40": runk[2]},
+                   "kernel": kernel_name},
         "solve_ms": solve_avg_ms, "prefilter_ms": t_max / args.steps - solve_avg_ms,
         "samples_per_s": world * samples * args.steps / (t_max * 1e-3),
         "iterations_mean": float(np.mean(res["iterations"])),
@@ -858,7 +1036,10 @@ def run_ours(args, world, rank, local):
         "accuracy": acc,
         "roofline": {"bound": "fp32" if t_fma >= t_bytes else "hbm", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak else None, "traffic": traffic,
-                     "kernel": "icgn_tile<2,128>" if prec == gpv.PREC_MIXED else "icgn_fp64",
+                     "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size "
+                                        f"{kernel_name} launch, captured separately (profiles/)"
+                                        if traffic else "not captured for this configuration"),
+                     "kernel": kernel_name,
                      "peak_scalar": peaks.fp32_scalar_tflops, "peak_paired": peaks.fp32_paired_tflops,
                      "peak_source": "measured live (gpv_probe_peaks): the larger of register-only FFMA and paired "
                                     "FFMA2 chains (of measured)",
@@ -883,6 +1064,12 @@ def run_ours(args, world, rank, local):
         line["uneven_batch"] = uneven
     if rigid is not None:
         line["rigid_texture"] = rigid
+    if fp64 is not None:
+        line["fp64_plain"] = fp64
+        line["fp64_plain_subsets_per_s"] = fp64["fp64_plain_subsets_per_s"]
+        line["mixed_over_fp64"] = fp64["mixed_over_fp64"]
+    if c1 is not None:
+        line["c1"] = c1
     if serving is not None:
         line["serving"] = serving
         line["p50_ms"] = serving["p50_ms"]

@@ -33,18 +33,36 @@ def _stale(target: str, sources: list[str]) -> bool:
     return any(os.path.getmtime(s) > t for s in sources)
 
 
+OBJ = os.path.join(HERE, "_build")  # per-source objects (git-ignored)
+FLAGS = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr"]
+
+
 def build_cuda(force: bool = False, verbose: bool = False) -> str:
+    """Each source compiles to its own object (recompiled when it, a local
+    header or include/gpv.h is newer), then one link; sources compile in
+    parallel."""
+    from concurrent.futures import ThreadPoolExecutor
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
-    deps = srcs + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+    headers = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
         [os.path.join(ROOT, "include", "gpv.h")]
     target = os.path.join(OUT, "libgpv_b200.so")
-    if not force and not _stale(target, deps):
-        return target
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-O3",
-           "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include"), "-o", target, *srcs, "-lcudart"]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    os.makedirs(OBJ, exist_ok=True)
+    objs, jobs = [], []
+    for src in srcs:
+        obj = os.path.join(OBJ, os.path.basename(src) + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src, *headers]):
+            cmd = [NVCC, *FLAGS, "-I" + os.path.join(ROOT, "include"), "-c", src, "-o", obj]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            jobs.append(cmd)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for r in ex.map(lambda c: subprocess.run(c, capture_output=not verbose, text=True), jobs):
+            if r.returncode != 0:
+                sys.stderr.write((r.stdout or "") + (r.stderr or ""))
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+    if jobs or force or _stale(target, objs):
+        subprocess.run([NVCC, *ARCH, "-shared", "-o", target, *objs, "-lcudart"], check=True)
     return target
 
 

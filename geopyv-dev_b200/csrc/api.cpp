@@ -288,7 +288,8 @@ static void context_release(gpv_context *ctx) {
     DeviceGuard dg(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (DevBuf *b : {&ctx->offs, &ctx->slots, &ctx->tab_off, &ctx->tab_n, &ctx->scratch, &ctx->queue, &ctx->desc_dev, &ctx->out_dev,
-                      &ctx->order_dev, &ctx->hist_dev, &ctx->eval_dev, &ctx->tile_ws, &ctx->slot_mask})
+                      &ctx->order_dev, &ctx->hist_dev, &ctx->eval_dev, &ctx->tile_ws, &ctx->slot_mask,
+                      &ctx->run_tasks, &ctx->run_off, &ctx->run_n})
         b->release();
     ctx->h_stage.release();
     for (int k = 0; k < 2; k++)
@@ -848,12 +849,13 @@ int gpv_solve_batch_device(gpv_context *ctx, const gpv_image *f, const gpv_image
 
 // Addresses of the context workspace a captured solve reads and writes.
 struct WorkspaceAddrs {
-    const void *p[8];
+    const void *p[11];
     bool operator==(const WorkspaceAddrs &o) const { return std::memcmp(p, o.p, sizeof p) == 0; }
 };
 static WorkspaceAddrs workspace_addrs(const gpv_context *ctx) {
     return WorkspaceAddrs{{ctx->scratch.ptr, ctx->queue.ptr, ctx->tile_ws.ptr, ctx->offs.ptr, ctx->slots.ptr,
-                           ctx->tab_off.ptr, ctx->tab_n.ptr, ctx->slot_mask.ptr}};
+                           ctx->tab_off.ptr, ctx->tab_n.ptr, ctx->slot_mask.ptr, ctx->run_tasks.ptr, ctx->run_off.ptr,
+                           ctx->run_n.ptr}};
 }
 
 struct gpv_batch_graph {
@@ -1010,6 +1012,12 @@ int gpv_mesh_solve(gpv_context *ctx, const gpv_image *f, const gpv_image *g, con
 
 static int radius_class(int r) { return r <= 20 ? 0 : (r <= 40 ? 1 : 2); }
 
+extern "C++" {
+namespace gpv {
+bool use_run_kernel();  // icgn_tile.cu
+}
+}
+
 static void tune_cache_load(gpv_context *ctx) {
     const char *path = getenv("GPV_TUNE_CACHE");
     if (!path) return;
@@ -1020,11 +1028,12 @@ static void tune_cache_load(gpv_context *ctx) {
     char line[512];
     while (fgets(line, sizeof line, fh)) {
         char name[256];
-        int cls = -1, nt = 0, layout = -1;
-        const int got = sscanf(line, "%255[^|]|%d|%d|%d", name, &cls, &nt, &layout);
+        int cls = -1, nt = 0, layout = -1, runk = 0;
+        const int got = sscanf(line, "%255[^|]|%d|%d|%d|%d", name, &cls, &nt, &layout, &runk);
         if (got >= 3 && cls >= 0 && cls < 3 && strcmp(name, prop.name) == 0 && (nt == 128 || nt == 256)) {
             ctx->tuned_threads[cls] = nt;  // later lines win
-            ctx->tuned_layout[cls] = (got == 4 && layout >= 0 && layout <= 2) ? layout : -1;
+            ctx->tuned_layout[cls] = (got >= 4 && layout >= 0 && layout <= 2) ? layout : -1;
+            ctx->tuned_run_k[cls] = (got == 5 && (runk == 4 || runk == 8)) ? runk : 0;
         }
     }
     fclose(fh);
@@ -1044,8 +1053,13 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
     p.precision = GPV_PREC_MIXED;
     p.history = nullptr;
     p.flags &= ~(GPV_SOLVE_ETA | GPV_SOLVE_FAGN | GPV_SOLVE_RIGID_TEXTURE);  // the tuned kernel is the mixed ICGN one
-    // candidates: threads per block x template layout (compact, 8 x 4 tiles)
-    static const int cand[4][2] = {{128, 0}, {256, 0}, {128, 2}, {256, 2}};
+    // candidates: threads per block x run length (run-layout kernel), or
+    // threads per block x template layout (compact, 8 x 4 tiles) when the
+    // tiled kernel is selected
+    const bool runs = use_run_kernel();
+    static const int cand_runs[4][2] = {{128, 8}, {256, 8}, {128, 4}, {256, 4}};
+    static const int cand_tile[4][2] = {{128, 0}, {256, 0}, {128, 2}, {256, 2}};
+    const int(*cand)[2] = runs ? cand_runs : cand_tile;
     for (int c = 0; c < 3; c++) {
         if (threads_out) threads_out[c] = 0;
         if (cls[c].empty()) continue;
@@ -1055,11 +1069,13 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
         for (size_t j = 0; j < k; j++) smp.push_back(cls[c][j * cls[c].size() / k]);
         std::vector<gpv_subset_result> out(smp.size());
         double best = 1e300;
-        int best_nt = 128, best_layout = 0;
-        for (const auto &cd : cand) {
+        int best_nt = 128, best_layout = 0, best_k = 0;
+        for (int ci = 0; ci < 4; ci++) {
+            const int *cd = cand[ci];
             const int t = cd[0];
             ctx->force_threads = t;
-            ctx->force_layout = cd[1];
+            ctx->force_layout = runs ? -1 : cd[1];
+            ctx->force_run_k = runs ? cd[1] : 0;
             double ms_best = 1e300;
             for (int rep = 0; rep < 3; rep++) {
                 cudaEvent_t e0, e1;
@@ -1073,21 +1089,28 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
                 cudaEventElapsedTime(&ms, e0, e1);
                 cudaEventDestroy(e0);
                 cudaEventDestroy(e1);
-                if (rc) { ctx->force_threads = 0; ctx->force_layout = -1; return rc; }
+                if (rc) { ctx->force_threads = 0; ctx->force_layout = -1; ctx->force_run_k = 0; return rc; }
                 if (rep > 0) ms_best = std::min(ms_best, (double)ms);
             }
-            if (ms_best < best) { best = ms_best; best_nt = t; best_layout = cd[1]; }
+            if (ms_best < best) {
+                best = ms_best;
+                best_nt = t;
+                best_layout = runs ? -1 : cd[1];
+                best_k = runs ? cd[1] : 0;
+            }
         }
         ctx->force_threads = 0;
         ctx->force_layout = -1;
+        ctx->force_run_k = 0;
         ctx->tuned_threads[c] = best_nt;
         ctx->tuned_layout[c] = best_layout;
+        ctx->tuned_run_k[c] = best_k;
         if (threads_out) threads_out[c] = best_nt;
         if (const char *path = getenv("GPV_TUNE_CACHE")) {
             cudaDeviceProp prop;
             if (cudaGetDeviceProperties(&prop, ctx->device) == cudaSuccess) {
                 if (FILE *fh = fopen(path, "a")) {
-                    fprintf(fh, "%s|%d|%d|%d\n", prop.name, c, best_nt, best_layout);
+                    fprintf(fh, "%s|%d|%d|%d|%d\n", prop.name, c, best_nt, best_layout, best_k);
                     fclose(fh);
                 }
             }
@@ -1102,6 +1125,20 @@ int gpv_context_tuning(gpv_context *ctx, int32_t *threads, int32_t *layouts) {
     for (int c = 0; c < 3; c++) {
         if (threads) threads[c] = ctx->tuned_threads[c];
         if (layouts) layouts[c] = ctx->tuned_layout[c];
+    }
+    return GPV_SUCCESS;
+}
+
+int gpv_context_tuning_get(gpv_context *ctx, gpv_tuning *out) {
+    if (!ctx || !out) { set_error("NULL argument"); return GPV_ERR_INVALID; }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    for (int c = 0; c < 3; c++) {
+        out[c].threads = ctx->tuned_threads[c];
+        out[c].layout = ctx->tuned_layout[c];
+        out[c].run_length = ctx->tuned_run_k[c];
+        out[c].subsets_per_block = 0;
+        out[c].staging = 0;
+        out[c].reserved = 0;
     }
     return GPV_SUCCESS;
 }

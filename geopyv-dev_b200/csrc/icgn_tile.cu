@@ -1217,6 +1217,8 @@ void tile_launch_one(int nt, bool per_subset, int order, bool rigid, int blocks,
 
 }  // namespace
 
+bool use_run_kernel();
+
 // Threads per block of the tiled kernel for subsets of radius r: the
 // autotuned choice when one was recorded for this radius class, else a
 // size rule (GPV_TILE_THREADS overrides).
@@ -1301,6 +1303,8 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
     struct Plan {
         int rmax = 0, nt = 0, layout = 0, cap = 0, blocks = 0, per_sm = 0;
         bool ps = false, rigid = false;  // one block per subset; rigid-texture template
+        bool runs = false;               // the run-layout kernel (icgn_runs.cu), run length run_k
+        int run_k = 0, nslot = 0;
         int64_t stride = 0;
         bool live = false;
     };
@@ -1321,8 +1325,15 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         P.rmax = std::min(kRBoundHost[c], K.max_radius);
         P.nt = tile_threads_for(ctx, P.rmax);
         P.layout = tile_layout_for(ctx, P.rmax);
-        P.cap = window_cap(P.rmax, P.layout);
-        const void *fn = tile_kernel(P.nt, P.ps, order, P.rigid);
+        // persistent deformable segments run the run-layout kernel unless
+        // GPV_SOLVE_KERNEL=tile asks for the tiled one
+        P.runs = !P.rigid && use_run_kernel();
+        if (P.runs) {
+            P.run_k = run_length_for(ctx, P.rmax);
+            if (int rc = ensure_run_tables(ctx, K.max_radius)) return rc;
+        }
+        P.cap = P.runs ? run_window_cap(P.rmax, P.run_k) : window_cap(P.rmax, P.layout);
+        const void *fn = P.runs ? run_kernel(order, P.nt, P.run_k, P.ps) : tile_kernel(P.nt, P.ps, order, P.rigid);
         int max_bytes = 0;
         if (int rc = allow_max_dynamic_smem(fn, &max_bytes)) return rc;
         // a window larger than the block can hold is not staged: those
@@ -1336,6 +1347,7 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         P.per_sm = per_sm;
         const int64_t nmax = (int64_t)(ctx->h_slot_n[P.rmax] + 31) / 32 * 32;
         P.stride = (P.rigid ? 9 : 5) * nmax;  // float4 record + eta sample (+ 3 grain samples, template) per pixel
+        if (P.runs) P.stride = run_scratch_floats(ctx, P.rmax, P.run_k, &P.nslot);
         int64_t slots;
         if (P.ps) {
             P.blocks = (int)ctx->seg_count[q];
@@ -1378,7 +1390,13 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         T.slots_per_sm = P.per_sm;
         T.n_mask = ctx->n_smid;
         const size_t smem = sizeof(float) * P.cap;
-        tile_launch_one(P.nt, P.ps, 2 - q / kRClasses, P.rigid, P.blocks, smem, st[k], T);
+        if (P.runs) {
+            if (int rc = run_launch(ctx, 2 - q / kRClasses, P.nt, P.run_k, P.blocks, smem, st[k], T.k, T.seg, T.queue,
+                                    P.cap, P.nslot, T.slot_mask, T.slots_per_sm, T.n_mask))
+                return rc;
+        } else {
+            tile_launch_one(P.nt, P.ps, 2 - q / kRClasses, P.rigid, P.blocks, smem, st[k], T);
+        }
         GPV_CUDA_TRY(cudaGetLastError());
     }
     for (int k = 1; k < 3; k++) {
@@ -1399,6 +1417,21 @@ int tile_layout_for(gpv_context *ctx, int max_radius) {
     if (ctx->force_layout >= 0) return ctx->force_layout;
     const int cls = max_radius <= 20 ? 0 : (max_radius <= 40 ? 1 : 2);
     return ctx->tuned_layout[cls] >= 0 ? ctx->tuned_layout[cls] : kLayoutCompact;
+}
+
+// GPV_SOLVE_KERNEL=tile selects the tiled kernel for every segment; the
+// default is the run-layout kernel for persistent deformable segments.
+bool use_run_kernel() {
+    const char *v = getenv("GPV_SOLVE_KERNEL");
+    return !(v && v[0] == 't');
+}
+
+int run_length_for(gpv_context *ctx, int max_radius) {
+    if (ctx->force_run_k) return ctx->force_run_k;
+    if (const char *v = getenv("GPV_RUN_K")) return atoi(v) == 4 ? 4 : 8;
+    const int cls = max_radius <= 20 ? 0 : (max_radius <= 40 ? 1 : 2);
+    if (ctx->tuned_run_k[cls]) return ctx->tuned_run_k[cls];
+    return 8;
 }
 
 int tile_threads_for(gpv_context *ctx, int max_radius) {

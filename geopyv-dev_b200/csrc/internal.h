@@ -101,6 +101,13 @@ struct gpv_context {
     uint32_t flags = 0;                // GPV_CONTEXT_*
     int n_smid = 0;                    // SM identifiers of the device (per-subset blocks)
     gpv::DevBuf slot_mask;             // per stream region, per SM: claimed scratch slots
+    // run tables of the run-layout solve (icgn_runs.cu): lengths 4 and 8, radii 1..run_table_radius
+    int run_table_radius = 0;
+    gpv::DevBuf run_tasks;             // int2 per task: dx | dy0 << 16, circle bits
+    gpv::DevBuf run_off, run_n;        // int32 [2][run_table_radius + 1]
+    std::vector<int32_t> h_run_n;
+    int tuned_run_k[3] = {0, 0, 0};    // autotuned run length by radius class (0: default)
+    int force_run_k = 0;               // set while the autotuner times a candidate
     gpv::HostBuf h_stage;              // pinned staging of host batches: desc | work order | results
     cudaEvent_t ev_chunk[8] = {};      // chunked result downloads through h_stage
     // owner reference + one per image / mask created on it: the context is
@@ -191,6 +198,19 @@ constexpr int kTileSegs = 12;
 int tile_segment_of(int r, int o);
 // Number of SM identifiers (%nsmid) of the current device.
 int query_nsmid(int *out);
+// icgn_runs.cu: the run-layout solve kernel (one block per subset at a
+// time, runs of K template pixels per lane)
+int ensure_run_tables(gpv_context *ctx, int max_radius);
+int run_window_cap(int rmax, int K);
+int64_t run_scratch_floats(gpv_context *ctx, int rmax, int K, int *nslot);
+const void *run_kernel(int order, int nt, int K, bool per_subset);
+struct KArgs;
+int run_launch(gpv_context *ctx, int order, int nt, int K, int blocks, size_t smem, cudaStream_t s, const KArgs &k,
+               const int32_t *seg, int *queue, int win_cap, int nslot, uint32_t *slot_mask, int slots_per_sm,
+               int n_mask);
+// Run length of the run-layout kernel for subsets up to max_radius
+// (GPV_RUN_K, else a candidate being timed, else the tuned choice, else 8).
+int run_length_for(gpv_context *ctx, int max_radius);
 int solve_noalloc_launch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
                          int64_t n, int max_radius, const gpv_solve_params *prm, gpv_subset_result *out_dev,
                          cudaStream_t s);

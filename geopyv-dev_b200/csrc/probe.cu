@@ -69,10 +69,12 @@ __global__ void __launch_bounds__(kProbeThreads) dfma_probe(double *out, double 
     if (s == 1234.5) out[threadIdx.x] = s;
 }
 
-// Each thread reads float4s at a lane-consecutive index that advances by a
-// whole warp's span per step, so every warp request touches 512 contiguous
-// bytes (four wavefronts, no bank conflict).  The index wraps inside the
-// block's array with a mask (kSmemFloats / 4 float4s, a power of two).
+// Each thread reads float4s at lane-consecutive indices, so every warp
+// request touches 512 contiguous bytes (four wavefronts, no bank conflict).
+// The index advances by four blocks' spans plus one float4 per step and
+// wraps inside the block's array with a mask (kSmemFloats / 4 float4s, a
+// power of two): the address pattern repeats only after 512 steps, so no
+// load can be hoisted out of the loop.
 __global__ void __launch_bounds__(kProbeThreads) lds_probe(float *out) {
     __shared__ float4 buf[kSmemFloats / 4];
     for (int i = threadIdx.x; i < kSmemFloats / 4; i += kProbeThreads)
@@ -89,7 +91,7 @@ __global__ void __launch_bounds__(kProbeThreads) lds_probe(float *out) {
             const float4 v = buf[(idx + c * kProbeThreads) & kMask];
             acc[c].x += v.x; acc[c].y += v.y; acc[c].z += v.z; acc[c].w += v.w;
         }
-        idx = (idx + 4 * kProbeThreads) & kMask;
+        idx = (idx + 4 * kProbeThreads + 1) & kMask;
     }
     float s = 0.f;
 #pragma unroll

@@ -57,12 +57,16 @@ class Context:
         return lib().gpv_context_stream(self._h) or 0
 
     def tuning(self):
-        """Tuned (threads per block, template layout) per radius class r <= 20, 21-40, > 40."""
-        t = (ct.c_int32 * 3)()
-        lay = (ct.c_int32 * 3)()
-        check(lib().gpv_context_tuning(self._h, t, lay), "gpv_context_tuning")
+        """Tuned launch dimensions per radius class r <= 20, 21-40, > 40: a dict
+        per class (threads per block, tiled-kernel template layout, run length,
+        subsets per block, window staging; None where untuned)."""
+        from ._lib import Tuning
+        t = (Tuning * 3)()
+        check(lib().gpv_context_tuning_get(self._h, t), "gpv_context_tuning_get")
         names = {-1: None, 0: "compact", 1: "rows", 2: "tiles"}
-        return [(t[c] or None, names[lay[c]]) for c in range(3)]
+        return [{"threads": t[c].threads or None, "layout": names.get(t[c].layout), "run_length": t[c].run_length or None,
+                 "subsets_per_block": t[c].subsets_per_block or None, "staging": t[c].staging or None}
+                for c in range(3)]
 
     def reserve(self, n_subsets: int, max_radius: int, max_iterations: int = 50) -> None:
         check(lib().gpv_context_reserve(self._h, n_subsets, max_radius, max_iterations), "gpv_context_reserve")

@@ -87,6 +87,14 @@ class Peaks(ct.Structure):
 
 assert ct.sizeof(Peaks) == 40
 
+
+class Tuning(ct.Structure):
+    _fields_ = [("threads", ct.c_int32), ("layout", ct.c_int32), ("run_length", ct.c_int32),
+                ("subsets_per_block", ct.c_int32), ("staging", ct.c_int32), ("reserved", ct.c_int32)]
+
+
+assert ct.sizeof(Tuning) == 24
+
 REQUEST_REUSE_REFERENCE, REQUEST_SEED_FROM_PREVIOUS = 1, 2
 CONTEXT_HIGH_PRIORITY, CONTEXT_PER_SUBSET_BLOCKS = 1, 2
 
@@ -135,6 +143,7 @@ SIGNATURES = {
     "gpv_probe_peaks": (ct.c_int, [P, P]),
     "gpv_autotune": (ct.c_int, [P, P, P, P, I64, P, I32, P]),
     "gpv_context_tuning": (ct.c_int, [P, P, P]),
+    "gpv_context_tuning_get": (ct.c_int, [P, P]),
     "gpv_batch_graph_create": (ct.c_int, [P, P, P, P, P, I64, P, P, P]),
     "gpv_batch_graph_launch": (ct.c_int, [P, P]),
     "gpv_batch_graph_destroy": (ct.c_int, [P]),

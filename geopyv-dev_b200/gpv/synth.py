@@ -203,3 +203,22 @@ def workload(config: int, scale_down: int = 1, seed_frame: int = 0):
         raise ValueError("config must be 1..4 (config 5 is the serving stream)")
     truth = displacement(fld, xy)
     return dict(f=f, g=g, coords=xy, radius=radius, order=order, p0=p0, truth_uv=truth, field=fld, name=name)
+
+
+def sequence_frames(frames, scale_down: int = 1, every: int = 1):
+    """The incremental-sequence workload's frames 0, every, 2 every, ... below
+    `frames` (simple shear rising linearly to 5% at frame 200): the reference
+    speckle is rendered once and each target warps it, so the frames equal
+    workload(4, scale_down, seed_frame=k)["g"].  Returns (frame-0 workload,
+    list of target images)."""
+    W0 = workload(4, scale_down, seed_frame=0)
+    n = W0["f"].shape[0]
+    c = (n - 1) / 2.0
+    seed = 1000 * 4
+    r0 = speckle(n, n, seed, 1.0)
+    gs = []
+    for k in range(0, frames, every):
+        fld = make_field(xc=c, yc=c, a=(0.0, 0.05 * k / 200.0, 0.0, 0.0))
+        gs.append(quantize(warp(r0, fld), seed, 12, 2.0, np.uint8))
+    return W0, gs
+

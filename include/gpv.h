@@ -450,8 +450,10 @@ int gpv_server_destroy(gpv_server *s);
 
 /* ---- autotuning (no counterpart in the reference) ------------------------
  * Times the candidate launch shapes of the mixed-precision kernel (threads
- * per subset block: 128 or 256; template layout: compact scan order or 8 x 4
- * tiles) on a sample of up to sample_per_class subsets of each radius class
+ * per subset block: 128 or 256; template pixels per run of the run-layout
+ * kernel: 4 or 8 -- or, with GPV_SOLVE_KERNEL=tile, the tiled kernel's
+ * template layout: compact scan order or 8 x 4 tiles) on a sample of up to
+ * sample_per_class subsets of each radius class
  * (r <= 20, 21..40, > 40) present in desc, keeps the fastest per class in the
  * context, and returns the thread choices in threads_out[3] (0 = class
  * absent).  If the environment variable GPV_TUNE_CACHE names a file, the
@@ -462,6 +464,20 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
 /* The context's tuned choices per radius class: threads (0 = none) and
  * layout (-1 = none, 0 compact, 1 padded rows, 2 tiles); either may be NULL. */
 int gpv_context_tuning(gpv_context *ctx, int32_t *threads, int32_t *layouts);
+
+/* Every tuned launch dimension of one radius class (no counterpart in the
+ * reference).  0 / -1 = not tuned (the default applies). */
+typedef struct {
+    int32_t threads;            /* threads per block: 128 or 256                        */
+    int32_t layout;             /* tiled kernel's template layout (-1, 0, 1, 2)         */
+    int32_t run_length;         /* run-layout kernel: template pixels per run, 4 or 8   */
+    int32_t subsets_per_block;  /* subsets a block solves side by side (1 or 2)         */
+    int32_t staging;            /* coefficient-window buffers per subset (1 or 2)       */
+    int32_t reserved;
+} gpv_tuning;
+
+/* The context's tuning for radius classes r <= 20, 21-40, > 40 (out[3]). */
+int gpv_context_tuning_get(gpv_context *ctx, gpv_tuning *out);
 
 /* ---- calibration (no counterpart in the reference) ----------------------
  * Measured FP32 FMA throughput of this device (TFLOP/s, 2 FLOP per FMA) from

@@ -191,7 +191,8 @@ def test_autotune_choices_do_not_change_results(oracle, gpv_mod):
     choice = F.ctx.tuning()
     for c in range(3):
         if present[c]:  # an absent class keeps whatever the shared context held
-            assert choice[c][0] == tuned[c] and choice[c][1] in ("compact", "tiles")
+            assert choice[c]["threads"] == tuned[c] and choice[c]["layout"] in (None, "compact", "tiles")
+            assert choice[c]["run_length"] in (4, 8)
     import os
     res = {}
     for nt in ("128", "256"):
@@ -211,12 +212,13 @@ def test_autotune_choices_do_not_change_results(oracle, gpv_mod):
 @pytest.mark.parametrize("layout", ["rows", "tiles"])
 def test_template_layouts_match_the_oracle(gpv_mod, oracle, layout, monkeypatch):
     """The padded-row and 8 x 4 tile slot layouts of the tiled kernel (chosen
-    with GPV_TILE_LAYOUT) solve every subset like the compact one."""
+    with GPV_TILE_LAYOUT) solve every subset like its compact one."""
     from gpv import synth
     W = synth.workload(3, scale_down=8)
     d = gpv_mod.make_desc(W["coords"], W["radius"], W["order"], W["p0"])
     F = gpv_mod.Image(image_gs=W["f"], border=20)
     G = gpv_mod.Image(image_gs=W["g"], border=20)
+    monkeypatch.setenv("GPV_SOLVE_KERNEL", "tile")
     base = gpv_mod.solve_batch(F, G, d)
     monkeypatch.setenv("GPV_TILE_LAYOUT", layout)
     got = gpv_mod.solve_batch(F, G, d)
@@ -243,6 +245,7 @@ def test_tune_cache_file_is_read_back(gpv_mod, tmp_path, monkeypatch):
     monkeypatch.setenv("GPV_TUNE_CACHE", str(cache))
     ctx = gpv_mod.Context(0)
     try:
-        assert ctx.tuning() == [(128, None), (256, "tiles"), (None, None)]
+        got = [(t["threads"], t["layout"]) for t in ctx.tuning()]
+        assert got == [(128, None), (256, "tiles"), (None, None)]
     finally:
         ctx.close()

@@ -145,7 +145,9 @@ def test_rigid_falls_back_and_is_refused_where_unsupported(gpv_mod):
     with pytest.raises(ValueError):
         gpv_mod.solve_batch(F, G, d1, texture="grainy")
     # textured but too small to measure a correlation length (src/texture.rs:555-566):
-    # the deformable template, texture 0, the deformable solve's result
+    # the deformable template, texture 0, the deformable solve's result (the
+    # rigid-capable kernel and the default deformable kernel round their FP32
+    # sums differently: equal within the mixed-precision bar, same iterations)
     y, x = np.mgrid[0:14, 0:14].astype(np.float64)
     small = 100.0 + 40.0 * np.sin(0.9 * x) * np.cos(0.7 * y)
     R = gpv_mod.Image(image_gs=small, border=8)
@@ -153,7 +155,7 @@ def test_rigid_falls_back_and_is_refused_where_unsupported(gpv_mod):
     a = gpv_mod.solve_batch(R, R, dr, texture="rigid", tolerance=0.0, max_iterations=20)
     b = gpv_mod.solve_batch(R, R, dr, tolerance=0.0, max_iterations=20)
     assert not R.grain()["built"] and np.all(a["texture"] == 0)
-    assert np.abs(a["p"] - b["p"]).max() < 1e-9 and np.array_equal(a["iterations"], b["iterations"])
+    assert np.abs(a["p"] - b["p"]).max() < 1e-5 and np.array_equal(a["iterations"], b["iterations"])
 
 
 def test_rigid_mesh_solve(gpv_mod, oracle):
