@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--no-rigid", action="store_true", help="skip the rigid-texture leg")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form on the full batch")
     ap.add_argument("--no-c1", action="store_true", help="skip the first-order 1024^2 workload at full size")
+    ap.add_argument("--no-precision-ab", action="store_true", help="skip the precision-form comparison")
     ap.add_argument("--sequence-frames", type=int, default=200, help="frames of the sequence leg")
     ap.add_argument("--serving-seconds", type=float, default=10.0)
     return ap.parse_args()
@@ -479,6 +480,65 @@ def fp64_leg(W, device, mixed_solve_ms, steps=3):
             "mixed_solve_ms": mixed_solve_ms, "mixed_over_fp64": ms / mixed_solve_ms,
             "iterations_mean": float(res["iterations"].mean()), "converged_frac": float(res["converged"].mean()),
             "timing": "CUDA events on the library stream, device-resident inputs, solve only (both forms)"}
+
+
+def precision_leg(ctx, F, G, desc, sample_idx, sample_ref, steps=3):
+    """The headline batch solved by three precision forms, device-resident,
+    each timed with CUDA events and compared with the same oracle sample:
+    the tiled kernel (FP32 sums over at most 8 pixels then FP64; Gauss-Jordan
+    inverse of the scaled Hessian), the run-layout kernel (FP32 sums over each
+    run then FP64; Cholesky factor, substitution solve) and the run-layout
+    kernel with Kahan-compensated FP64 ZNSSD sums (GPV_SOLVE_KAHAN)."""
+    import ctypes as ct
+
+    import torch
+
+    import gpv
+    from gpv import _lib
+    n = len(desc)
+    d_dev = torch.from_numpy(desc.view(np.uint8).copy()).cuda()
+    out_dev = torch.zeros(n * _lib.RESULT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    L = _lib.lib()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    forms = {"tile_chunked_fp32_gauss_jordan": ("tile", 0), "runs_fp32_per_run_cholesky": ("runs", 0),
+             "runs_kahan_fp64_cholesky": ("runs", _lib.SOLVE_KAHAN)}
+    out = {}
+    saved = os.environ.get("GPV_SOLVE_KERNEL")
+    try:
+        for name, (kern, flags) in forms.items():
+            os.environ["GPV_SOLVE_KERNEL"] = kern
+            prm = _lib.SolveParams(max_norm=1e-5, tolerance=0.75, max_iterations=50, flags=flags,
+                                   precision=gpv.PREC_MIXED, reserved=0, mask=None, history=None)
+            args = (ctx.handle, F.handle, G.handle, ct.c_void_p(d_dev.data_ptr()), None, n, ct.byref(prm),
+                    ct.c_void_p(out_dev.data_ptr()), None)
+            _lib.check(L.gpv_solve_batch_device(*args), name)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                _lib.check(L.gpv_solve_batch_device(*args), name)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            res = np.frombuffer(out_dev.cpu().numpy().tobytes(), dtype=_lib.RESULT_DTYPE).copy()
+            entry = {"solve_ms": e0.elapsed_time(e1) / steps, "iterations_mean": float(res["iterations"].mean())}
+            if sample_idx is not None:
+                ok = (sample_ref["status"] == 0) & (sample_ref["converged"] == 1)
+                r = res[sample_idx]
+                entry.update({
+                    "max_disp_err_px": float(np.abs(r["p"][ok, :2] - sample_ref["p"][ok, :2]).max()),
+                    "max_strain_err": float(np.abs(r["p"][ok, 2:6] - sample_ref["p"][ok, 2:6]).max()),
+                    "flag_agreement": float(np.mean((r["converged"] == sample_ref["converged"]) &
+                                                    (r["quality_ok"] == sample_ref["quality_ok"]))),
+                    "iteration_agreement": float(np.mean(r["iterations"] == sample_ref["iterations"]))})
+            out[name] = entry
+    finally:
+        if saved is None:
+            os.environ.pop("GPV_SOLVE_KERNEL", None)
+        else:
+            os.environ["GPV_SOLVE_KERNEL"] = saved
+    out["oracle_sample"] = int(len(sample_idx)) if sample_idx is not None else 0
+    out["timing"] = "CUDA events on the library stream, device-resident inputs, solve only"
+    return out
 
 
 def c1_leg(device, steps=10):
@@ -993,6 +1053,9 @@ def run_ours(args, world, rank, local):
     rigid = None
     if not args.no_rigid and args.config == 2 and args.scale_down == 1 and prec == gpv.PREC_MIXED:
         rigid = rigid_leg(W, local)
+    prec_ab = None
+    if not args.no_precision_ab and args.config == 2 and prec == gpv.PREC_MIXED:
+        prec_ab = precision_leg(ctx, F, G, desc, cpu["sample_idx"] if cpu else None, cpu["sample_res"] if cpu else None)
     fp64 = None
     if not args.no_fp64 and args.config == 2 and prec == gpv.PREC_MIXED:
         fp64 = fp64_leg(W, local, float(np.mean(solve_ms)))
@@ -1064,6 +1127,8 @@ def run_ours(args, world, rank, local):
         line["uneven_batch"] = uneven
     if rigid is not None:
         line["rigid_texture"] = rigid
+    if prec_ab is not None:
+        line["precision_forms"] = prec_ab
     if fp64 is not None:
         line["fp64_plain"] = fp64
         line["fp64_plain_subsets_per_s"] = fp64["fp64_plain_subsets_per_s"]

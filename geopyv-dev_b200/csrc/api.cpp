@@ -1030,7 +1030,7 @@ static void tune_cache_load(gpv_context *ctx) {
         char name[256];
         int cls = -1, nt = 0, layout = -1, runk = 0;
         const int got = sscanf(line, "%255[^|]|%d|%d|%d|%d", name, &cls, &nt, &layout, &runk);
-        if (got >= 3 && cls >= 0 && cls < 3 && strcmp(name, prop.name) == 0 && (nt == 128 || nt == 256)) {
+        if (got >= 3 && cls >= 0 && cls < 3 && strcmp(name, prop.name) == 0 && (nt == 64 || nt == 128 || nt == 256)) {
             ctx->tuned_threads[cls] = nt;  // later lines win
             ctx->tuned_layout[cls] = (got >= 4 && layout >= 0 && layout <= 2) ? layout : -1;
             ctx->tuned_run_k[cls] = (got == 5 && (runk == 4 || runk == 8)) ? runk : 0;
@@ -1057,9 +1057,10 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
     // threads per block x template layout (compact, 8 x 4 tiles) when the
     // tiled kernel is selected
     const bool runs = use_run_kernel();
-    static const int cand_runs[4][2] = {{128, 8}, {256, 8}, {128, 4}, {256, 4}};
+    static const int cand_runs[6][2] = {{128, 8}, {256, 8}, {128, 4}, {256, 4}, {64, 4}, {64, 8}};
     static const int cand_tile[4][2] = {{128, 0}, {256, 0}, {128, 2}, {256, 2}};
     const int(*cand)[2] = runs ? cand_runs : cand_tile;
+    const int ncand = runs ? 6 : 4;
     for (int c = 0; c < 3; c++) {
         if (threads_out) threads_out[c] = 0;
         if (cls[c].empty()) continue;
@@ -1070,7 +1071,7 @@ int gpv_autotune(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const
         std::vector<gpv_subset_result> out(smp.size());
         double best = 1e300;
         int best_nt = 128, best_layout = 0, best_k = 0;
-        for (int ci = 0; ci < 4; ci++) {
+        for (int ci = 0; ci < ncand; ci++) {
             const int *cd = cand[ci];
             const int t = cd[0];
             ctx->force_threads = t;

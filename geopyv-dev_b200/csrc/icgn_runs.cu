@@ -50,7 +50,7 @@
 namespace gpv {
 namespace {
 
-constexpr int kRunMaxWarps = 8;  // blocks of 128 or 256 threads
+constexpr int kRunMaxWarps = 8;  // blocks of 64, 128 or 256 threads
 constexpr int kRunMargin = 4;
 constexpr int kRunLengths[2] = {4, 8};  // run lengths K with task tables
 
@@ -92,9 +92,16 @@ __host__ __device__ __forceinline__ int run_pitch(int ww) { return (ww + 31) & ~
 
 // Copy coefficient rows [r0, r0+wh) x cols [c0, c0+ww) (c0, ww multiples of
 // 4) into win with row pitch `pitch`; out-of-range rows / columns clamped.
+// Threads [t0, NT) issue asynchronous 16-byte global-to-shared copies
+// (cp.async, no registers held for the data), so all of a thread's copies
+// are in flight at once; each thread waits for its own copies before it
+// returns, and the caller's block barrier publishes the window.  Both
+// addresses are 16-byte aligned: coefficient rows are a multiple of 32 floats
+// apart, c0 and the clamped columns are multiples of 4, and the window's
+// pitch is a multiple of 32 floats.
 template <int NT>
 __device__ __forceinline__ void run_stage(const float *__restrict__ C, int64_t cpitch, int ch, int r0, int c0, int wh,
-                                          int ww, int pitch, float *win, int t0 = 0) {
+                                          int ww, int pitch, float *win, int t0) {
     const int nv = ww >> 2;
     for (int idx = (int)threadIdx.x - t0; idx < wh * nv; idx += NT - t0) {
         const int rr = idx / nv, cc = (idx - rr * nv) << 2;
@@ -102,9 +109,11 @@ __device__ __forceinline__ void run_stage(const float *__restrict__ C, int64_t c
         row = row < 0 ? 0 : (row > ch - 1 ? ch - 1 : row);
         int col = c0 + cc;
         col = col < 0 ? 0 : (col > (int)cpitch - 4 ? (int)cpitch - 4 : col);
-        const float4 v = __ldg(reinterpret_cast<const float4 *>(C + (int64_t)row * cpitch + col));
-        *reinterpret_cast<float4 *>(win + rr * pitch + cc) = v;
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(win + rr * pitch + cc);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(C + (int64_t)row * cpitch + col)
+                     : "memory");
     }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 // A window covering pixel indices [xlo, xhi] x [ylo, yhi] (clamped to the
@@ -290,14 +299,36 @@ struct RunAcc {
     float2 m0, m1, m2;  // sum G, sum G dy, sum G dy^2 with G = (gx, gy) (g - f_m)
 };
 
-template <int ORDER>
-__device__ __forceinline__ void acc_sample(RunAcc &a, bool valid, float g, float fmf, float f, float gx, float gy,
-                                           float dyf) {
-    const float gc = valid ? g - fmf : 0.f;
-    a.p1 += gc;
-    a.p2 = fmaf(gc, gc, a.p2);
-    a.pfg = fmaf(f - fmf, gc, a.pfg);
-    const float gxc = gx * gc, gyc = gy * gc;
+// A Kahan-compensated FP64 sum: add() carries the rounding error of each
+// addition into the next one.
+struct KSum {
+    double s = 0.0, c = 0.0;
+    __device__ __forceinline__ void add(double x) {
+        const double y = x - c, t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
+// One sample: rec = (f - s, df/dx, df/dy, w) with w = 1 for template
+// pixels, 0 outside; pfg sums (f - s)(g - f_m) (corrected to f - f_m with
+// the block totals).  KAHAN: the three ZNSSD sums (g - f_m, its square and
+// the cross term) go straight into the thread's compensated FP64 sums ks
+// instead of the run's FP32 partials.
+template <int ORDER, bool KAHAN>
+__device__ __forceinline__ void acc_sample(RunAcc &a, KSum (&ks)[3], float4 rec, float g, float fmf, float dyf) {
+    const float gc = (g - fmf) * rec.w;
+    if (KAHAN) {
+        const double gd = (double)gc;
+        ks[0].add(gd);
+        ks[1].add(gd * gd);
+        ks[2].add((double)rec.x * gd);
+    } else {
+        a.p1 += gc;
+        a.p2 = fmaf(gc, gc, a.p2);
+        a.pfg = fmaf(rec.x, gc, a.pfg);
+    }
+    const float gxc = rec.y * gc, gyc = rec.z * gc;
     a.m0.x += gxc;
     a.m0.y += gyc;
     if (ORDER >= 1) {
@@ -333,7 +364,7 @@ __device__ __forceinline__ void unpack_task(int2 tk, int &dx, int &dy0) {
     dy0 = tk.x >> 16;
 }
 
-template <int ORDER, int NT, int K>
+template <int ORDER, int NT, int K, bool KAHAN>
 __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, float *base, float *win, RunSmem &sm) {
     const KArgs &A = R.k;
     using O = Ord<ORDER>;
@@ -344,8 +375,11 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
     const int T = R.task_n[r];
     const int2 *tasks = R.tasks + R.task_off[r];
     const int NS = T * K;
-    float *RF = base, *RGX = base + R.nslot, *RGY = base + 2 * R.nslot, *RSG = base + 3 * R.nslot;
-    int *RVM = reinterpret_cast<int *>(base + 4 * R.nslot);
+    // per-pixel records (f - s, df/dx, df/dy, 1 in the template / 0 outside:
+    // zero gradients outside) in slot j * T + t of run t; eta resamples; run bits
+    float4 *REC = reinterpret_cast<float4 *>(base);
+    float *RSG = base + 4 * R.nslot;
+    int *RVM = reinterpret_cast<int *>(base + 5 * R.nslot);
     const double cx = d.coord[0], cy = d.coord[1];
     const int cxi = (int)cx, cyi = (int)cy;
     const double fxd = floor(cx), fyd = floor(cy);
@@ -360,7 +394,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
         const int ylo = max(0, min(by - re - 1, A.h - 1)), yhi = max(0, min(by + re + 1, A.h - 1));
         int r0, c0, wh, ww, pitch;
         const bool ok = run_plan(xlo, xhi, ylo, yhi, B, R.win_cap, r0, c0, wh, ww, pitch);
-        if (ok) run_stage<NT>(A.f32, A.pitch32, ch, r0, c0, wh, ww, pitch, win);
+        if (ok) run_stage<NT>(A.f32, A.pitch32, ch, r0, c0, wh, ww, pitch, win, 0);
         if (tid == 0) {
             sm.win_ok = 0;  // g must be staged before the iterations
             sm.win_r0 = r0; sm.win_c0 = c0; sm.win_h = wh; sm.win_w = ww; sm.win_p = pitch;
@@ -469,9 +503,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
                         vy = fmaf(da0[rr], s[j + rr], vy);
                     }
                     const bool v = (vm >> j) & 1u;
-                    RF[j * T + t] = val;
-                    RGX[j * T + t] = v ? vx : 0.f;
-                    RGY[j * T + t] = v ? vy : 0.f;
+                    REC[j * T + t] = v ? make_float4(val - shift, vx, vy, 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
                     pix1(v, val, vx, vy, dx, dy0 + j);
                 }
             } else {
@@ -492,9 +524,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
                         const float *F = A.f32 + (int64_t)(iy + B - 2) * A.pitch32 + (ix + B - 2);
                         f = contract_grad<float>(F, A.pitch32, a, da, b, db, gx, gy);
                     }
-                    RF[j * T + t] = f;
-                    RGX[j * T + t] = v ? gx : 0.f;
-                    RGY[j * T + t] = v ? gy : 0.f;
+                    REC[j * T + t] = v ? make_float4(f - shift, gx, gy, 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
                     pix1(v, f, gx, gy, dx, dy0 + j);
                 }
             }
@@ -518,7 +548,8 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
                 for (int b = 0; b < NB; b++) V[p][b] = 0.f;
 #pragma unroll
             for (int j = 0; j < K; j++) {
-                const float gx = RGX[j * T + t], gy = RGY[j * T + t];  // zero for pixels outside the template
+                const float4 rec = REC[j * T + t];
+                const float gx = rec.y, gy = rec.z;  // zero for pixels outside the template
                 const float gg[3] = {gx * gx, gx * gy, gy * gy};
                 const float dyf = (float)(dy0 + j);
                 float pw = 1.f;
@@ -633,7 +664,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
                 int r0, c0, wh, ww, pitch;
                 const bool ok = run_plan(xlo, xhi, ylo, yhi, B, R.win_cap, r0, c0, wh, ww, pitch);
                 __syncthreads();  // nobody still reads the old window
-                if (ok) run_stage<NT>(A.g32, A.pitch32, ch, r0, c0, wh, ww, pitch, win);
+                if (ok) run_stage<NT>(A.g32, A.pitch32, ch, r0, c0, wh, ww, pitch, win, 0);
                 if (tid == 0) {
                     sm.win_ok = ok;
                     sm.win_r0 = r0; sm.win_c0 = c0; sm.win_h = wh; sm.win_w = ww; sm.win_p = pitch;
@@ -665,13 +696,13 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
         const float2 O2 = make_float2(oy, ox), U1 = make_float2(vx, ux), U2 = make_float2(vy, uy);
         const float2 Q1 = make_float2(vxx, uxx), Q2 = make_float2(vxy, uxy), C2 = make_float2(vyy, uyy);
         double s1 = 0.0, s2 = 0.0, sfg = 0.0;
+        KSum ks[3];
         float2 PB[6];
 #pragma unroll
         for (int k = 0; k < 6; k++) PB[k] = make_float2(0.f, 0.f);
         for (int t = tid; t < T; t += NT) {
             int dx, dy0;
             unpack_task(tasks[t], dx, dy0);
-            const uint32_t vm = (uint32_t)RVM[t];
             const float dxf = (float)dx;
             float2 A2 = O2, B2 = make_float2(0.f, 0.f);
             if (ORDER >= 1) {
@@ -727,7 +758,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
                     for (int rr = 0; rr < 6; rr++) sr[rr] = row_dot(Rg[(j + rr) % 6], Bw);
                     const float g = combine6(sr, Aw);
                     const int sl = j * T + t;
-                    acc_sample<ORDER>(ac, (vm >> j) & 1u, g, fmf, RF[sl], RGX[sl], RGY[sl], dyf);
+                    acc_sample<ORDER, KAHAN>(ac, ks, REC[sl], g, fmf, dyf);
                 }
             } else {
                 for (int j = 0; j < K; j++) {
@@ -750,12 +781,14 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
                         g = contract<float>(A.g32 + (int64_t)(iy + B - 2) * A.pitch32 + (ix + B - 2), A.pitch32, a, b);
                     }
                     const int sl = j * T + t;
-                    acc_sample<ORDER>(ac, (vm >> j) & 1u, g, fmf, RF[sl], RGX[sl], RGY[sl], dyf);
+                    acc_sample<ORDER, KAHAN>(ac, ks, REC[sl], g, fmf, dyf);
                 }
             }
-            s1 += (double)ac.p1;
-            s2 += (double)ac.p2;
-            sfg += (double)ac.pfg;
+            if (!KAHAN) {
+                s1 += (double)ac.p1;
+                s2 += (double)ac.p2;
+                sfg += (double)ac.pfg;
+            }
             acc_expand<ORDER>(ac, dxf, PB);
         }
         // block sums: warp partials to shared memory, one barrier, then warp 0
@@ -763,6 +796,11 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
         constexpr int KR = 3 + M;
         {
             double v[KR];
+            if (KAHAN) {
+                s1 = ks[0].s;
+                s2 = ks[1].s;
+                sfg = ks[2].s;
+            }
             v[0] = s1; v[1] = s2; v[2] = sfg;
 #pragma unroll
             for (int j = 0; j < M / 2; j++) {
@@ -783,7 +821,9 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
             const double gmt = t0 / dn;
             const double dg2 = t1 - t0 * gmt;
             const double dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
-            const double sab = t2;  // sum (f - f_m)(g - g_m) = sum (f - f_m)(g - f_m): sum (f - f_m) = 0
+            // sum (f - f_m)(g - g_m) = sum (f - f_m)(g - f_m) (sum (f - f_m) = 0)
+            //                     = sum (f - s)(g - f_m) - (f_m - s) sum (g - f_m)
+            const double sab = t2 - (fm - (double)shift) * t0;
             const double znssd = 2.0 - 2.0 * sab / (df * dg);
             const double ratio = df / dg;
             // lane j < M: grad_j = A_j - (df/dg)(B_j - g~_m S_j); B_j sits at lane 3 + j
@@ -879,7 +919,9 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
             if (!((RVM[t] >> j) & 1)) return false;
             int dxi, dy0;
             unpack_task(tasks[t], dxi, dy0);
-            f = RF[i]; gx = RGX[i]; gy = RGY[i]; g = RSG[i];
+            const float4 rec = REC[i];
+            f = (double)rec.x + (double)shift;
+            gx = rec.y; gy = rec.z; g = RSG[i];
             dx = dxi; dy = dy0 + j;
             return true;
         };
@@ -932,7 +974,7 @@ __device__ int run_claim_slot(const RunArgs &R) {
 // PER_SUBSET: one block per subset with a claimed scratch slot (subsets
 // free SMs one at a time, for callers sharing the GPU); else a persistent
 // grid whose blocks take subsets of their segment from the queue.
-template <int ORDER, int NT, int K, bool PER_SUBSET>
+template <int ORDER, int NT, int K, bool PER_SUBSET, bool KAHAN>
 __global__ void __launch_bounds__(NT, 512 / NT) icgn_runs(RunArgs R) {
     extern __shared__ float4 win4[];
     float *win = reinterpret_cast<float *>(win4);
@@ -956,7 +998,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) icgn_runs(RunArgs R) {
         if (d.radius < 1 || d.radius > A.max_radius) {
             if (threadIdx.x == 0) write_failed(A, idx, d, 12, GPV_INVALID_SUBSET, 0, 0.0, 0.0);
         } else {
-            run_subset<ORDER, NT, K>(R, idx, d, base, win, sm);
+            run_subset<ORDER, NT, K, KAHAN>(R, idx, d, base, win, sm);
         }
         __threadfence();  // every scratch access of the block is done before the slot is free
         __syncthreads();
@@ -979,32 +1021,54 @@ __global__ void __launch_bounds__(NT, 512 / NT) icgn_runs(RunArgs R) {
             if (threadIdx.x == 0) write_failed(A, idx, d, 12, GPV_INVALID_SUBSET, 0, 0.0, 0.0);
             continue;
         }
-        run_subset<ORDER, NT, K>(R, idx, d, base, win, sm);
+        run_subset<ORDER, NT, K, KAHAN>(R, idx, d, base, win, sm);
     }
 }
 
-template <int NT, int K, bool PS>
+template <int NT, int K, bool PS, bool KH>
 const void *run_kernel_t(int order) {
-    return order == 2 ? (const void *)icgn_runs<2, NT, K, PS>
-                      : (order == 1 ? (const void *)icgn_runs<1, NT, K, PS> : (const void *)icgn_runs<0, NT, K, PS>);
+    return order == 2 ? (const void *)icgn_runs<2, NT, K, PS, KH>
+                      : (order == 1 ? (const void *)icgn_runs<1, NT, K, PS, KH> : (const void *)icgn_runs<0, NT, K, PS, KH>);
 }
 
-template <int NT, int K, bool PS>
+template <int NT, int K, bool PS, bool KH>
 void run_launch_t(int order, int blocks, size_t smem, cudaStream_t s, const RunArgs &R) {
-    if (order == 2) icgn_runs<2, NT, K, PS><<<blocks, NT, smem, s>>>(R);
-    else if (order == 1) icgn_runs<1, NT, K, PS><<<blocks, NT, smem, s>>>(R);
-    else icgn_runs<0, NT, K, PS><<<blocks, NT, smem, s>>>(R);
+    if (order == 2) icgn_runs<2, NT, K, PS, KH><<<blocks, NT, smem, s>>>(R);
+    else if (order == 1) icgn_runs<1, NT, K, PS, KH><<<blocks, NT, smem, s>>>(R);
+    else icgn_runs<0, NT, K, PS, KH><<<blocks, NT, smem, s>>>(R);
 }
 
-template <int NT, bool PS>
+template <int NT, bool PS, bool KH>
 const void *run_kernel_k(int order, int K) {
-    return K == 4 ? run_kernel_t<NT, 4, PS>(order) : run_kernel_t<NT, 8, PS>(order);
+    return K == 4 ? run_kernel_t<NT, 4, PS, KH>(order) : run_kernel_t<NT, 8, PS, KH>(order);
 }
 
-template <int NT, bool PS>
+template <int NT, bool PS, bool KH>
 void run_launch_k(int order, int K, int blocks, size_t smem, cudaStream_t s, const RunArgs &R) {
-    if (K == 4) run_launch_t<NT, 4, PS>(order, blocks, smem, s, R);
-    else run_launch_t<NT, 8, PS>(order, blocks, smem, s, R);
+    if (K == 4) run_launch_t<NT, 4, PS, KH>(order, blocks, smem, s, R);
+    else run_launch_t<NT, 8, PS, KH>(order, blocks, smem, s, R);
+}
+
+// Instantiations: every (threads, run length, one block per subset); the
+// compensated-sum form on persistent grids of 128 or 256 threads only.
+template <int NT>
+const void *run_kernel_nt(int order, int K, bool ps, bool kahan) {
+    if constexpr (NT >= 128) {
+        if (kahan) return run_kernel_k<NT, false, true>(order, K);
+    }
+    return ps ? run_kernel_k<NT, true, false>(order, K) : run_kernel_k<NT, false, false>(order, K);
+}
+
+template <int NT>
+void run_launch_nt(int order, int K, bool ps, bool kahan, int blocks, size_t smem, cudaStream_t s, const RunArgs &R) {
+    if constexpr (NT >= 128) {
+        if (kahan) {
+            run_launch_k<NT, false, true>(order, K, blocks, smem, s, R);
+            return;
+        }
+    }
+    if (ps) run_launch_k<NT, true, false>(order, K, blocks, smem, s, R);
+    else run_launch_k<NT, false, false>(order, K, blocks, smem, s, R);
 }
 
 }  // namespace
@@ -1078,25 +1142,25 @@ int run_window_cap(int rmax, int K) {
 }
 
 // Record slots per block (largest radius's tasks x K, rounded to 32) and the
-// scratch floats per block: f, df/dx, df/dy, eta resample per slot + one
-// validity word per task.
+// scratch floats per block: a float4 record and an eta resample per slot +
+// one validity word per task.
 int64_t run_scratch_floats(gpv_context *ctx, int rmax, int K, int *nslot) {
     const int R1 = ctx->run_table_radius + 1;
     int T = 0;  // the most tasks of any radius up to rmax (the count is not monotone in r)
     for (int r = 1; r <= rmax; r++) T = std::max(T, (int)ctx->h_run_n[run_length_index(K) * R1 + r]);
     const int ns = (T * K + 31) / 32 * 32;
     *nslot = ns;
-    return 4 * (int64_t)ns + (T + 31) / 32 * 32;
+    return 5 * (int64_t)ns + (T + 31) / 32 * 32;
 }
 
-const void *run_kernel(int order, int nt, int K, bool per_subset) {
-    if (nt == 256) return per_subset ? run_kernel_k<256, true>(order, K) : run_kernel_k<256, false>(order, K);
-    return per_subset ? run_kernel_k<128, true>(order, K) : run_kernel_k<128, false>(order, K);
+const void *run_kernel(int order, int nt, int K, bool per_subset, bool kahan) {
+    if (nt == 64) return run_kernel_nt<64>(order, K, per_subset, kahan);
+    return nt == 256 ? run_kernel_nt<256>(order, K, per_subset, kahan) : run_kernel_nt<128>(order, K, per_subset, kahan);
 }
 
-int run_launch(gpv_context *ctx, int order, int nt, int K, int blocks, size_t smem, cudaStream_t s, const KArgs &k,
-               const int32_t *seg, int *queue, int win_cap, int nslot, uint32_t *slot_mask, int slots_per_sm,
-               int n_mask) {
+int run_launch(gpv_context *ctx, int order, int nt, int K, bool kahan, int blocks, size_t smem, cudaStream_t s,
+               const KArgs &k, const int32_t *seg, int *queue, int win_cap, int nslot, uint32_t *slot_mask,
+               int slots_per_sm, int n_mask) {
     RunArgs R;
     R.k = k;
     const int R1 = ctx->run_table_radius + 1, kk = run_length_index(K);
@@ -1111,13 +1175,13 @@ int run_launch(gpv_context *ctx, int order, int nt, int K, int blocks, size_t sm
     R.slots_per_sm = slots_per_sm;
     R.n_mask = n_mask;
     const bool ps = slot_mask != nullptr;
-    if (nt == 256) {
-        if (ps) run_launch_k<256, true>(order, K, blocks, smem, s, R);
-        else run_launch_k<256, false>(order, K, blocks, smem, s, R);
-    } else {
-        if (ps) run_launch_k<128, true>(order, K, blocks, smem, s, R);
-        else run_launch_k<128, false>(order, K, blocks, smem, s, R);
+    if (kahan && (ps || nt == 64)) {
+        set_error("the compensated-sum form runs on persistent grids of 128 or 256 threads");
+        return GPV_ERR_INVALID;
     }
+    if (nt == 64) run_launch_nt<64>(order, K, ps, kahan, blocks, smem, s, R);
+    else if (nt == 256) run_launch_nt<256>(order, K, ps, kahan, blocks, smem, s, R);
+    else run_launch_nt<128>(order, K, ps, kahan, blocks, smem, s, R);
     GPV_CUDA_TRY(cudaGetLastError());
     return GPV_SUCCESS;
 }

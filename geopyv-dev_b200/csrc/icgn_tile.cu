@@ -1327,13 +1327,19 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         P.layout = tile_layout_for(ctx, P.rmax);
         // persistent deformable segments run the run-layout kernel unless
         // GPV_SOLVE_KERNEL=tile asks for the tiled one
-        P.runs = !P.rigid && use_run_kernel();
+        // GPV_SOLVE_KAHAN (compensated FP64 ZNSSD sums): run-layout
+        // kernel on a persistent grid
+        const bool kahan = (K.flags & GPV_SOLVE_KAHAN) != 0;
+        P.runs = !P.rigid && (use_run_kernel() || kahan);
+        if (kahan) P.ps = false;
         if (P.runs) {
             P.run_k = run_length_for(ctx, P.rmax);
             if (int rc = ensure_run_tables(ctx, K.max_radius)) return rc;
         }
         P.cap = P.runs ? run_window_cap(P.rmax, P.run_k) : window_cap(P.rmax, P.layout);
-        const void *fn = P.runs ? run_kernel(order, P.nt, P.run_k, P.ps) : tile_kernel(P.nt, P.ps, order, P.rigid);
+        // 64-thread blocks exist for the run-layout kernel (not its compensated form) only
+        if (P.nt == 64 && (!P.runs || kahan)) P.nt = 128;
+        const void *fn = P.runs ? run_kernel(order, P.nt, P.run_k, P.ps, kahan) : tile_kernel(P.nt, P.ps, order, P.rigid);
         int max_bytes = 0;
         if (int rc = allow_max_dynamic_smem(fn, &max_bytes)) return rc;
         // a window larger than the block can hold is not staged: those
@@ -1391,8 +1397,9 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         T.n_mask = ctx->n_smid;
         const size_t smem = sizeof(float) * P.cap;
         if (P.runs) {
-            if (int rc = run_launch(ctx, 2 - q / kRClasses, P.nt, P.run_k, P.blocks, smem, st[k], T.k, T.seg, T.queue,
-                                    P.cap, P.nslot, T.slot_mask, T.slots_per_sm, T.n_mask))
+            if (int rc = run_launch(ctx, 2 - q / kRClasses, P.nt, P.run_k, (K.flags & GPV_SOLVE_KAHAN) != 0, P.blocks,
+                                    smem, st[k], T.k, T.seg, T.queue, P.cap, P.nslot, T.slot_mask, T.slots_per_sm,
+                                    T.n_mask))
                 return rc;
         } else {
             tile_launch_one(P.nt, P.ps, 2 - q / kRClasses, P.rigid, P.blocks, smem, st[k], T);
@@ -1436,7 +1443,10 @@ int run_length_for(gpv_context *ctx, int max_radius) {
 
 int tile_threads_for(gpv_context *ctx, int max_radius) {
     if (ctx->force_threads) return ctx->force_threads;
-    if (const char *v = getenv("GPV_TILE_THREADS")) return atoi(v) == 256 ? 256 : 128;
+    if (const char *v = getenv("GPV_TILE_THREADS")) {
+        const int t = atoi(v);
+        return t == 256 ? 256 : (t == 64 ? 64 : 128);
+    }
     const int cls = max_radius <= 20 ? 0 : (max_radius <= 40 ? 1 : 2);
     if (ctx->tuned_threads[cls]) return ctx->tuned_threads[cls];
     return max_radius > 40 ? 256 : 128;

@@ -203,11 +203,11 @@ int query_nsmid(int *out);
 int ensure_run_tables(gpv_context *ctx, int max_radius);
 int run_window_cap(int rmax, int K);
 int64_t run_scratch_floats(gpv_context *ctx, int rmax, int K, int *nslot);
-const void *run_kernel(int order, int nt, int K, bool per_subset);
+const void *run_kernel(int order, int nt, int K, bool per_subset, bool kahan);
 struct KArgs;
-int run_launch(gpv_context *ctx, int order, int nt, int K, int blocks, size_t smem, cudaStream_t s, const KArgs &k,
-               const int32_t *seg, int *queue, int win_cap, int nslot, uint32_t *slot_mask, int slots_per_sm,
-               int n_mask);
+int run_launch(gpv_context *ctx, int order, int nt, int K, bool kahan, int blocks, size_t smem, cudaStream_t s,
+               const KArgs &k, const int32_t *seg, int *queue, int win_cap, int nslot, uint32_t *slot_mask,
+               int slots_per_sm, int n_mask);
 // Run length of the run-layout kernel for subsets up to max_radius
 // (GPV_RUN_K, else a candidate being timed, else the tuned choice, else 8).
 int run_length_for(gpv_context *ctx, int max_radius);

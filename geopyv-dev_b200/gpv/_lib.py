@@ -101,7 +101,7 @@ CONTEXT_HIGH_PRIORITY, CONTEXT_PER_SUBSET_BLOCKS = 1, 2
 # enums
 GPV_U8, GPV_U16, GPV_F32, GPV_F64 = 1, 2, 3, 4
 PREC_MIXED, PREC_FP64 = 0, 1
-SOLVE_ETA, SOLVE_HISTORY, SOLVE_FAGN, SOLVE_RIGID_TEXTURE = 1, 2, 4, 8
+SOLVE_ETA, SOLVE_HISTORY, SOLVE_FAGN, SOLVE_RIGID_TEXTURE, SOLVE_KAHAN = 1, 2, 4, 8, 16
 IMAGE_KEEP_F64, IMAGE_GRAIN = 1, 2
 STATUS = {0: "OK", 1: "EMPTY_MASK", 2: "FEATURELESS", 3: "SINGULAR_H", 4: "SINGULAR_WDELTA", 5: "NONFINITE",
           6: "TIMEOUT", 7: "CANCELLED", 8: "INVALID_SUBSET"}

@@ -64,6 +64,12 @@ typedef enum {
                                 (solve_fagn_result, src/subset.rs:1228-1334);
                                 FP64 arithmetic in either precision mode, on the
                                 FP64 coefficients when precision is FP64     */
+#define GPV_SOLVE_KAHAN 16u  /* mixed precision: accumulate the ZNSSD sums
+                                (g - g_m, its square, the cross term with
+                                f - f_m) per sample in Kahan-compensated FP64
+                                instead of FP32 over each run of template
+                                pixels (no counterpart in the reference: its
+                                sums are plain FP64, src/subset.rs:418-446) */
 #define GPV_SOLVE_RIGID_TEXTURE 8u /* Texture::Rigid (src/texture.rs,
                                 src/subset.rs:1062-1097, 1151-1168): fit g to the
                                 template f + G(E(p)) rebuilt every iteration
@@ -450,8 +456,9 @@ int gpv_server_destroy(gpv_server *s);
 
 /* ---- autotuning (no counterpart in the reference) ------------------------
  * Times the candidate launch shapes of the mixed-precision kernel (threads
- * per subset block: 128 or 256; template pixels per run of the run-layout
- * kernel: 4 or 8 -- or, with GPV_SOLVE_KERNEL=tile, the tiled kernel's
+ * per subset block: 64, 128 or 256; template pixels per run of the
+ * run-layout kernel: 4 or 8 -- or, with GPV_SOLVE_KERNEL=tile, 128 or 256
+ * threads and the tiled kernel's
  * template layout: compact scan order or 8 x 4 tiles) on a sample of up to
  * sample_per_class subsets of each radius class
  * (r <= 20, 21..40, > 40) present in desc, keeps the fastest per class in the
@@ -468,7 +475,7 @@ int gpv_context_tuning(gpv_context *ctx, int32_t *threads, int32_t *layouts);
 /* Every tuned launch dimension of one radius class (no counterpart in the
  * reference).  0 / -1 = not tuned (the default applies). */
 typedef struct {
-    int32_t threads;            /* threads per block: 128 or 256                        */
+    int32_t threads;            /* threads per block: 64, 128 or 256                    */
     int32_t layout;             /* tiled kernel's template layout (-1, 0, 1, 2)         */
     int32_t run_length;         /* run-layout kernel: template pixels per run, 4 or 8   */
     int32_t subsets_per_block;  /* subsets a block solves side by side (1 or 2)         */
