@@ -1438,7 +1438,7 @@ int run_length_for(gpv_context *ctx, int max_radius) {
     if (const char *v = getenv("GPV_RUN_K")) return atoi(v) == 4 ? 4 : 8;
     const int cls = max_radius <= 20 ? 0 : (max_radius <= 40 ? 1 : 2);
     if (ctx->tuned_run_k[cls]) return ctx->tuned_run_k[cls];
-    return 8;
+    return 4;
 }
 
 int tile_threads_for(gpv_context *ctx, int max_radius) {

@@ -209,7 +209,7 @@ int run_launch(gpv_context *ctx, int order, int nt, int K, bool kahan, int block
                const KArgs &k, const int32_t *seg, int *queue, int win_cap, int nslot, uint32_t *slot_mask,
                int slots_per_sm, int n_mask);
 // Run length of the run-layout kernel for subsets up to max_radius
-// (GPV_RUN_K, else a candidate being timed, else the tuned choice, else 8).
+// (GPV_RUN_K, else a candidate being timed, else the tuned choice, else 4).
 int run_length_for(gpv_context *ctx, int max_radius);
 int solve_noalloc_launch(gpv_context *ctx, const gpv_image *f, const gpv_image *g, const gpv_subset_desc *desc_dev,
                          int64_t n, int max_radius, const gpv_solve_params *prm, gpv_subset_result *out_dev,
