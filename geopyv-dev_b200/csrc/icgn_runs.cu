@@ -57,9 +57,8 @@ constexpr int kRunLengths[2] = {4, 8};  // run lengths K with task tables
 
 struct RunSmem {
     double mom[3 * 15];
-    double L[144];     // Cholesky factor of the scaled Hessian (lower triangle, row-major)
-    double Hi[144];    // H^-1 formed from the factor (explicit-inverse update)
-    double dsc[12];    // Jacobi scale 1 / sqrt(H_jj)
+    double L[144];     // Cholesky factor of the scaled Hessian, then its inverse (row-major)
+    double Hi[144];    // the Hessian, replaced by H^-1 formed from the factor
     double linv[12];   // 1 / L_jj
     double A[12], S[12];
     double p[12], pprev[12], dp[12], grad[12];
@@ -204,46 +203,49 @@ __device__ __forceinline__ double run_block_sum(double v, RunSmem &sm) {
     return t;
 }
 
-// Cholesky factor of the Jacobi-scaled SPD Hessian by one warp, in place:
-// Lm holds H (M x M, row-major) on entry; on exit its lower triangle holds
-// L with D H D = L L^T, D = diag(1 / sqrt(H_jj)) in dsc, 1 / L_jj in linv.
-// False when a pivot is not positive or not finite (a singular Hessian).
-// Warp-uniform result.
+// H^-1 of the Jacobi-scaled SPD Hessian by one warp, through its Cholesky
+// factor, in registers: D H D = L L^T with D = diag(1 / sqrt(H_jj)), then
+// H^-1 = D L^-T L^-1 D.  Lane i < M holds row i of the matrix; the pivot
+// and the column entries each step needs travel by shuffle, so the M steps
+// of the factorisation are shuffle-latency bound instead of shared-memory
+// round trips.  Lane c then solves L x = e_c for column c of L^-1 (rows of L
+// read from Lm, M*M shared scratch) and lane i forms row i of H^-1 into Hi.
+// H (M x M, row-major, shared) is read only.  False (warp-uniform) when a
+// pivot is not positive or not finite: a singular Hessian.
 template <int M>
-__device__ bool chol_warp(double *Lm, double *dsc, double *linv, int lane) {
-    bool ok = true;
-    for (int i = 0; i < M; i++) ok = ok && (Lm[i * M + i] > 0.0) && isfinite(Lm[i * M + i]);
-    if (!ok) return false;
-    if (lane < M) dsc[lane] = 1.0 / sqrt(Lm[lane * M + lane]);
-    __syncwarp();
-    for (int e = lane; e < M * M; e += 32) Lm[e] *= dsc[e / M] * dsc[e % M];
-    __syncwarp();
-    for (int k = 0; k < M; k++) {
-        const double piv = Lm[k * M + k];
-        if (!(piv > 0.0) || !isfinite(piv)) return false;  // uniform (same shared value)
-        const double lkk = sqrt(piv);
-        __syncwarp();
-        if (lane > k && lane < M) Lm[lane * M + k] /= lkk;
-        if (lane == k) {
-            Lm[k * M + k] = lkk;
-            linv[k] = 1.0 / lkk;
-        }
-        __syncwarp();
-        if (lane > k && lane < M) {
-            const double lik = Lm[lane * M + k];
-            for (int j = k + 1; j <= lane; j++) Lm[lane * M + j] = fma(-lik, Lm[j * M + k], Lm[lane * M + j]);
-        }
-        __syncwarp();
+__device__ bool chol_inverse_regs(const double *H, double *Lm, double *linv, double *Hi, int lane) {
+    constexpr unsigned kAll = 0xffffffffu;
+    const int li = lane < M ? lane : 0;  // lanes >= M shadow row 0; their results are never read
+    const double dii = H[li * M + li];
+    if (__any_sync(kAll, !(dii > 0.0) || !isfinite(dii))) return false;
+    const double si = 1.0 / sqrt(dii);
+    double h[M];
+#pragma unroll
+    for (int j = 0; j < M; j++) {
+        const double sj = __shfl_sync(kAll, si, j);
+        h[j] = H[li * M + j] * (si * sj);
     }
-    return true;
-}
-
-// H^-1 = D L^-T L^-1 D from the factor of chol_warp, formed once per subset
-// by one warp into Hi (M x M, row-major): lane c solves L x = e_c for
-// column c of L^-1 (forward substitution in registers), the columns replace
-// the factor in Lm, then each lane forms entries of D L^-T L^-1 D.
-template <int M>
-__device__ void chol_inverse_warp(double *Lm, const double *dsc, const double *linv, double *Hi, int lane) {
+    // 1 / L_kk into linv (shared, M doubles) by lane k
+#pragma unroll
+    for (int k = 0; k < M; k++) {
+        const double piv = __shfl_sync(kAll, h[k], k);
+        if (!(piv > 0.0) || !isfinite(piv)) return false;  // uniform: every lane has lane k's value
+        const double lkk = sqrt(piv);
+        const double rk = 1.0 / lkk;
+        if (lane == k) linv[k] = rk;
+        h[k] = li > k ? h[k] * rk : (li == k ? lkk : h[k]);
+#pragma unroll
+        for (int j = k + 1; j < M; j++) {
+            const double ljk = __shfl_sync(kAll, h[k], j);
+            if (li >= j) h[j] = fma(-h[k], ljk, h[j]);
+        }
+    }
+    if (lane < M) {
+#pragma unroll
+        for (int j = 0; j < M; j++) Lm[lane * M + j] = j <= lane ? h[j] : 0.0;
+    }
+    __syncwarp();
+    // column c = lane of L^-1 by forward substitution (zero above the diagonal)
     double x[M];
 #pragma unroll
     for (int i = 0; i < M; i++) {
@@ -258,13 +260,24 @@ __device__ void chol_inverse_warp(double *Lm, const double *dsc, const double *l
         for (int i = 0; i < M; i++) Lm[i * M + lane] = x[i];  // Lm now holds L^-1 (lower)
     }
     __syncwarp();
-    for (int e = lane; e < M * M; e += 32) {
-        const int i = e / M, j = e % M;
-        double acc = 0.0;
-        for (int k = (i > j ? i : j); k < M; k++) acc = fma(Lm[k * M + i], Lm[k * M + j], acc);
-        Hi[e] = dsc[i] * dsc[j] * acc;
+    // row i = lane of D L^-T L^-1 D: entry j is the dot product of columns i
+    // and j of L^-1 (four entries at a time)
+#pragma unroll
+    for (int j0 = 0; j0 < M; j0 += 4) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < M; k++) {
+#pragma unroll
+            for (int j = 0; j < 4 && j0 + j < M; j++) acc[j] = fma(x[k], Lm[k * M + j0 + j], acc[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 4 && j0 + j < M; j++) {
+            const double sj = __shfl_sync(kAll, si, j0 + j);
+            if (lane < M) Hi[lane * M + j0 + j] = si * sj * acc[j];
+        }
     }
     __syncwarp();
+    return true;
 }
 
 // The quintic basis at fraction t as symmetric pairs W[k] = (w_k, w_{5-k}),
@@ -611,9 +624,8 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
             if (lane < 3 * NMOM) sm.mom[lane] = sm.aug[NVA + lane];
             if (lane + 32 < 3 * NMOM) sm.mom[lane + 32] = sm.aug[NVA + lane + 32];
             __syncwarp();
-            assemble_hessian<ORDER>(sm.mom, sm.L, lane);
-            if (!chol_warp<M>(sm.L, sm.dsc, sm.linv, lane)) st = GPV_SINGULAR_H;
-            else chol_inverse_warp<M>(sm.L, sm.dsc, sm.linv, sm.Hi, lane);
+            assemble_hessian<ORDER>(sm.mom, sm.Hi, lane);
+            if (!chol_inverse_regs<M>(sm.Hi, sm.L, sm.linv, sm.Hi, lane)) st = GPV_SINGULAR_H;
         }
         if (lane == 0) {
             sm.flag[0] = st;
@@ -661,6 +673,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
 
     // ---- ICGN iterations --------------------------------------------------
     const double size = sqrt(dn);
+    const double inv_dn = 1.0 / dn, inv_df = 1.0 / df;
     int iters = 0, status = GPV_OK;
     bool converged = false;
     double c_zncc = 0.0, c_znssd = 4.0, last_norm = 0.0, gm_last = 0.0, dg_last = 0.0;
@@ -828,14 +841,15 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
             }
             const double t0 = __shfl_sync(0xffffffffu, tl, 0), t1 = __shfl_sync(0xffffffffu, tl, 1);
             const double t2 = __shfl_sync(0xffffffffu, tl, 2);
-            const double gmt = t0 / dn;
+            const double gmt = t0 * inv_dn;
             const double dg2 = t1 - t0 * gmt;
             const double dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
             // sum (f - f_m)(g - g_m) = sum (f - f_m)(g - f_m) (sum (f - f_m) = 0)
             //                     = sum (f - s)(g - f_m) - (f_m - s) sum (g - f_m)
             const double sab = t2 - (fm - (double)shift) * t0;
-            const double znssd = 2.0 - 2.0 * sab / (df * dg);
-            const double ratio = df / dg;
+            const double rdg = 1.0 / dg;  // one reciprocal on the update's critical path
+            const double znssd = 2.0 - 2.0 * sab * (inv_df * rdg);
+            const double ratio = df * rdg;
             // lane j < M: grad_j = A_j - (df/dg)(B_j - g~_m S_j); B_j sits at lane 3 + j
             const double bj = __shfl_down_sync(0xffffffffu, tl, 3);
             const double gj = lane < M ? sm.A[lane] - ratio * (bj - gmt * sm.S[lane]) : 0.0;

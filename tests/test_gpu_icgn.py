@@ -51,7 +51,8 @@ def _compare(res, ref, exact, label):
     assert np.array_equal(res["quality_ok"], ref["quality_ok"]), label
 
 
-@pytest.mark.parametrize("config,scale", [(1, 4), (2, 16), (3, 8)])
+# (1, 1): the rigid 1024^2 workload at full size, every one of its 2,401 subsets
+@pytest.mark.parametrize("config,scale", [(1, 1), (1, 4), (2, 16), (3, 8)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_batch_matches_oracle(oracle, gpv_mod, config, scale, precision):
     from gpv import synth
