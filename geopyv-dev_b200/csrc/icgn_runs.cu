@@ -55,6 +55,8 @@ constexpr int kRunMaxWarps = 8;  // blocks of 64, 128 or 256 threads
 constexpr int kRunMargin = 4;
 constexpr int kRunLengths[2] = {4, 8};  // run lengths K with task tables
 
+// NW: warps per block (block sums are kept per warp)
+template <int NW>
 struct RunSmem {
     double mom[3 * 15];
     double L[144];     // Cholesky factor of the scaled Hessian, then its inverse (row-major)
@@ -62,8 +64,8 @@ struct RunSmem {
     double linv[12];   // 1 / L_jj
     double A[12], S[12];
     double p[12], pprev[12], dp[12], grad[12];
-    double red[kRunMaxWarps][16];
-    double red2[kRunMaxWarps][80];
+    double red[NW][16];
+    double red2[NW][80];
     double aug[80];
     double tot[16];
     double misc[10];
@@ -89,7 +91,13 @@ struct RunArgs {
     int slots_per_sm, n_mask;
 };
 
-__host__ __device__ __forceinline__ int run_pitch(int ww) { return (ww + 31) & ~31; }
+// Window row pitch: a multiple of 4 floats (16-byte rows for cp.async) that
+// is not a multiple of 32, so two bands' rows read by one warp start on
+// different banks.  Lanes of a warp read consecutive columns of one row.
+__host__ __device__ __forceinline__ int run_pitch(int ww) {
+    const int p = (ww + 3) & ~3;
+    return (p & 31) ? p : p + 4;
+}
 
 // Copy coefficient rows [r0, r0+wh) x cols [c0, c0+ww) (c0, ww multiples of
 // 4) into win with row pitch `pitch`; out-of-range rows / columns clamped.
@@ -99,7 +107,7 @@ __host__ __device__ __forceinline__ int run_pitch(int ww) { return (ww + 31) & ~
 // returns, and the caller's block barrier publishes the window.  Both
 // addresses are 16-byte aligned: coefficient rows are a multiple of 32 floats
 // apart, c0 and the clamped columns are multiples of 4, and the window's
-// pitch is a multiple of 32 floats.
+// pitch is a multiple of 4 floats (run_pitch).
 template <int NT>
 __device__ __forceinline__ void run_stage(const float *__restrict__ C, int64_t cpitch, int ch, int r0, int c0, int wh,
                                           int ww, int pitch, float *win, int t0) {
@@ -119,8 +127,7 @@ __device__ __forceinline__ void run_stage(const float *__restrict__ C, int64_t c
 
 // A window covering pixel indices [xlo, xhi] x [ylo, yhi] (clamped to the
 // image) plus the taps and kRunMargin; false if it does not fit in cap
-// floats.  The row pitch is a multiple of 32 floats, so lanes reading one
-// column range of two neighbouring rows hit different banks.
+// floats (the margin is dropped when the window with it does not fit).
 __device__ __forceinline__ bool run_plan(int xlo, int xhi, int ylo, int yhi, int border, int cap, int &r0, int &c0,
                                          int &wh, int &ww, int &pitch) {
     for (int m = kRunMargin; m >= 0; m -= kRunMargin) {
@@ -136,7 +143,8 @@ __device__ __forceinline__ bool run_plan(int xlo, int xhi, int ylo, int yhi, int
     return false;
 }
 
-__device__ __forceinline__ bool run_covers(const RunSmem &sm, int xlo, int xhi, int ylo, int yhi, int border) {
+template <class S>
+__device__ __forceinline__ bool run_covers(const S &sm, int xlo, int xhi, int ylo, int yhi, int border) {
     if (!sm.win_ok) return false;
     return xlo + border - 2 >= sm.win_c0 && xhi + border + 3 < sm.win_c0 + sm.win_w && ylo + border - 2 >= sm.win_r0 &&
            yhi + border + 3 < sm.win_r0 + sm.win_h;
@@ -186,7 +194,7 @@ __device__ __forceinline__ void run_warp_sums(const float (&a)[KV], double *dst,
 }
 
 template <int NT>
-__device__ __forceinline__ double run_block_sum(double v, RunSmem &sm) {
+__device__ __forceinline__ double run_block_sum(double v, RunSmem<NT / 32> &sm) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const double s = warp_sum(v);
     if (lane == 0) sm.red[wid][0] = s;
@@ -387,7 +395,8 @@ __device__ __forceinline__ void unpack_task(int2 tk, int &dx, int &dy0) {
 }
 
 template <int ORDER, int NT, int K, bool KAHAN>
-__device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, float *base, float *win, RunSmem &sm) {
+__device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, float *base, float *win,
+                           RunSmem<NT / 32> &sm) {
     const KArgs &A = R.k;
     using O = Ord<ORDER>;
     constexpr int M = O::M, NMU = O::NMU, NMOM = O::NMOM, NB = 2 * O::DEG + 1;
@@ -1015,7 +1024,7 @@ template <int ORDER, int NT, int K, bool PER_SUBSET, bool KAHAN>
 __global__ void __launch_bounds__(NT, 512 / NT) icgn_runs(RunArgs R) {
     extern __shared__ float4 win4[];
     float *win = reinterpret_cast<float *>(win4);
-    __shared__ RunSmem sm;
+    __shared__ RunSmem<NT / 32> sm;
     const KArgs &A = R.k;
     const int start = R.seg[0], count = R.seg[1];
     if (PER_SUBSET) {

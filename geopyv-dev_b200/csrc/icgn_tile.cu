@@ -1345,6 +1345,19 @@ int tile_launch(gpv_context *ctx, const KArgs &K, int64_t n, cudaStream_t s) {
         // a window larger than the block can hold is not staged: those
         // subsets read g's coefficients from global memory
         P.cap = std::min(P.cap, max_bytes / (int)sizeof(float) / 4 * 4);
+        if (P.runs && P.nt == 64) {
+            // 64-thread blocks: a window cap that lets 8 blocks share an SM
+            // (16 warps, as 4 blocks of 128 threads, but 8 subsets in flight);
+            // a warped window larger than the cap reads g from global memory,
+            // which the autotuner weighs against 128-thread blocks
+            int sm_bytes = 0, reserved = 0;
+            GPV_CUDA_TRY(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+            GPV_CUDA_TRY(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, ctx->device));
+            cudaFuncAttributes fa;
+            GPV_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
+            const int cap8 = ((sm_bytes / 8 - reserved - (int)fa.sharedSizeBytes) / (int)sizeof(float)) & ~3;
+            if (cap8 > 0) P.cap = std::min(P.cap, cap8);
+        }
         const size_t smem = sizeof(float) * P.cap;
         int per_sm = 0;
         GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, P.nt, smem));
