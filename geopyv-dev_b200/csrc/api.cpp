@@ -330,7 +330,8 @@ static int image_alloc(gpv_context *ctx, int64_t h, int64_t w, int32_t border, u
     img->flags = flags;
     cudaError_t e = cudaMalloc(&img->c32, sizeof(float) * img->pitch32 * img->ch);
     if (e == cudaSuccess && (flags & GPV_IMAGE_KEEP_F64)) e = cudaMalloc(&img->c64, sizeof(double) * img->pitch64 * img->ch);
-    if (e == cudaSuccess) e = cudaMalloc(&img->rowpass, sizeof(double) * (img->h * img->cw + 2 * 89 + 8));
+    if (const size_t rb = prefilter_rowpass_bytes(img->h, img->cw, img->ch); e == cudaSuccess && rb)
+        e = cudaMalloc(&img->rowpass, rb);
     if (e == cudaSuccess && (flags & GPV_IMAGE_GRAIN) && grain_alloc(img) != GPV_SUCCESS) e = cudaErrorMemoryAllocation;
     if (e != cudaSuccess) {
         set_error(std::string("image allocation: ") + cudaGetErrorString(e));

@@ -123,7 +123,7 @@ struct gpv_image {
     int64_t pitch32 = 0, pitch64 = 0;  // elements per coefficient row
     float *c32 = nullptr;
     double *c64 = nullptr;
-    double *rowpass = nullptr;  // FP64 row-pass intermediate (h, cw)
+    double *rowpass = nullptr;  // FP64 row-pass intermediate (h, cw): images with a line under 89 samples only
     void *px_dev = nullptr;     // staging for host pixels
     size_t px_bytes = 0;
     uint8_t *rgb_dev = nullptr;  // staging for colour pixels (h * w * 3)
@@ -150,6 +150,8 @@ struct gpv_mask {
 namespace gpv {
 // prefilter.cu
 int prefilter_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s);
+// the FP64 row-pass buffer an image of this padded size needs (bytes; 0: none)
+size_t prefilter_rowpass_bytes(int64_t h, int64_t cw, int64_t ch);
 // host pixels (pinned) -> img->px_dev in row chunks on cs, each chunk's row
 // pass on s once it has landed, then the column pass on s; ev: nev >= 2 events
 int prefilter_from_host(gpv_image *img, const void *px_host, int dtype, cudaStream_t s, cudaStream_t cs,

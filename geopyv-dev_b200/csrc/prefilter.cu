@@ -14,13 +14,13 @@
 // |m| <= 44 reproduces the FFT result to FP64 rounding (1e-14 relative; see
 // tests/test_prefilter_*).  An image whose coefficients are kept in FP32
 // only uses |m| <= 28: the dropped taps sum to 2.7e-10 of the largest input
-// per pass, below FP32 rounding.  Each pass is one kernel: a tile of 32 lines
-// is staged in shared memory with its circular halo and every thread slides
-// a (2 MT + 1)-tap FP64 window along 16 outputs of one line (taps are kernel
-// parameters, i.e. constant-bank operands).  Row pass: pixels -> FP64
-// (h, w + 2b) (rows of the border are copies of rows 0 / h-1, so only the h
-// image rows are filtered); column pass: -> FP32 (and optionally FP64)
-// coefficients (h + 2b, w + 2b).
+// per pass, below FP32 rounding.  Both passes run in one kernel
+// (prefilter_fused): every thread slides a (2 MT + 1)-tap FP64 window along
+// 16 outputs of one line (taps are kernel parameters, i.e. constant-bank
+// operands), first along staged pixel rows, then down a ring of FP64
+// row-pass lines held in shared memory; the coefficients come out as FP32
+// (and optionally FP64), (h + 2b, w + 2b).  Images with a line shorter than
+// 89 samples take two simple kernels through an FP64 row-pass buffer.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -33,10 +33,8 @@ namespace {
 constexpr int kM = 44;             // taps on each side of the centre (FP64 coefficients)
 constexpr int kM32 = 28;           // the same when the coefficients are kept in FP32 only
 constexpr int kT = 2 * kM + 1;     // 89
-constexpr int kLines = 32;         // lines per tile (one per lane)
 constexpr int kGroups = 8;         // warps per block
 constexpr int kQ = 16;             // outputs per thread
-constexpr int kSpan = kGroups * kQ;  // 128 outputs per line per block
 
 struct TapArg {
     double h[kT];  // h[k] multiplies x[j - mr + k]  (i.e. h_N[mr - k])
@@ -50,97 +48,150 @@ __device__ __forceinline__ double px_load(const P *p, int64_t i) {
     return (double)p[i];
 }
 
-// Row pass: out[r][j] = sum_k taps[k] * X[r][(j - MT + k) mod cw], X = replicate-padded row r,
-// k = 0 .. 2 MT.
-template <typename P, int MT>
-__global__ void __launch_bounds__(kGroups * 32) rowpass_fir(const P *__restrict__ px, int64_t h, int64_t w, int64_t border,
-                                                            int64_t cw, int mr, TapArg taps, double *__restrict__ out) {
-    constexpr int kTaps = 2 * MT + 1, kHalo = kTaps - 1;
-    extern __shared__ double tile[];  // [kLines][kSpan + kHalo + 1]
-    constexpr int stride = kSpan + kHalo + 1;
-    const int64_t r0 = (int64_t)blockIdx.y * kLines;
-    const int64_t j0 = (int64_t)blockIdx.x * kSpan;
-    for (int idx = threadIdx.x; idx < kLines * (kSpan + kHalo); idx += blockDim.x) {
-        const int rr = idx / (kSpan + kHalo), s = idx % (kSpan + kHalo);
-        int64_t r = r0 + rr;
-        if (r > h - 1) r = h - 1;
-        int64_t jj = (j0 - mr + s) % cw;
-        if (jj < 0) jj += cw;
-        int64_t c = jj - border;
-        c = c < 0 ? 0 : (c > w - 1 ? w - 1 : c);
-        tile[rr * stride + s] = px_load(px, r * w + c);
-    }
-    __syncthreads();
-    const int rr = threadIdx.x & 31, grp = threadIdx.x >> 5;
-    const double *x = tile + rr * stride + grp * kQ;
-    double acc[kQ];
-#pragma unroll
-    for (int q = 0; q < kQ; q++) acc[q] = 0.0;
-#pragma unroll
-    for (int s = 0; s < kQ + kHalo; s++) {
-        const double xv = x[s];
-#pragma unroll
-        for (int q = 0; q < kQ; q++) {
-            const int k = s - q;
-            if (k >= 0 && k < kTaps) acc[q] = fma(taps.h[k], xv, acc[q]);
-        }
-    }
-    const int64_t r = r0 + rr;
-    if (r < h) {
-#pragma unroll
-        for (int q = 0; q < kQ; q++) {
-            const int64_t j = j0 + grp * kQ + q;
-            if (j < cw) out[r * cw + j] = acc[q];
-        }
-    }
+// Both passes in one kernel.  A block owns a strip of kStrip padded columns
+// [j0, j0 + kStrip) and a segment of output rows [i_beg, i_end).  It walks
+// down the segment kStep rows at a time: the row pass of the next kStep
+// padded rows (from pixel lines staged in shared memory) lands in a ring of
+// FP64 lines that also holds the 2 MT lines before them, and the column pass
+// of kStep outputs reads that ring.  The FP64 row-pass lines never leave the
+// SM: DRAM sees the pixels (read once per strip; the halo columns of
+// neighbouring strips come from L2) and the coefficients written.  Each
+// output is the same FMA sequence, in the same order, as a separate row
+// pass and column pass would give (taps k = 0 .. 2 MT, increasing).
+//   row pass:    R[r][j] = sum_k tr[k] X[r][(j - MT + k) mod cw],
+//                X[r][jj] = px[r][clamp(jj - border, 0, w - 1)]
+//   column pass: C[i][j] = sum_k tc[k] R[clamp((i - MT + k) mod ch - border, 0, h - 1)][j]
+constexpr int kStrip = 32;   // columns per block (one per lane in the column pass)
+constexpr int kStep = 128;   // output rows per step (8 warps x kQ)
+constexpr int kFusedThreads = kGroups * 32;
+static_assert(kStep == kGroups * kQ && kStrip == 2 * kQ, "one row-pass line per two threads, one output column per lane");
+
+// Staged pixel line pitch (elements) for kPxW pixels: lanes of a warp read 32
+// different lines at one column, so the pitch in 4-byte words is odd (an odd
+// number of doubles for FP64 pixels).
+template <typename P, int W>
+__host__ __device__ constexpr int px_pitch() {
+    return sizeof(P) == 8 ? (W | 1) : (((W * (int)sizeof(P) + 3) / 4) | 1) * 4 / (int)sizeof(P);
 }
 
-// Column pass over padded rows i: C[i][j] = sum_k taps[k] * R[(i - mr + k) mod ch][j],
-// R[ii] = rowpass[clamp(ii - border, 0, h - 1)].
-template <int MT>
-__global__ void __launch_bounds__(kGroups * 32) colpass_fir(const double *__restrict__ rp, int64_t h, int64_t cw,
-                                                            int64_t ch, int64_t border, int mr, TapArg taps,
-                                                            float *__restrict__ c32, int64_t pitch32,
-                                                            double *__restrict__ c64, int64_t pitch64) {
-    constexpr int kTaps = 2 * MT + 1, kHalo = kTaps - 1;
-    extern __shared__ double tile[];  // [kSpan + kHalo][kLines]
-    const int64_t i0 = (int64_t)blockIdx.y * kSpan;
-    const int64_t j0 = (int64_t)blockIdx.x * kLines;
-    for (int idx = threadIdx.x; idx < (kSpan + kHalo) * kLines; idx += blockDim.x) {
-        const int s = idx / kLines, c = idx % kLines;
-        int64_t ii = (i0 - mr + s) % ch;
-        if (ii < 0) ii += ch;
-        int64_t r = ii - border;
-        r = r < 0 ? 0 : (r > h - 1 ? h - 1 : r);
-        int64_t j = j0 + c;
-        if (j > cw - 1) j = cw - 1;
-        tile[s * kLines + c] = rp[r * cw + j];
+template <typename P, int MT>
+struct Fused {
+    static constexpr int kTaps = 2 * MT + 1, kHalo = 2 * MT;
+    static constexpr int kRing = kStep + kHalo;   // FP64 row-pass lines held
+    static constexpr int kRingPitch = kStrip + 1;  // doubles
+    static constexpr int kPxW = kStrip + kHalo;   // pixels per staged line
+    static constexpr int kPxPitch = px_pitch<P, kPxW>();
+    static constexpr size_t kRingBytes = sizeof(double) * kRing * kRingPitch;
+    static constexpr size_t kSmem = kRingBytes + sizeof(P) * kStep * kPxPitch;
+};
+
+template <typename P, int MT>
+__global__ void __launch_bounds__(kFusedThreads) prefilter_fused(const P *__restrict__ px, int64_t h, int64_t w,
+                                                                int64_t border, int64_t cw, int64_t ch, int64_t i_lo,
+                                                                int64_t i_hi, int64_t seg, TapArg tr, TapArg tc,
+                                                                float *__restrict__ c32, int64_t pitch32,
+                                                                double *__restrict__ c64, int64_t pitch64) {
+    using G = Fused<P, MT>;
+    extern __shared__ double smem[];
+    double *ring = smem;
+    P *pxs = reinterpret_cast<P *>(reinterpret_cast<unsigned char *>(smem) + G::kRingBytes);
+    const int64_t j0 = (int64_t)blockIdx.x * kStrip;
+    const int64_t i_beg = i_lo + (int64_t)blockIdx.y * seg;
+    const int64_t i_end = i_beg + seg < i_hi ? i_beg + seg : i_hi;
+    if (i_beg >= i_end) return;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+
+    // the strip's source columns, the same for every line: entry m of lane
+    // l is staged column l + 32 m, its image column (-1 past the staged width)
+    constexpr int kCols = (G::kPxW + 31) / 32;
+    int csrc[kCols];
+#pragma unroll
+    for (int m = 0; m < kCols; m++) {
+        const int sx = lane + 32 * m;
+        int jj = (int)j0 - MT + sx;  // in [-MT, cw + kStrip + MT): one wrap at most (cw >= 2 MT + 1)
+        jj = jj < 0 ? jj + (int)cw : (jj >= (int)cw ? jj - (int)cw : jj);
+        const int c = jj - (int)border;
+        csrc[m] = sx < G::kPxW ? (c < 0 ? 0 : (c > (int)w - 1 ? (int)w - 1 : c)) : -1;
     }
-    __syncthreads();
-    const int c = threadIdx.x & 31, grp = threadIdx.x >> 5;
-    const double *x = tile + grp * kQ * kLines + c;
-    double acc[kQ];
+    // row pass of n padded rows (row0 + t) mod ch, t < n <= kStep, into ring
+    // lines [dst, dst + n); the pixel lines are staged one per warp at a time
+    auto produce = [&](int64_t row0, int n, int dst) {
+        int base = (int)(row0 % ch);  // row0 >= -MT
+        if (base < 0) base += (int)ch;
+        for (int rr = wid; rr < n; rr += kGroups) {
+            int ii = base + rr;
+            while (ii >= (int)ch) ii -= (int)ch;
+            int r = ii - (int)border;
+            r = r < 0 ? 0 : (r > (int)h - 1 ? (int)h - 1 : r);
+            const P *src = px + (int64_t)r * w;
+            P *d = pxs + rr * G::kPxPitch + lane;
 #pragma unroll
-    for (int q = 0; q < kQ; q++) acc[q] = 0.0;
-#pragma unroll
-    for (int s = 0; s < kQ + kHalo; s++) {
-        const double xv = x[s * kLines];
-#pragma unroll
-        for (int q = 0; q < kQ; q++) {
-            const int k = s - q;
-            if (k >= 0 && k < kTaps) acc[q] = fma(taps.h[k], xv, acc[q]);
+            for (int m = 0; m < kCols; m++)
+                if (csrc[m] >= 0) d[32 * m] = src[csrc[m]];
         }
-    }
-    const int64_t j = j0 + c;
-    if (j < cw) {
+        __syncthreads();
+        const int rr = (wid & 3) * 32 + lane, half = wid >> 2;
+        if (rr < n) {
+            const P *x = pxs + rr * G::kPxPitch + half * kQ;
+            double acc[kQ];
 #pragma unroll
-        for (int q = 0; q < kQ; q++) {
-            const int64_t i = i0 + grp * kQ + q;
-            if (i < ch) {
-                c32[i * pitch32 + j] = (float)acc[q];
-                if (c64) c64[i * pitch64 + j] = acc[q];
+            for (int q = 0; q < kQ; q++) acc[q] = 0.0;
+#pragma unroll
+            for (int sx = 0; sx < kQ + G::kHalo; sx++) {
+                const double xv = (double)x[sx];
+#pragma unroll
+                for (int q = 0; q < kQ; q++) {
+                    const int k = sx - q;
+                    if (k >= 0 && k < G::kTaps) acc[q] = fma(tr.h[k], xv, acc[q]);
+                }
+            }
+            double *o = ring + (dst + rr) * G::kRingPitch + half * kQ;
+#pragma unroll
+            for (int q = 0; q < kQ; q++) o[q] = acc[q];
+        }
+        __syncthreads();
+    };
+
+    // the 2 MT lines before the first output
+    produce(i_beg - MT, G::kHalo, 0);
+    for (int64_t done = 0; done < i_end - i_beg; done += kStep) {
+        const int n = (int)(i_end - i_beg - done < kStep ? i_end - i_beg - done : kStep);
+        produce(i_beg + MT + done, n, G::kHalo);
+        // column pass: lane = column, warp wid = outputs [wid kQ, wid kQ + kQ) of this step
+        if (wid * kQ < n) {
+            const double *x = ring + (wid * kQ) * G::kRingPitch + lane;
+            double acc[kQ];
+#pragma unroll
+            for (int q = 0; q < kQ; q++) acc[q] = 0.0;
+#pragma unroll
+            for (int sx = 0; sx < kQ + G::kHalo; sx++) {
+                const double xv = x[sx * G::kRingPitch];
+#pragma unroll
+                for (int q = 0; q < kQ; q++) {
+                    const int k = sx - q;
+                    if (k >= 0 && k < G::kTaps) acc[q] = fma(tc.h[k], xv, acc[q]);
+                }
+            }
+            const int64_t j = j0 + lane;
+            if (j < cw) {
+#pragma unroll
+                for (int q = 0; q < kQ; q++) {
+                    if (wid * kQ + q < n) {
+                        const int64_t i = i_beg + done + wid * kQ + q;
+                        c32[i * pitch32 + j] = (float)acc[q];
+                        if (c64) c64[i * pitch64 + j] = acc[q];
+                    }
+                }
             }
         }
+        if (n < kStep) break;  // the segment's last step
+        __syncthreads();  // every column pass has read the ring
+        // the last 2 MT lines become the first ones of the next step (n = kStep >= 2 MT: no overlap)
+        for (int idx = tid; idx < G::kHalo * kStrip; idx += kFusedThreads) {
+            const int rr = idx / kStrip, c = idx - rr * kStrip;
+            ring[rr * G::kRingPitch + c] = ring[(kStep + rr) * G::kRingPitch + c];
+        }
+        __syncthreads();
     }
 }
 
@@ -191,44 +242,69 @@ void fill_taparg_central(const Taps &t, int mt, TapArg &a) {
     for (int k = 0; k <= 2 * mt; k++) a.h[k] = t.h[t.ml + mt - k];
 }
 
-// One FIR pass pair for lines of at least kT samples, MT taps on each side.
-// Rows [r0, r0 + nr) of the image (rows are filtered independently).
+// Blocks per SM of one fused instantiation at its shared memory (cached per
+// device); also raises the kernel's dynamic shared-memory limit.
 template <typename P, int MT>
-int launch_fir_rows(gpv_image *img, const P *px, const Taps &tr, cudaStream_t s, int64_t r0 = 0, int64_t nr = -1) {
-    constexpr int kHalo = 2 * MT;
-    if (nr < 0) nr = img->h - r0;
-    const size_t smem_row = sizeof(double) * kLines * (kSpan + kHalo + 1);
-    TapArg a;
-    fill_taparg_central(tr, MT, a);
-    GPV_CUDA_TRY(cudaFuncSetAttribute(rowpass_fir<P, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_row));
-    dim3 grid((unsigned)((img->cw + kSpan - 1) / kSpan), (unsigned)((nr + kLines - 1) / kLines));
-    rowpass_fir<P, MT><<<grid, kGroups * 32, smem_row, s>>>(px + r0 * img->w, nr, img->w, img->border, img->cw, MT, a,
-                                                             img->rowpass + r0 * img->cw);
+int fused_blocks_per_sm(int *bps) {
+    static std::mutex mu;
+    static std::map<int, int> done;
+    int dev = 0;
+    GPV_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = done.find(dev);
+    if (it == done.end()) {
+        constexpr size_t smem = Fused<P, MT>::kSmem;
+        GPV_CUDA_TRY(cudaFuncSetAttribute(prefilter_fused<P, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int n = 0;
+        GPV_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, prefilter_fused<P, MT>, kFusedThreads, smem));
+        it = done.emplace(dev, n > 0 ? n : 1).first;
+    }
+    *bps = it->second;
     return GPV_SUCCESS;
 }
 
-template <int MT>
-int launch_fir_cols(gpv_image *img, const Taps &tc, cudaStream_t s) {
-    constexpr int kHalo = 2 * MT;
-    const size_t smem_col = sizeof(double) * (kSpan + kHalo) * kLines;
-    TapArg a;
-    fill_taparg_central(tc, MT, a);
-    GPV_CUDA_TRY(cudaFuncSetAttribute(colpass_fir<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_col));
-    dim3 grid((unsigned)((img->cw + kLines - 1) / kLines), (unsigned)((img->ch + kSpan - 1) / kSpan));
-    colpass_fir<MT><<<grid, kGroups * 32, smem_col, s>>>(img->rowpass, img->h, img->cw, img->ch, img->border, MT, a,
-                                                         img->c32, img->pitch32, img->c64, img->pitch64);
+// Coefficient rows [lo, hi) of an image whose lines both have at least kT
+// samples, MT taps on each side.  Segments of rows split the work into about
+// three waves of blocks, each segment at least 6 x 2 MT rows long (its 2 MT
+// lead-in row-pass lines are the only work done twice).
+template <typename P, int MT>
+int launch_fused(gpv_image *img, const P *px, const Taps &tr, const Taps &tc, cudaStream_t s, int64_t lo, int64_t hi) {
+    if (hi <= lo) return GPV_SUCCESS;
+    int bps = 1;
+    if (int rc = fused_blocks_per_sm<P, MT>(&bps)) return rc;
+    TapArg ar, ac;
+    fill_taparg_central(tr, MT, ar);
+    fill_taparg_central(tc, MT, ac);
+    const int64_t strips = (img->cw + kStrip - 1) / kStrip, rows = hi - lo;
+    const int64_t target = 3LL * bps * std::max(1, img->ctx->num_sms);
+    int64_t segs = std::max<int64_t>(1, (target + strips - 1) / strips);
+    segs = std::min<int64_t>(segs, std::max<int64_t>(1, rows / (6 * 2 * MT)));
+    const int64_t seg = (rows + segs - 1) / segs;
+    segs = (rows + seg - 1) / seg;
+    prefilter_fused<P, MT><<<dim3((unsigned)strips, (unsigned)segs), kFusedThreads, Fused<P, MT>::kSmem, s>>>(
+        px, img->h, img->w, img->border, img->cw, img->ch, lo, hi, seg, ar, ac, img->c32, img->pitch32, img->c64,
+        img->pitch64);
+    GPV_CUDA_TRY(cudaGetLastError());
     return GPV_SUCCESS;
 }
+
+template <typename P>
+int launch_fused_rows(gpv_image *img, const P *px, const Taps &tr, const Taps &tc, cudaStream_t s, int64_t lo,
+                      int64_t hi) {
+    // coefficients kept in FP32 only: |m| <= kM32
+    return img->c64 == nullptr ? launch_fused<P, kM32>(img, px, tr, tc, s, lo, hi)
+                               : launch_fused<P, kM>(img, px, tr, tc, s, lo, hi);
+}
+
+bool long_lines(const gpv_image *img) { return img->cw >= kT && img->ch >= kT; }
 
 template <typename P>
 int run_prefilter(gpv_image *img, const P *px, cudaStream_t s) {
     const Taps &tr = taps_for(img->cw);
     const Taps &tc = taps_for(img->ch);
-    const bool f32_only = img->c64 == nullptr;  // coefficients kept in FP32 only: |m| <= kM32
-    if (tr.ml + tr.mr + 1 == kT) {
-        if (int rc = f32_only ? launch_fir_rows<P, kM32>(img, px, tr, s) : launch_fir_rows<P, kM>(img, px, tr, s))
-            return rc;
-    } else {
+    if (long_lines(img)) return launch_fused_rows(img, px, tr, tc, s, 0, img->ch);
+    // a short line: every circulant tap, through the FP64 row-pass buffer
+    {
         const int nt = tr.ml + tr.mr + 1;
         TapArg a;
         fill_taparg(tr, a);
@@ -240,9 +316,7 @@ int run_prefilter(gpv_image *img, const P *px, cudaStream_t s) {
         GPV_CUDA_TRY(cudaStreamSynchronize(s));  // host tap array is reused below
     }
     GPV_CUDA_TRY(cudaGetLastError());
-    if (tc.ml + tc.mr + 1 == kT) {
-        if (int rc = f32_only ? launch_fir_cols<kM32>(img, tc, s) : launch_fir_cols<kM>(img, tc, s)) return rc;
-    } else {
+    {
         const int nt = tc.ml + tc.mr + 1;
         TapArg a;
         fill_taparg(tc, a);
@@ -292,30 +366,32 @@ const Taps &taps_for(int64_t n) {
 }
 
 namespace {
-// Host pixels in row chunks into img->px_dev on the copy stream cs; the row
-// pass of each chunk starts on s as soon as its copy has landed, so the
-// copies overlap the row passes; then the column pass on s.  Lines too short
-// for the FIR kernels take the whole copy, then the ordinary prefilter.
+// Host pixels in row chunks into img->px_dev on the copy stream cs.  As each
+// chunk lands, the coefficient rows whose lines all come from rows already
+// landed are filtered on s, so the copies overlap the filtering; the first
+// MT coefficient rows (their column taps wrap to the image's last rows) go
+// after the last chunk.  Images with a short line take the whole copy, then
+// the ordinary prefilter.
 template <typename P>
 int prefilter_host(gpv_image *img, const P *px_host, cudaStream_t s, cudaStream_t cs, cudaEvent_t *ev, int nev) {
     P *dst = static_cast<P *>(img->px_dev);
     const size_t row_bytes = sizeof(P) * (size_t)img->w;
     const Taps &tr = taps_for(img->cw);
     const Taps &tc = taps_for(img->ch);
-    const bool fir = tr.ml + tr.mr + 1 == kT && tc.ml + tc.mr + 1 == kT;
-    // rows per copy: ceil(h / (nev - 1)) rounded up to whole row tiles, so at
-    // most nev - 1 chunks (events ev[1 .. nev-1]) cover the image
-    const int64_t chunk = ((img->h + nev - 2) / (nev - 1) + kLines - 1) / kLines * kLines;
+    // rows per copy: ceil(h / (nev - 1)) rounded up to 32, so at most nev - 1
+    // chunks (events ev[1 .. nev-1]) cover the image
+    const int64_t chunk = ((img->h + nev - 2) / (nev - 1) + 31) / 32 * 32;
     // the copies wait for earlier work on s that may still read px_dev
     GPV_CUDA_TRY(cudaEventRecord(ev[0], s));
     GPV_CUDA_TRY(cudaStreamWaitEvent(cs, ev[0], 0));
-    if (!fir || img->h < 2 * kLines * (nev - 1)) {
+    if (!long_lines(img) || img->h < 2 * 32 * (nev - 1)) {
         GPV_CUDA_TRY(cudaMemcpyAsync(dst, px_host, row_bytes * (size_t)img->h, cudaMemcpyHostToDevice, cs));
         GPV_CUDA_TRY(cudaEventRecord(ev[1], cs));
         GPV_CUDA_TRY(cudaStreamWaitEvent(s, ev[1], 0));
         return run_prefilter(img, static_cast<const P *>(dst), s);
     }
-    const bool f32_only = img->c64 == nullptr;
+    const int64_t mt = img->c64 == nullptr ? kM32 : kM;
+    int64_t lo = mt;  // coefficient rows [0, mt) wait for the last chunk
     int k = 1;
     for (int64_t r0 = 0; r0 < img->h; r0 += chunk, k++) {
         // the last event takes whatever rows remain (never an event past ev[nev - 1])
@@ -324,14 +400,15 @@ int prefilter_host(gpv_image *img, const P *px_host, cudaStream_t s, cudaStream_
                                      cudaMemcpyHostToDevice, cs));
         GPV_CUDA_TRY(cudaEventRecord(ev[k], cs));
         GPV_CUDA_TRY(cudaStreamWaitEvent(s, ev[k], 0));
-        if (int rc = f32_only ? launch_fir_rows<P, kM32>(img, dst, tr, s, r0, nr)
-                              : launch_fir_rows<P, kM>(img, dst, tr, s, r0, nr))
-            return rc;
+        // coefficient row i reads image rows up to min(h - 1, i + mt - border)
+        const int64_t landed = r0 + nr;
+        const int64_t hi = landed >= img->h ? img->ch : std::min(img->ch, landed - mt + img->border);
+        if (hi > lo) {
+            if (int rc = launch_fused_rows(img, static_cast<const P *>(dst), tr, tc, s, lo, hi)) return rc;
+            lo = hi;
+        }
     }
-    GPV_CUDA_TRY(cudaGetLastError());
-    if (int rc = f32_only ? launch_fir_cols<kM32>(img, tc, s) : launch_fir_cols<kM>(img, tc, s)) return rc;
-    GPV_CUDA_TRY(cudaGetLastError());
-    return GPV_SUCCESS;
+    return launch_fused_rows(img, static_cast<const P *>(dst), tr, tc, s, 0, mt);
 }
 }  // namespace
 
@@ -344,6 +421,11 @@ int prefilter_from_host(gpv_image *img, const void *px_host, int dtype, cudaStre
         case GPV_F64: return prefilter_host(img, static_cast<const double *>(px_host), s, cs, ev, nev);
         default: set_error("unknown pixel dtype"); return GPV_ERR_INVALID;
     }
+}
+
+size_t prefilter_rowpass_bytes(int64_t h, int64_t cw, int64_t ch) {
+    // the row pass plus two tap vectors of scratch, for the short-line kernels only
+    return (cw >= kT && ch >= kT) ? 0 : sizeof(double) * (size_t)(h * cw + 2 * kT + 8);
 }
 
 int prefilter_launch(gpv_image *img, const void *px_dev, int dtype, cudaStream_t s) {

@@ -76,7 +76,7 @@ size_t estimate_footprint(const gpv_request &r) {
     const size_t pitch = (cw + 31) / 32 * 32;
     const size_t esz = r.dtype == GPV_U8 ? 1 : r.dtype == GPV_U16 ? 2 : r.dtype == GPV_F32 ? 4 : 8;
     const size_t coef = 2 * sizeof(float) * pitch * ch;             // f and g coefficients
-    const size_t rowpass = 2 * sizeof(double) * (size_t)r.h * cw;   // row-pass intermediates
+    const size_t rowpass = 2 * prefilter_rowpass_bytes(r.h, (int64_t)cw, (int64_t)ch);  // short-line images only
     const size_t pixels = 2 * esz * (size_t)r.h * (size_t)r.w;       // staged pixels
     const size_t subsets = (size_t)r.n * (sizeof(gpv_subset_desc) + sizeof(gpv_subset_result) + 4);
     return coef + rowpass + pixels + subsets;

@@ -20,7 +20,9 @@ def _desc(gpv, n):
 def _footprint(h, w, n, border=20, esz=1):
     cw, ch = w + 2 * border, h + 2 * border
     pitch = (cw + 31) // 32 * 32
-    return 2 * 4 * pitch * ch + 2 * 8 * h * cw + 2 * esz * h * w + n * (120 + 200 + 4)
+    # an FP64 row-pass buffer only for images with a line under 89 samples
+    rowpass = 0 if min(cw, ch) >= 89 else 8 * (h * cw + 2 * 89 + 8)
+    return 2 * 4 * pitch * ch + 2 * rowpass + 2 * esz * h * w + n * (120 + 200 + 4)
 
 
 class Recorder:
