@@ -219,7 +219,7 @@ __device__ __forceinline__ bool compose2_regs(const double *p, const double *d, 
     for (int k = 0; k < 6; k++) {
         const double piv = A[k][k];
         ok = ok && (piv != 0.0) && isfinite(piv);
-        const double inv = 1.0 / piv;
+        const double inv = __drcp_rn(piv);  // the correctly rounded 1 / piv, without a general division
 #pragma unroll
         for (int i = k + 1; i < 6; i++) {
             const double f = A[i][k] * inv;
@@ -236,7 +236,7 @@ __device__ __forceinline__ bool compose2_regs(const double *p, const double *d, 
             X[k][0] = fma(-A[k][j], X[j][0], X[k][0]);
             X[k][1] = fma(-A[k][j], X[j][1], X[k][1]);
         }
-        const double inv = 1.0 / A[k][k];
+        const double inv = __drcp_rn(A[k][k]);
         X[k][0] *= inv;
         X[k][1] *= inv;
     }

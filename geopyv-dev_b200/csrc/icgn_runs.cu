@@ -213,33 +213,44 @@ __device__ __forceinline__ double run_block_sum(double v, RunSmem<NT / 32> &sm) 
 
 // H^-1 of the Jacobi-scaled SPD Hessian by one warp, through its Cholesky
 // factor, in registers: D H D = L L^T with D = diag(1 / sqrt(H_jj)), then
-// H^-1 = D L^-T L^-1 D.  Lane i < M holds row i of the matrix; the pivot
-// and the column entries each step needs travel by shuffle, so the M steps
-// of the factorisation are shuffle-latency bound instead of shared-memory
-// round trips.  Lane c then solves L x = e_c for column c of L^-1 (rows of L
-// read from Lm, M*M shared scratch) and lane i forms row i of H^-1 into Hi.
-// H (M x M, row-major, shared) is read only.  False (warp-uniform) when a
-// pivot is not positive or not finite: a singular Hessian.
-template <int M>
-__device__ bool chol_inverse_regs(const double *H, double *Lm, double *linv, double *Hi, int lane) {
+// H^-1 = D L^-T L^-1 D.  Lane i < M builds row i of H from the gradient
+// moments (H_jk = c_j c_k sum g_p g_q dx^a dy^b, the entries assemble_hessian
+// gives) and keeps it in registers; the pivot and the column entries each
+// step needs travel by shuffle.  Each pivot takes one reciprocal square root
+// (1 / L_kk, and L_kk = pivot x that), not a square root and a division:
+// the serial chain of a lone warp is what this stretch costs.  Lane c then
+// solves L x = e_c for column c of L^-1 (rows of L read from Lm, M*M shared
+// scratch) and lane i forms row i of H^-1 into Hi.  False (warp-uniform)
+// when a pivot is not positive or not finite: a singular Hessian.
+template <int ORDER>
+__device__ bool hess_inverse_regs(const double *mom, double *Lm, double *linv, double *Hi, int lane) {
+    using O = Ord<ORDER>;
+    constexpr int M = O::M;
     constexpr unsigned kAll = 0xffffffffu;
     const int li = lane < M ? lane : 0;  // lanes >= M shadow row 0; their results are never read
-    const double dii = H[li * M + li];
-    if (__any_sync(kAll, !(dii > 0.0) || !isfinite(dii))) return false;
-    const double si = 1.0 / sqrt(dii);
+    const int mi = li >> 1, ci = li & 1, ai = mu_a(mi), bi = mu_b(mi);
+    const double cci = mu_c(mi);
     double h[M];
+#pragma unroll
+    for (int k = 0; k < M; k++) {
+        const int mk = k >> 1, ck = k & 1;
+        h[k] = cci * mu_c(mk) * mom[(ci + ck) * O::NMOM + mom_idx(ai + mu_a(mk), bi + mu_b(mk))];
+    }
+    const double dii = cci * cci * mom[(2 * ci) * O::NMOM + mom_idx(2 * ai, 2 * bi)];  // h[li]
+    if (__any_sync(kAll, !(dii > 0.0) || !isfinite(dii))) return false;
+    const double si = rsqrt(dii);
 #pragma unroll
     for (int j = 0; j < M; j++) {
         const double sj = __shfl_sync(kAll, si, j);
-        h[j] = H[li * M + j] * (si * sj);
+        h[j] *= si * sj;
     }
     // 1 / L_kk into linv (shared, M doubles) by lane k
 #pragma unroll
     for (int k = 0; k < M; k++) {
         const double piv = __shfl_sync(kAll, h[k], k);
         if (!(piv > 0.0) || !isfinite(piv)) return false;  // uniform: every lane has lane k's value
-        const double lkk = sqrt(piv);
-        const double rk = 1.0 / lkk;
+        const double rk = rsqrt(piv);
+        const double lkk = piv * rk;
         if (lane == k) linv[k] = rk;
         h[k] = li > k ? h[k] * rk : (li == k ? lkk : h[k]);
 #pragma unroll
@@ -253,14 +264,17 @@ __device__ bool chol_inverse_regs(const double *H, double *Lm, double *linv, dou
         for (int j = 0; j < M; j++) Lm[lane * M + j] = j <= lane ? h[j] : 0.0;
     }
     __syncwarp();
-    // column c = lane of L^-1 by forward substitution (zero above the diagonal)
+    // column c = lane of L^-1 by forward substitution (zero above the
+    // diagonal), right-looking: each x_k, once known, updates every later
+    // row at once, so the dependent chain is M steps, not M (M - 1) / 2
     double x[M];
 #pragma unroll
-    for (int i = 0; i < M; i++) {
-        double v = (i == lane) ? 1.0 : 0.0;
+    for (int i = 0; i < M; i++) x[i] = (i == lane) ? 1.0 : 0.0;
 #pragma unroll
-        for (int k = 0; k < i; k++) v = fma(-Lm[i * M + k], x[k], v);
-        x[i] = (i >= lane) ? v * linv[i] : 0.0;
+    for (int k = 0; k < M; k++) {
+        x[k] = (k >= lane) ? x[k] * linv[k] : 0.0;
+#pragma unroll
+        for (int i = k + 1; i < M; i++) x[i] = fma(-Lm[i * M + k], x[k], x[i]);
     }
     __syncwarp();
     if (lane < M) {
@@ -269,20 +283,19 @@ __device__ bool chol_inverse_regs(const double *H, double *Lm, double *linv, dou
     }
     __syncwarp();
     // row i = lane of D L^-T L^-1 D: entry j is the dot product of columns i
-    // and j of L^-1 (four entries at a time)
+    // and j of L^-1 (all M entries side by side: chains of M FMAs)
+    double acc[M];
 #pragma unroll
-    for (int j0 = 0; j0 < M; j0 += 4) {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int j = 0; j < M; j++) acc[j] = 0.0;
 #pragma unroll
-        for (int k = 0; k < M; k++) {
+    for (int k = 0; k < M; k++) {
 #pragma unroll
-            for (int j = 0; j < 4 && j0 + j < M; j++) acc[j] = fma(x[k], Lm[k * M + j0 + j], acc[j]);
-        }
+        for (int j = 0; j < M; j++) acc[j] = fma(x[k], Lm[k * M + j], acc[j]);
+    }
 #pragma unroll
-        for (int j = 0; j < 4 && j0 + j < M; j++) {
-            const double sj = __shfl_sync(kAll, si, j0 + j);
-            if (lane < M) Hi[lane * M + j0 + j] = si * sj * acc[j];
-        }
+    for (int j = 0; j < M; j++) {
+        const double sj = __shfl_sync(kAll, si, j);
+        if (lane < M) Hi[lane * M + j] = si * sj * acc[j];
     }
     __syncwarp();
     return true;
@@ -633,8 +646,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
             if (lane < 3 * NMOM) sm.mom[lane] = sm.aug[NVA + lane];
             if (lane + 32 < 3 * NMOM) sm.mom[lane + 32] = sm.aug[NVA + lane + 32];
             __syncwarp();
-            assemble_hessian<ORDER>(sm.mom, sm.Hi, lane);
-            if (!chol_inverse_regs<M>(sm.Hi, sm.L, sm.linv, sm.Hi, lane)) st = GPV_SINGULAR_H;
+            if (!hess_inverse_regs<ORDER>(sm.mom, sm.L, sm.linv, sm.Hi, lane)) st = GPV_SINGULAR_H;
         }
         if (lane == 0) {
             sm.flag[0] = st;
@@ -852,11 +864,12 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
             const double t2 = __shfl_sync(0xffffffffu, tl, 2);
             const double gmt = t0 * inv_dn;
             const double dg2 = t1 - t0 * gmt;
-            const double dg = sqrt(dg2 > 0.0 ? dg2 : 0.0);
+            const double dg2p = dg2 > 0.0 ? dg2 : 0.0;
+            const double dg = sqrt(dg2p);
             // sum (f - f_m)(g - g_m) = sum (f - f_m)(g - f_m) (sum (f - f_m) = 0)
             //                     = sum (f - s)(g - f_m) - (f_m - s) sum (g - f_m)
             const double sab = t2 - (fm - (double)shift) * t0;
-            const double rdg = 1.0 / dg;  // one reciprocal on the update's critical path
+            const double rdg = rsqrt(dg2p);  // 1 / delta_g: one reciprocal square root on the update's critical path
             const double znssd = 2.0 - 2.0 * sab * (inv_df * rdg);
             const double ratio = df * rdg;
             // lane j < M: grad_j = A_j - (df/dg)(B_j - g~_m S_j); B_j sits at lane 3 + j
