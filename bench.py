@@ -43,7 +43,7 @@ os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one full-size
 # second-order solve launch, by kernel (captured separately, not in this run)
-ICGN_C2_DRAM_BYTES = {"icgn_tile<2,128>": 977.85e6, "icgn_runs<2,128,4>": 1161.24e6}
+ICGN_C2_DRAM_BYTES = {"icgn_tile<2,128>": 977.85e6, "icgn_runs<2,128,4>": 1136.39e6}
 
 METRIC = "ICGN subsets/s at <=1e-3 px vs FP64 oracle; p50/p99 served solve latency"
 
