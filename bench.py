@@ -238,7 +238,7 @@ def load_workload(args):
 def common_config(W, args, world):
     """The workload's `config` object, the same in both arms."""
     h, w = W["f"].shape
-    l2_bytes = 2 * 4 * (h + 40) * (w + 40) + 2 * 8 * h * (w + 40)
+    l2_bytes = 2 * 4 * (h + 40) * (w + 40) + 2 * W["f"].dtype.itemsize * h * w
     orders = np.unique(W["order"])
     return {"workload": W["name"], "subsets": int(len(W["coords"])), "image": [int(h), int(w)],
             "pixel_dtype": str(W["f"].dtype), "radius": int(np.max(W["radius"])),
@@ -246,18 +246,19 @@ def common_config(W, args, world):
             "max_iterations": 15 if args.config == 1 else 50,
             "step": "prefilter(f)+prefilter(g)+batched ICGN solve of every subset",
             "l2": (("inputs larger than L2" if l2_bytes > 126e6 else "inputs SMALLER than L2 (profiling case)") +
-                   f": 2 x {h + 40}x{w + 40} FP32 coefficients + FP64 row passes ({l2_bytes / 1e6:.0f} MB)"
+                   f": 2 x {h + 40}x{w + 40} FP32 coefficients + 2 x {h}x{w} pixels ({l2_bytes / 1e6:.0f} MB)"
                    " rewritten each step"),
             "parallelism": f"replicas x{world}"}
 
 
 def measured_hbm_gbs():
-    """HBM copy bandwidth measured on this pool (MEASURED_PEAKS.json), else
-    the pool's earlier measurement."""
+    """(GB/s, source): the HBM copy bandwidth measured on this pool
+    (MEASURED_PEAKS.json), else the pool's earlier measurement (fallback)."""
     try:
-        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), \
+            "MEASURED_PEAKS.json hbm_gbs (of measured)"
     except Exception:
-        return 6650.0
+        return 6650.0, "6,650 GB/s copy rate measured earlier on this pool (of fallback: MEASURED_PEAKS.json absent)"
 
 
 def algorithmic_flop(res):
@@ -1078,10 +1079,9 @@ def run_ours(args, world, rank, local):
     # coefficient-window bytes at the measured HBM bandwidth
     coef_bytes = float(np.sum((res["iterations"].astype(np.float64) + 1.0) *
                               (2.0 * desc["radius"].astype(np.float64) + 6.0) ** 2 * 4.0))
-    hbm_gbs = measured_hbm_gbs()
+    hbm_gbs, hbm_source = measured_hbm_gbs()
     t_fma = flop / (fp32_peak * 1e12) if fp32_peak else 0.0
     t_bytes = coef_bytes / (hbm_gbs * 1e9)
-    l2_bytes = 2 * 4 * (h + 40) * (w + 40) + 2 * 8 * h * (w + 40)
     line = {
         "metric": METRIC, "value": value, "unit": "subsets/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -1112,7 +1112,7 @@ def run_ours(args, world, rank, local):
                      "roofline_frac": max(t_fma, t_bytes) / (solve_avg_ms * 1e-3),
                      "hbm": {"algorithmic_bytes": coef_bytes, "achieved_gbs": coef_bytes / (solve_avg_ms * 1e-3) / 1e9,
                              "peak_gbs": hbm_gbs, "frac": coef_bytes / (solve_avg_ms * 1e-3) / 1e9 / hbm_gbs,
-                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                             "peak_source": hbm_source,
                              "bytes": "(2r+6)^2 x 4 B coefficient window per subset per iteration and per setup"}},
         "e2e": {"value": e2e_value, "unit": "subsets/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "latency_ms": {"p50": 1e3 * float(np.percentile(lat, 50)), "p99": 1e3 * float(np.percentile(lat, 99))}},
