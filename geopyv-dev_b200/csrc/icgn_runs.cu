@@ -62,6 +62,7 @@ struct RunSmem {
     double L[144];     // Cholesky factor of the scaled Hessian, then its inverse (row-major)
     double Hi[144];    // the Hessian, replaced by H^-1 formed from the factor
     double linv[12];   // 1 / L_jj
+    double dsc[12];    // Jacobi scale 1 / sqrt(H_jj)
     double A[12], S[12];
     double p[12], pprev[12], dp[12], grad[12];
     double red[NW][16];
@@ -211,19 +212,21 @@ __device__ __forceinline__ double run_block_sum(double v, RunSmem<NT / 32> &sm) 
     return t;
 }
 
-// H^-1 of the Jacobi-scaled SPD Hessian by one warp, through its Cholesky
-// factor, in registers: D H D = L L^T with D = diag(1 / sqrt(H_jj)), then
-// H^-1 = D L^-T L^-1 D.  Lane i < M builds row i of H from the gradient
+// The Cholesky factor of the Jacobi-scaled SPD Hessian and the factor's
+// inverse, by one warp in registers: D H D = L L^T with D = diag(1 /
+// sqrt(H_jj)), so H^-1 = D L^-T L^-1 D.  Lane i < M builds row i of H from the gradient
 // moments (H_jk = c_j c_k sum g_p g_q dx^a dy^b, the entries assemble_hessian
 // gives) and keeps it in registers; the pivot and the column entries each
 // step needs travel by shuffle.  Each pivot takes one reciprocal square root
 // (1 / L_kk, and L_kk = pivot x that), not a square root and a division:
 // the serial chain of a lone warp is what this stretch costs.  Lane c then
 // solves L x = e_c for column c of L^-1 (rows of L read from Lm, M*M shared
-// scratch) and lane i forms row i of H^-1 into Hi.  False (warp-uniform)
-// when a pivot is not positive or not finite: a singular Hessian.
+// scratch), which then holds L^-1 (zeros above the diagonal), and lane i
+// stores s_i = 1 / sqrt(H_ii) in dsc; hess_inverse_block forms H^-1 from
+// them.  False (warp-uniform) when a pivot is not positive or not finite:
+// a singular Hessian.
 template <int ORDER>
-__device__ bool hess_inverse_regs(const double *mom, double *Lm, double *linv, double *Hi, int lane) {
+__device__ bool hess_factor_regs(const double *mom, double *Lm, double *linv, double *dsc, int lane) {
     using O = Ord<ORDER>;
     constexpr int M = O::M;
     constexpr unsigned kAll = 0xffffffffu;
@@ -281,24 +284,24 @@ __device__ bool hess_inverse_regs(const double *mom, double *Lm, double *linv, d
 #pragma unroll
         for (int i = 0; i < M; i++) Lm[i * M + lane] = x[i];  // Lm now holds L^-1 (lower)
     }
-    __syncwarp();
-    // row i = lane of D L^-T L^-1 D: entry j is the dot product of columns i
-    // and j of L^-1 (all M entries side by side: chains of M FMAs)
-    double acc[M];
-#pragma unroll
-    for (int j = 0; j < M; j++) acc[j] = 0.0;
-#pragma unroll
-    for (int k = 0; k < M; k++) {
-#pragma unroll
-        for (int j = 0; j < M; j++) acc[j] = fma(x[k], Lm[k * M + j], acc[j]);
-    }
-#pragma unroll
-    for (int j = 0; j < M; j++) {
-        const double sj = __shfl_sync(kAll, si, j);
-        if (lane < M) Hi[lane * M + j] = si * sj * acc[j];
-    }
+    if (lane < M) dsc[lane] = si;
     __syncwarp();
     return true;
+}
+
+// H^-1 = D L^-T L^-1 D from hess_factor_regs's L^-1 (Lm) and D (dsc), by
+// the whole block between two barriers (no warp waits on another's serial
+// work here): entry (i, j) is s_i s_j times the dot product of columns i
+// and j of L^-1.
+template <int M, int NT>
+__device__ __forceinline__ void hess_inverse_block(const double *Lm, const double *dsc, double *Hi) {
+    for (int e = threadIdx.x; e < M * M; e += NT) {
+        const int i = e / M, j = e - (e / M) * M;
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < M; k++) acc = fma(Lm[k * M + i], Lm[k * M + j], acc);
+        Hi[e] = dsc[i] * dsc[j] * acc;
+    }
 }
 
 // The quintic basis at fraction t as symmetric pairs W[k] = (w_k, w_{5-k}),
@@ -646,7 +649,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
             if (lane < 3 * NMOM) sm.mom[lane] = sm.aug[NVA + lane];
             if (lane + 32 < 3 * NMOM) sm.mom[lane + 32] = sm.aug[NVA + lane + 32];
             __syncwarp();
-            if (!hess_inverse_regs<ORDER>(sm.mom, sm.L, sm.linv, sm.Hi, lane)) st = GPV_SINGULAR_H;
+            if (!hess_factor_regs<ORDER>(sm.mom, sm.L, sm.linv, sm.dsc, lane)) st = GPV_SINGULAR_H;
         }
         if (lane == 0) {
             sm.flag[0] = st;
@@ -691,6 +694,8 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
         }
         return;
     }
+    // H^-1 by every thread (warp 0 reads it only after the first iteration's barrier)
+    hess_inverse_block<M, NT>(sm.L, sm.dsc, sm.Hi);
 
     // ---- ICGN iterations --------------------------------------------------
     const double size = sqrt(dn);
