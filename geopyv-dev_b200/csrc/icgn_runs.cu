@@ -356,9 +356,10 @@ struct KSum {
     }
 };
 
-// One sample: rec = (f - s, df/dx, df/dy, w) with w = 1 for template
-// pixels, 0 outside; pfg sums (f - s)(g - f_m) (corrected to f - f_m with
-// the block totals).  KAHAN: the three ZNSSD sums (g - f_m, its square and
+// One sample: rec = (df/dx, df/dy, f - s, w) with w = 1 for template
+// pixels, 0 outside (the gradient pair first: one aligned register pair,
+// so the steepest-descent products and sums are paired FP32 operations);
+// pfg sums (f - s)(g - f_m) (corrected to f - f_m with the block totals).  KAHAN: the three ZNSSD sums (g - f_m, its square and
 // the cross term) go straight into the thread's compensated FP64 sums ks
 // instead of the run's FP32 partials.
 template <int ORDER, bool KAHAN>
@@ -368,23 +369,18 @@ __device__ __forceinline__ void acc_sample(RunAcc &a, KSum (&ks)[3], float4 rec,
         const double gd = (double)gc;
         ks[0].add(gd);
         ks[1].add(gd * gd);
-        ks[2].add((double)rec.x * gd);
+        ks[2].add((double)rec.z * gd);
     } else {
         a.p1 += gc;
         a.p2 = fmaf(gc, gc, a.p2);
-        a.pfg = fmaf(rec.x, gc, a.pfg);
+        a.pfg = fmaf(rec.z, gc, a.pfg);
     }
-    const float gxc = rec.y * gc, gyc = rec.z * gc;
-    a.m0.x += gxc;
-    a.m0.y += gyc;
-    if (ORDER >= 1) {
-        a.m1.x = fmaf(gxc, dyf, a.m1.x);
-        a.m1.y = fmaf(gyc, dyf, a.m1.y);
-    }
+    const float2 gxy = __fmul2_rn(make_float2(rec.x, rec.y), make_float2(gc, gc));
+    a.m0 = __fadd2_rn(a.m0, gxy);
+    if (ORDER >= 1) a.m1 = __ffma2_rn(gxy, make_float2(dyf, dyf), a.m1);
     if (ORDER == 2) {
         const float d2 = dyf * dyf;
-        a.m2.x = fmaf(gxc, d2, a.m2.x);
-        a.m2.y = fmaf(gyc, d2, a.m2.y);
+        a.m2 = __ffma2_rn(gxy, make_float2(d2, d2), a.m2);
     }
 }
 
@@ -422,7 +418,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
     const int T = R.task_n[r];
     const int2 *tasks = R.tasks + R.task_off[r];
     const int NS = T * K;
-    // per-pixel records (f - s, df/dx, df/dy, 1 in the template / 0 outside:
+    // per-pixel records (df/dx, df/dy, f - s, 1 in the template / 0 outside:
     // zero gradients outside) in slot j * T + t of run t; eta resamples; run bits
     float4 *REC = reinterpret_cast<float4 *>(base);
     float *RSG = base + 4 * R.nslot;
@@ -550,7 +546,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
                         vy = fmaf(da0[rr], s[j + rr], vy);
                     }
                     const bool v = (vm >> j) & 1u;
-                    REC[j * T + t] = v ? make_float4(val - shift, vx, vy, 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    REC[j * T + t] = v ? make_float4(vx, vy, val - shift, 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
                     pix1(v, val, vx, vy, dx, dy0 + j);
                 }
             } else {
@@ -571,7 +567,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
                         const float *F = A.f32 + (int64_t)(iy + B - 2) * A.pitch32 + (ix + B - 2);
                         f = contract_grad<float>(F, A.pitch32, a, da, b, db, gx, gy);
                     }
-                    REC[j * T + t] = v ? make_float4(f - shift, gx, gy, 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    REC[j * T + t] = v ? make_float4(gx, gy, f - shift, 1.f) : make_float4(0.f, 0.f, 0.f, 0.f);
                     pix1(v, f, gx, gy, dx, dy0 + j);
                 }
             }
@@ -596,7 +592,7 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
 #pragma unroll
             for (int j = 0; j < K; j++) {
                 const float4 rec = REC[j * T + t];
-                const float gx = rec.y, gy = rec.z;  // zero for pixels outside the template
+                const float gx = rec.x, gy = rec.y;  // zero for pixels outside the template
                 const float gg[3] = {gx * gx, gx * gy, gy * gy};
                 const float dyf = (float)(dy0 + j);
                 float pw = 1.f;
@@ -984,8 +980,8 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
             int dxi, dy0;
             unpack_task(tasks[t], dxi, dy0);
             const float4 rec = REC[i];
-            f = (double)rec.x + (double)shift;
-            gx = rec.y; gy = rec.z; g = RSG[i];
+            f = (double)rec.z + (double)shift;
+            gx = rec.x; gy = rec.y; g = RSG[i];
             dx = dxi; dy = dy0 + j;
             return true;
         };
