@@ -305,22 +305,23 @@ __device__ __forceinline__ void hess_inverse_block(const double *Lm, const doubl
 }
 
 // The quintic basis at fraction t as symmetric pairs W[k] = (w_k, w_{5-k}),
-// k = 0..2: the same values as basis() (the split about t = 1/2, w_k = e_k +
-// o_k, w_{5-k} = e_k - o_k), in scalar FP32 ops whose polynomial
-// coefficients are instruction immediates; each sum and difference lands in
-// its half of the pair.
+// k = 0..2: the weights of basis() split about t = 1/2 into an even part
+// e_k(v) and an odd part -u P_k(v) (u = t - 1/2, v = u^2), w_k = e_k - u P_k
+// and w_{5-k} = e_k + u P_k, each one FMA (the odd part is never rounded on
+// its own), in scalar FP32 ops whose polynomial coefficients are
+// instruction immediates; each weight lands in its half of the pair.
 __device__ __forceinline__ void basis_sym1(float t, float2 W[3]) {
     const float u = t - 0.5f;
     const float v = u * u;
     const float e0 = fmaf(fmaf(v, 1.0f / 48.0f, 1.0f / 96.0f), v, 1.0f / 3840.0f);
     const float e1 = fmaf(fmaf(v, -1.0f / 16.0f, 7.0f / 32.0f), v, 79.0f / 1280.0f);
     const float e2 = fmaf(fmaf(v, 1.0f / 24.0f, -11.0f / 48.0f), v, 841.0f / 1920.0f);
-    const float o0 = -u * fmaf(fmaf(v, 1.0f / 120.0f, 1.0f / 48.0f), v, 1.0f / 384.0f);
-    const float o1 = -u * fmaf(fmaf(v, -1.0f / 24.0f, 1.0f / 16.0f), v, 25.0f / 128.0f);
-    const float o2 = -u * fmaf(fmaf(v, 1.0f / 12.0f, -7.0f / 24.0f), v, 77.0f / 192.0f);
-    W[0] = make_float2(e0 + o0, e0 - o0);
-    W[1] = make_float2(e1 + o1, e1 - o1);
-    W[2] = make_float2(e2 + o2, e2 - o2);
+    const float q0 = fmaf(fmaf(v, 1.0f / 120.0f, 1.0f / 48.0f), v, 1.0f / 384.0f);
+    const float q1 = fmaf(fmaf(v, -1.0f / 24.0f, 1.0f / 16.0f), v, 25.0f / 128.0f);
+    const float q2 = fmaf(fmaf(v, 1.0f / 12.0f, -7.0f / 24.0f), v, 77.0f / 192.0f);
+    W[0] = make_float2(fmaf(-u, q0, e0), fmaf(u, q0, e0));
+    W[1] = make_float2(fmaf(-u, q1, e1), fmaf(u, q1, e1));
+    W[2] = make_float2(fmaf(-u, q2, e2), fmaf(u, q2, e2));
 }
 
 // One coefficient row against the column weights: sum_k b_k c_k with the
@@ -768,9 +769,10 @@ __device__ void run_subset(const RunArgs &R, int idx, const gpv_subset_desc &d, 
                 int fxp = 0, fyp = 0;
                 // window position of the run's first pixel at zero small part
                 const float *rbase = win + (dy0 + wy0) * gP + (dx + wx0);
+                const float dy0f = (float)dy0;
 #pragma unroll
                 for (int j = 0; j < K; j++) {
-                    const float dyf = (float)(dy0 + j);
+                    const float dyf = dy0f + (float)j;  // exact: small integers
                     float2 L = A2;
                     if (ORDER >= 1) L = __ffma2_rn(B2, make_float2(dyf, dyf), L);
                     if (ORDER == 2) L = __ffma2_rn(C2, make_float2(dyf * dyf, dyf * dyf), L);
