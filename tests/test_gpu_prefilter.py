@@ -15,6 +15,8 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("shape,border,dtype", [
     ((40, 57), 20, np.uint8),     # short lines: the all-residue (N < 89) path
     ((64, 50), 3, np.float64),    # minimum border
+    ((40, 300), 20, np.uint8),    # long rows, short columns: the short-line path with 89-tap rows
+    ((130, 100), 20, np.float64),  # fused kernel, FP64 pixels and FP64 coefficients (its largest staging)
     ((200, 300), 20, np.uint8),
     ((257, 129), 20, np.uint16),
     ((1024, 1024), 20, np.uint8),
